@@ -1,0 +1,380 @@
+#!/usr/bin/env python
+"""bench.py -- throughput of nuosc's RK4 time step on B200 (cell-steps/s).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (the production configuration): periodic 2D box of 1024 x 1024 cells
+(dx = dz = 0.05, x,z in [-25.6, 25.6)), 642 icosahedral velocities (nn = 8),
+FP64 state, 6th-difference Kreiss-Oliger (3 ghosts), CFL 0.4, ko 0.1, mu 1,
+alpha 0.9, spectra widths 0.6/0.5, seeded eps = 1e-6 U(-1,1) per cell.
+One step = one RK4 step over the whole grid; cell-steps/s = nx*nz*nv per
+step / seconds per step.  Each register is 43 GB, far larger than L2, so
+no L2 flush is needed between steps.
+
+value    device-timed (CUDA events on the solver's stream), W warm-up steps,
+         then K steps, max over ranks; state resident in HBM.
+e2e      the same metric through the public C ABI with host buffers: upload
+         the state from pinned host memory, K steps each followed by
+         analysis() (diagnostics read back), download the final state.
+roofline the dominant kernel (the S2/S3 stage kernel) timed live with CUDA
+         events: algorithmic bytes per launch (5 state passes x 8 fields x
+         8 B per cell-velocity) / mean launch time, against the measured HBM
+         copy bandwidth in MEASURED_PEAKS.json.
+N > 1    one independent full-size solve per GPU (the reference's hot path has
+         no exchange on one GPU); value = all ranks' cell-steps / max time.
+--impl reference   the reference's own CPU build (oracle/_ref, or the C
+         oracle where that build is absent) on the host cores, each step one
+         RK4 step of a bounded 128 x 128 x 642 sample of the workload.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "cell-steps/s"
+BYTES_PER_CELL_STEP = {"f64": 1024, "f32": 512}  # 16 state passes x 8 fields x sizeof(real)
+STAGE_S23_PASSES = 5
+
+
+def workload(size, nn, precision):
+    dx = 0.05 if size == 1024 else 51.2 / size
+    L = size * dx / 2.0
+    return dict(n=size, nn=nn, dx=dx, x0=-L, x1=L, precision=precision, cfl=0.4, ko=0.1, mu=1.0, alpha=0.9,
+                lnue=0.6, lnueb=0.5, eps0=1e-6, seed=20240601)
+
+
+def config_of(w, nv, l2_note):
+    return {"workload": "RK4 step, %dx%d cells x %d velocities (icosahedron nn=%d), %s state, 6th-difference KO"
+                        % (w["n"], w["n"], nv, w["nn"], "FP64" if w["precision"] == 0 else "FP32"),
+            "nx": w["n"], "nz": w["n"], "nv": nv, "dx": w["dx"], "cfl": w["cfl"], "ko": w["ko"], "mu": w["mu"],
+            "alpha": w["alpha"], "precision": "fp64" if w["precision"] == 0 else "fp32",
+            "l2": l2_note, "parallelism": "replicas (one solve per GPU)"}
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(prefix="nuosc_clocks_", suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        try:
+            for line in open(self.path):
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        except Exception:
+            pass
+        finally:
+            try:
+                os.unlink(self.path)
+            except Exception:
+                pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ---------------------------------------------------------------- helpers
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def traffic_per_launch(kernel_key):
+    """DRAM bytes per launch of the named kernel from the committed ncu summary, or None."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            return json.load(f).get(kernel_key)
+    except Exception:
+        return None
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# ---------------------------------------------------------------- CPU arms
+def cpu_worker(args):
+    """Runs in a subprocess: time RK4 steps of the reference build (or oracle)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as po
+    w = workload(args.cpu_size, args.cpu_nn, 0)
+    L = w["n"] * 0.1 / 2
+    kw = dict(nn=w["nn"], x0=-L, x1=L, z0=-L, z1=L, dx=0.1, dz=0.1, cfl=0.4, ko=0.1, ko_order=6, mu=1.0, pmo=0.0)
+    kind = "reference" if po.ref_available(6) else "port"
+    sim = po.RefSim(**kw) if kind == "reference" else po.Oracle(**kw)
+    sim.fill_init(ipt=1, alpha=0.9, eps0=1e-6, lnue=0.6, lnueb=0.5, seed=w["seed"])
+    nx, nz, nv = sim.shape
+    for _ in range(args.cpu_warmup):
+        sim.step(1)
+    times = []
+    t_start = time.perf_counter()
+    for k in range(args.cpu_steps):
+        t0 = time.perf_counter()
+        sim.step(1)
+        times.append(time.perf_counter() - t0)
+        if time.perf_counter() - t_start > args.cpu_budget and k + 1 >= 2:
+            break
+    total = sum(times)
+    print(json.dumps({"kind": kind, "nx": nx, "nz": nz, "nv": nv, "steps": len(times), "seconds": total,
+                      "value": nx * nz * nv * len(times) / total, "ms_per_step": 1e3 * total / len(times)}))
+
+
+def run_cpu(size, nn, steps, warmup, budget):
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    env = dict(os.environ, OMP_NUM_THREADS=str(cores), OMP_PROC_BIND="close")
+    cmd = [sys.executable, os.path.abspath(__file__), "--cpu-worker", "--cpu-size", str(size), "--cpu-nn", str(nn),
+           "--cpu-steps", str(steps), "--cpu-warmup", str(warmup), "--cpu-budget", str(budget)]
+    out = subprocess.run(cmd, env=env, stdout=subprocess.PIPE, stderr=subprocess.PIPE, check=True, timeout=1800)
+    res = json.loads(out.stdout.decode().strip().splitlines()[-1])
+    res["cores"] = cores
+    return res
+
+
+def cpu_baseline_obj(res):
+    return {"value": res["value"], "unit": METRIC, "cores": res["cores"], "kind": res["kind"],
+            "sample": "%dx%d cells x %d velocities, FP64, 6th-difference KO, %d RK4 steps after 1 warm-up, "
+                      "OMP threads=%d (%s)" % (res["nx"], res["nz"], res["nv"], res["steps"], res["cores"],
+                                               "reference CPU build oracle/_ref" if res["kind"] == "reference"
+                                               else "C restatement oracle/")}
+
+
+def bench_reference(args, world, rank):
+    w = workload(args.size, args.nn, args.precision)
+    nv = 10 * args.nn * args.nn + 2
+    if rank != 0:
+        return 0
+    res = run_cpu(args.cpu_sample, args.nn, args.steps, max(1, args.warmup), budget=1e9)
+    line = {"metric": METRIC, "value": res["value"], "unit": METRIC, "impl": "reference", "n_gpus": world,
+            "steps": res["steps"], "warmup": args.warmup, "ms_per_step": res["ms_per_step"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded eps per cell)", "config": config_of(w, nv, "n/a (CPU)"),
+            "cpu_baseline": cpu_baseline_obj(res),
+            "e2e": {"value": res["value"], "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------- GPU arm
+def bench_ours(args, world, rank, local):
+    import numpy as np
+    import torch
+    import nuosc_b200 as nb
+
+    torch.cuda.set_device(local)
+    w = workload(args.size, args.nn, args.precision)
+    g = 3
+    s = nb.NuOsc(1, 1, w["nn"], 0, g, g, w["x0"], w["x1"], w["x0"], w["x1"], w["dx"], w["dx"], w["cfl"], w["ko"],
+                 precision=w["precision"], device=local)
+    s.set_mu(w["mu"])
+    s.set_pmo(0.0)
+    if args.kernel is not None:
+        s.set_kernel(args.kernel)
+    s.fillInitValue(1, w["alpha"], w["eps0"], 1.0, w["lnue"], w["lnueb"], seed=w["seed"] + rank)
+    nx, nz, nv = s.grid.nx, s.grid.nz, s.grid.nv
+    cells = nx * nz * nv
+    dtype = "f64" if w["precision"] == nb.FP64 else "f32"
+    esize = 8 if dtype == "f64" else 4
+    stream = torch.cuda.ExternalStream(nb.lib().nuosc_stream(s.handle))
+
+    # warm-up
+    s.step_rk4(args.warmup)
+    s.synchronize()
+    # timed region: K steps, events on the solver's stream, per-kernel events too
+    s.set_profiling(True)
+    s.get_profile()
+    l0 = s.kernel_launches
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    barrier(world)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        s.step_rk4(args.steps)
+        e1.record(stream)
+        e1.synchronize()
+    torch.cuda.synchronize()
+    barrier(world)
+    launches = s.kernel_launches - l0
+    prof = s.get_profile()
+    s.set_profiling(False)
+    ms = max_over_ranks(e0.elapsed_time(e1), world)
+    ms_per_step = ms / args.steps
+    value = world * cells * args.steps / (ms / 1e3)
+    diag = s.analysis()
+
+    # dominant kernel: the S2/S3 stage kernel (two of four stages, five state passes)
+    k_ms, k_n = prof["stage_s23"]
+    peak, peak_kind = measured_peaks()
+    alg_bytes = STAGE_S23_PASSES * 8 * esize * cells
+    achieved = alg_bytes / (k_ms / k_n / 1e3) / 1e9 if k_n else None
+    step_gbs = BYTES_PER_CELL_STEP[dtype] * cells / (ms_per_step / 1e3) / 1e9
+    total_prof = sum(v[0] for v in prof.values()) or 1.0
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak if achieved else None,
+                "traffic": traffic_per_launch("stage_s23_%s_%d_%d" % (dtype, nx, nv)),
+                "kernel": "stage S2/S3 (%s)" % ("x-march" if prof["moment_finalize"][1] else "direct"),
+                "algorithmic_bytes_per_launch": alg_bytes,
+                "mean_launch_ms": k_ms / k_n if k_n else None,
+                "peak_source": "%s (MEASURED_PEAKS.json hbm_gbs)" % peak_kind if peak_kind == "measured"
+                else "fallback 6.65 TB/s",
+                "step_bytes_per_cell_step": BYTES_PER_CELL_STEP[dtype], "step_achieved_gbs": step_gbs,
+                "step_frac": step_gbs / peak, "frac_vs_8tbs": step_gbs / 8000.0,
+                "kernel_shares": {k: round(v[0] / total_prof, 4) for k, v in prof.items() if v[1]}}
+
+    # e2e through the C ABI with pinned host buffers
+    e2e = None
+    if not args.no_e2e:
+        host = [torch.empty((nx, nz, nv), dtype=torch.float64, pin_memory=True) for _ in range(8)]
+        arrs = [h.numpy() for h in host]
+        for f in range(8):
+            arrs[f][...] = s.get_field(f)
+        barrier(world)
+        t0 = time.perf_counter()
+        for f in range(8):
+            s.set_field(f, arrs[f])
+        for _ in range(args.steps):
+            s.step_rk4(1)
+            s.analysis()
+        for f in range(8):
+            nb._lib.check(nb.lib().nuosc_get_state(s.handle, 0, f, arrs[f].ctypes.data_as(
+                __import__("ctypes").POINTER(__import__("ctypes").c_double)), 0))
+        t1 = time.perf_counter()
+        barrier(world)
+        e2e_s = max_over_ranks(t1 - t0, world)
+        state_bytes = 8 * cells * 8
+        diag_bytes = 12 * 8
+        e2e = {"value": world * cells * args.steps / e2e_s, "unit": METRIC,
+               "h2d_bytes_per_step": state_bytes / args.steps,
+               "d2h_bytes_per_step": state_bytes / args.steps + diag_bytes,
+               "seconds": e2e_s, "pinned": True,
+               "note": "upload state from pinned host memory, K x (step_rk4 + analysis), download state"}
+        del host, arrs
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            cpu = cpu_baseline_obj(run_cpu(args.cpu_sample, args.nn, 20, 1, budget=args.cpu_seconds))
+        except Exception as ex:  # report, do not fail the GPU number
+            cpu = {"value": None, "error": str(ex)[:200]}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": dtype, "data": "synthetic (seeded eps per cell)",
+                "config": config_of(w, nv, "inputs larger than L2 (%.1f GB per register)" % (8 * cells * esize / 1e9)),
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(),
+                "gpu_launches": launches, "diag_after": {k: diag[k] for k in ("phy_time", "maxdP", "surv", "aM0")}}
+        print(json.dumps(line))
+    s.close()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--size", type=int, default=1024)
+    ap.add_argument("--nn", type=int, default=8)
+    ap.add_argument("--precision", type=int, default=0, help="0 fp64, 1 fp32")
+    ap.add_argument("--kernel", type=int, default=None, help="0 auto, 1 direct, 2 x-march")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-sample", type=int, default=128)
+    ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    # internal: CPU worker subprocess
+    ap.add_argument("--cpu-worker", action="store_true")
+    ap.add_argument("--cpu-size", type=int, default=128)
+    ap.add_argument("--cpu-nn", type=int, default=8)
+    ap.add_argument("--cpu-steps", type=int, default=5)
+    ap.add_argument("--cpu-warmup", type=int, default=1)
+    ap.add_argument("--cpu-budget", type=float, default=20.0)
+    args = ap.parse_args()
+    if args.cpu_worker:
+        return cpu_worker(args)
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    world, rank, local = dist_setup(args)
+    try:
+        if args.impl == "reference":
+            return bench_reference(args, world, rank)
+        return bench_ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

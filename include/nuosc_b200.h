@@ -1,0 +1,201 @@
+/*
+ * nuosc_b200.h -- C ABI of the B200-native nuosc RK4 time step.
+ *
+ * One handle = one solve on one GPU: the 2D periodic (x,z) box times the
+ * icosahedral velocity sphere, with the 8 real fields of rho and rho-bar
+ * (ee, mm, Re em, Im em and their barred partners) resident in HBM.  Every
+ * entry point returns 0 on success or a NUOSC_ERR_* code; the message of the
+ * last failure on the calling thread is available from nuosc_last_error().
+ * Device memory is owned by the handle.  Work is ordered on the handle's own
+ * CUDA stream; entry points that return host data synchronise that stream.
+ *
+ * Each declaration names the member of the reference's C++ class NuOsc
+ * (chunyulin/nuosc, nuosc_class.h:99-191) that it replaces.  Register ids
+ * stand for NuOsc's FieldVar pointers v_stat, v_rhs, v_pre, v_cor
+ * (nuosc_class.h:108); field ids follow FieldVar::getAllFields
+ * (nuosc_class.h:58-65).
+ */
+#ifndef NUOSC_B200_H
+#define NUOSC_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define NUOSC_OK 0
+#define NUOSC_ERR_INVALID 1     /* bad argument or call order */
+#define NUOSC_ERR_CUDA 2        /* a CUDA runtime call failed */
+#define NUOSC_ERR_OOM 3         /* not enough device memory for the request */
+#define NUOSC_ERR_NUMERIC 4     /* non-finite state or max||P|-1| >= 10 (nuosc_ana.cpp:131 assert) */
+#define NUOSC_ERR_TIMEOUT 5     /* a bounded in-kernel wait expired; the kernel returned early */
+#define NUOSC_ERR_UNSUPPORTED 6 /* a configuration this build does not implement */
+
+/* precision of the resident state */
+#define NUOSC_FP64 0 /* state and arithmetic in double (the reference's real, common.h:58) */
+#define NUOSC_FP32 1 /* state and stencil arithmetic in float; moments and diagnostics in double */
+
+/* registers (NuOsc FieldVar pointers) */
+#define NUOSC_REG_STAT 0
+#define NUOSC_REG_RHS 1
+#define NUOSC_REG_PRE 2
+#define NUOSC_REG_COR 3
+
+/* fields: 0..7 are the state (FieldVar order); 8..15 are derived per point
+ * from the current v_stat as eval_conserved does (nuosc_ana.cpp:8-28) */
+#define NUOSC_EE 0
+#define NUOSC_MM 1
+#define NUOSC_EMR 2
+#define NUOSC_EMI 3
+#define NUOSC_BEE 4
+#define NUOSC_BMM 5
+#define NUOSC_BEMR 6
+#define NUOSC_BEMI 7
+#define NUOSC_P1 8
+#define NUOSC_P2 9
+#define NUOSC_P3 10
+#define NUOSC_P1B 11
+#define NUOSC_P2B 12
+#define NUOSC_P3B 13
+#define NUOSC_DP 14
+#define NUOSC_DPB 15
+
+/* host array layouts for state transfer */
+#define NUOSC_LAYOUT_COMPACT 0 /* [x][z][v], nx*nz*nv doubles, no ghosts */
+#define NUOSC_LAYOUT_GHOSTED 1 /* the reference's array: [(i+gx)*(nz+2gz)+j+gz]*nv+v (CartGrid.h:91) */
+
+/* stage-kernel selection (nuosc_set_kernel) */
+#define NUOSC_KERNEL_AUTO 0   /* the fused x-march kernel when the geometry allows, else direct */
+#define NUOSC_KERNEL_DIRECT 1 /* one thread per (cell, velocity), separate moment pass */
+#define NUOSC_KERNEL_XMARCH 2 /* bulk-copy staged x-march with fused moments */
+
+typedef struct nuosc_handle nuosc_handle;
+
+/* Constructor arguments of NuOsc::NuOsc (nuosc_class.cpp:454-457). */
+typedef struct nuosc_params {
+    int px, pz;    /* process grid; must be 1, 1: one solve lives on one GPU */
+    int nv;        /* icosahedron subdivision count nn: 10*nn*nn+2 velocities (the reference's --nv) */
+    int nphi;      /* unused (polar velocity grid, IM_V2D_POLAR_GRID, is not built) */
+    int gx, gz;    /* ghost width: 3 selects the 6th-difference KO (KO_ORD_3 undefined), 2 the 4th-difference KO */
+    double x0, x1; /* box [x0, x1) */
+    double z0, z1; /* box [z0, z1) */
+    double dx, dz; /* nx = int((x1-x0)/dx), nz = int((z1-z0)/dz) (CartGrid.cpp:196-197) */
+    double cfl;    /* dt = dz*cfl (nuosc_class.cpp:464) */
+    double ko;     /* Kreiss-Oliger strength */
+    int precision; /* NUOSC_FP64 or NUOSC_FP32 */
+    int device;    /* CUDA device ordinal */
+} nuosc_params;
+
+typedef struct nuosc_geometry {
+    int nx, nz, nv;     /* interior cells and velocities */
+    int nv_stride;      /* velocities per (x,z) row in device memory (nv padded to a 16-byte row) */
+    int gx, gz;         /* ghost width given at creation (selects the KO order) */
+    int precision;
+    double dt, ds_L, phy_time;
+    double x0, x1, z0, z1, dx, dz;
+    double n_nue0[2];   /* initial number densities (nuosc_init.cpp:129-130) */
+    size_t device_bytes; /* device memory held by the handle */
+} nuosc_geometry;
+
+/* One analysis() record: the analysis.dat columns (nuosc_ana.cpp:126-129). */
+typedef struct nuosc_diag {
+    double phy_time, maxdP, surv, survb, avgP, avgPb, aM0, Lex, ELNe;
+    long long nonfinite; /* count of non-finite state values seen by the reduction */
+} nuosc_diag;
+
+/* gen_v2d_icosahedron (CartGrid.cpp:46-61, icosahedron.h:36-171): the velocity
+ * quadrature for subdivision nn, host only (no GPU needed); arrays hold
+ * 10*nn*nn+2 entries.  Returns the count in *n_out when n_out is not null. */
+int nuosc_velocity_quadrature(int nn, double *vx, double *vy, double *vz, double *vw, int *n_out);
+
+/* NuOsc::NuOsc (nuosc_class.cpp:454-576) and CartGrid::CartGrid (CartGrid.cpp:122-247) */
+int nuosc_create(const nuosc_params *params, nuosc_handle **out);
+/* NuOsc::~NuOsc (nuosc_class.h:136-146) */
+int nuosc_destroy(nuosc_handle *h);
+/* message of the last failed call on this thread ("" if none) */
+const char *nuosc_last_error(void);
+
+/* NuOsc::set_mu / set_pmo / set_renorm (nuosc_class.h:148-159) */
+int nuosc_set_mu(nuosc_handle *h, double mu);
+int nuosc_set_pmo(nuosc_handle *h, double pmo);
+int nuosc_set_renorm(nuosc_handle *h, int renorm);
+/* stage-kernel choice (NUOSC_KERNEL_*); no counterpart in the reference */
+int nuosc_set_kernel(nuosc_handle *h, int kind);
+
+/* grid geometry (CartGrid members) and the velocity quadrature (CartGrid::vx,vy,vz,vw) */
+int nuosc_get_geometry(const nuosc_handle *h, nuosc_geometry *out);
+int nuosc_get_velocities(const nuosc_handle *h, double *vx, double *vy, double *vz, double *vw);
+/* the angular spectra G0, G0b per velocity (NuOsc::G0, G0b; nuosc_init.cpp:95-96) */
+int nuosc_get_spectra(const nuosc_handle *h, double *G0, double *G0b);
+/* set G0/G0b and n_nue0 directly (for a state supplied with nuosc_set_state) */
+int nuosc_set_spectra(nuosc_handle *h, const double *G0, const double *G0b, double n_nue0, double n_nueb0);
+/* physical time (NuOsc::phy_time) */
+int nuosc_set_time(nuosc_handle *h, double phy_time);
+
+/* NuOsc::fillInitValue (nuosc_init.cpp:17-137), generic branch.  ipt 0: Gaussian
+ * eps in z; 1: eps0*U(-1,1) per (x,z) cell from `seed` (replaces rand());
+ * 2: eps_p profile; 3: constant eps0.  lnuex/lnuebx <= 0 mean unbounded
+ * (the reference default DBL_MAX). */
+int nuosc_fill_init(nuosc_handle *h, int ipt, double alpha, double eps0, double sigma, double lnue,
+                    double lnueb, double lnuex, double lnuebx, uint64_t seed);
+
+/* direct access to FieldVar arrays (callers of the reference read and write
+ * v_stat->ee[...] in place); host arrays of double in the given layout */
+int nuosc_set_state(nuosc_handle *h, int reg, int field, const double *host, int layout);
+int nuosc_get_state(nuosc_handle *h, int reg, int field, double *host, int layout);
+
+/* NuOsc::updatePeriodicBoundary (nuosc_boundary.cpp:4-52).  The stencil
+ * kernels wrap indices periodically, so no ghost cells exist on the device;
+ * this validates `reg` and returns. */
+int nuosc_update_periodic_boundary(nuosc_handle *h, int reg);
+
+/* NuOsc::calRHS (nuosc_class.cpp:11-307): register out = L(register in) */
+int nuosc_calrhs(nuosc_handle *h, int out_reg, int in_reg);
+/* NuOsc::vectorize (nuosc_class.cpp:313-351): dst = a1 + a*a2, dst = a1 + a*(a2 + a3) */
+int nuosc_vectorize(nuosc_handle *h, int dst, int src1, double a, int src2);
+int nuosc_vectorize2(nuosc_handle *h, int dst, int src1, double a, int src2, int src3);
+/* NuOsc::step_rk4 (nuosc_class.cpp:374-427), nsteps times; v_stat holds the
+ * new state afterwards (the other registers hold stage scratch) */
+int nuosc_step_rk4(nuosc_handle *h, int nsteps);
+
+/* NuOsc::analysis (nuosc_ana.cpp:34-137); appends a line to the analysis file
+ * when one is open (nuosc_open_analysis_file) */
+int nuosc_analysis(nuosc_handle *h, nuosc_diag *out);
+/* opens the analysis.dat writer the NuOsc constructor opens (nuosc_class.cpp:536-540) */
+int nuosc_open_analysis_file(nuosc_handle *h, const char *path);
+
+/* NuOsc::addSnapShotAtV / addSnapShotAtXV / checkSnapShot (nuosc_snapshot.cpp:13-122).
+ * `fields` are NUOSC_* field ids of the current v_stat (0..15). */
+int nuosc_add_snapshot_at_v(nuosc_handle *h, const int *fields, int nfields, const char *fntpl, int every,
+                            const int *vidx, int n_vidx);
+int nuosc_add_snapshot_at_xv(nuosc_handle *h, const int *fields, int nfields, const char *fntpl, int every,
+                             const int *xidx, int n_xidx, const int *vidx, int n_vidx);
+int nuosc_check_snapshot(nuosc_handle *h, int t);
+/* gather one snapshot block (sx * nz * sv doubles, (i,j,v) order) into host memory */
+int nuosc_gather(nuosc_handle *h, int field, const int *xidx, int n_xidx, const int *vidx, int n_vidx,
+                 double *host);
+
+/* wait for all work queued on the handle's stream */
+int nuosc_synchronize(nuosc_handle *h);
+/* the handle's cudaStream_t (as void*), for callers that order their own work after it */
+void *nuosc_stream(nuosc_handle *h);
+/* number of kernel launches issued by step_rk4/calrhs of this handle so far */
+long long nuosc_kernel_launches(const nuosc_handle *h);
+
+/* Per-kernel timing with CUDA events on the handle's stream (no counterpart
+ * in the reference, which prints wall time per step, nuosc.cpp:222-235).
+ * Kinds: 0 stage S1, 1 stage S2/S3, 2 stage S4, 3 calRHS, 4 moments,
+ * 5 moment finalize.  nuosc_get_profile synchronises, fills ms[k] (total
+ * milliseconds) and launches[k] for k < nkinds, and resets the counters. */
+#define NUOSC_PROF_KINDS 6
+int nuosc_set_profiling(nuosc_handle *h, int on);
+int nuosc_get_profile(nuosc_handle *h, double *ms, long long *launches, int nkinds);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NUOSC_B200_H */

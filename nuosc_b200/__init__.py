@@ -1,0 +1,261 @@
+"""nuosc_b200 -- B200-native RK4 time step of nuosc's 2D-space x velocity-sphere
+neutrino flavour kinetic equations.
+
+`NuOsc` mirrors the reference's C++ class NuOsc (nuosc_class.h:99-191): same
+constructor arguments, the same method names (set_mu, set_pmo, set_renorm,
+fillInitValue, calRHS, vectorize, step_rk4, updatePeriodicBoundary, analysis,
+addSnapShotAtV, addSnapShotAtXV, checkSnapShot) and the same meaning.  All of
+them call the C ABI of include/nuosc_b200.h; the state lives in HBM.
+
+    from nuosc_b200 import NuOsc
+    s = NuOsc(1, 1, 4, 0, 3, 3, -3.2, 3.2, -3.2, 3.2, 0.1, 0.1, 0.4, 0.1)
+    s.set_mu(1.0); s.set_pmo(0.0)
+    s.fillInitValue(1, 0.9, 1e-6, 1.0, 0.6, 0.5, 0, 0, seed=7)
+    for t in range(100):
+        s.step_rk4()
+    print(s.analysis())
+"""
+import ctypes as C
+import math
+
+import numpy as np
+
+from . import _lib
+from ._lib import (FP32, FP64, KERNEL_AUTO, KERNEL_DIRECT, KERNEL_XMARCH, LAYOUT_COMPACT, LAYOUT_GHOSTED,
+                   REG_COR, REG_PRE, REG_RHS, REG_STAT, FIELDS, NuoscError, check, lib)
+
+__all__ = ["NuOsc", "NuoscError", "FP32", "FP64", "REG_STAT", "REG_RHS", "REG_PRE", "REG_COR",
+           "KERNEL_AUTO", "KERNEL_DIRECT", "KERNEL_XMARCH", "FIELDS", "lib"]
+
+lib()  # fail at import time if the CUDA library is missing
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _ip(seq):
+    arr = (C.c_int * len(seq))(*[int(x) for x in seq])
+    return arr
+
+
+class Grid:
+    """Geometry view (the reference's CartGrid members used by callers)."""
+
+    def __init__(self, g, vx, vy, vz, vw):
+        self.nx, self.nz, self.nv = g.nx, g.nz, g.nv
+        self.nv_stride = g.nv_stride
+        self.gx, self.gz = g.gx, g.gz
+        self.x0, self.x1, self.z0, self.z1 = g.x0, g.x1, g.z0, g.z1
+        self.dx, self.dz = g.dx, g.dz
+        self.vx, self.vy, self.vz, self.vw = vx, vy, vz, vw
+        self.X = g.x0 + (np.arange(g.nx) + 0.5) * g.dx  # CartGrid.cpp:199
+        self.Z = g.z0 + (np.arange(g.nz) + 0.5) * g.dz  # CartGrid.cpp:200
+        self.lpts = (g.nx + 2 * g.gx) * (g.nz + 2 * g.gz) * g.nv  # CartGrid.cpp:208
+
+    def get_lpts(self):
+        return self.lpts
+
+    def idx(self, i, j, v):
+        """Ghosted linear index of the reference (CartGrid.h:91)."""
+        return ((i + self.gx) * (self.nz + 2 * self.gz) + j + self.gz) * self.nv + v
+
+
+class NuOsc:
+    """Drop-in for the reference's NuOsc on one B200 (nuosc_class.h:99-191).
+
+    Constructor arguments are those of NuOsc::NuOsc (nuosc_class.cpp:454):
+    px, pz (must be 1), nv (icosahedron subdivision count), nphi (unused),
+    gx, gz (3: 6th-difference KO; 2: 4th-difference KO), the box x0, x1, z0,
+    z1, spacings dx, dz, CFL and ko.  Extra keywords: precision (FP64 or
+    FP32), device.
+    """
+
+    def __init__(self, px, pz, nv, nphi, gx, gz, x0, x1, z0, z1, dx, dz, CFL, ko, precision=FP64, device=0):
+        p = _lib.Params(px=px, pz=pz, nv=nv, nphi=nphi, gx=gx, gz=gz, x0=x0, x1=x1, z0=z0, z1=z1, dx=dx, dz=dz,
+                        cfl=CFL, ko=ko, precision=precision, device=device)
+        h = C.c_void_p()
+        check(lib().nuosc_create(C.byref(p), C.byref(h)))
+        self._h = h
+        self.CFL, self.ko, self.precision = CFL, ko, precision
+        self.mu, self.pmo, self.renorm = 1.0, 0.1, False  # NuOsc defaults (nuosc_class.h:124-126)
+        g = self._geometry()
+        nv_ = g.nv
+        vx, vy, vz, vw = (np.zeros(nv_) for _ in range(4))
+        check(lib().nuosc_get_velocities(h, _dp(vx), _dp(vy), _dp(vz), _dp(vw)))
+        self.grid = Grid(g, vx, vy, vz, vw)
+        self.dt, self.dx, self.dz, self.ds_L = g.dt, g.dx, g.dz, g.ds_L
+
+    # ------------------------------------------------------------ lifetime
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().nuosc_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    # ------------------------------------------------------------ settings
+    def set_mu(self, mu):
+        self.mu = mu
+        check(lib().nuosc_set_mu(self._h, mu))
+
+    def set_pmo(self, pmo):
+        self.pmo = pmo
+        check(lib().nuosc_set_pmo(self._h, pmo))
+
+    def set_renorm(self, renorm):
+        self.renorm = bool(renorm)
+        check(lib().nuosc_set_renorm(self._h, int(bool(renorm))))
+
+    def set_kernel(self, kind):
+        check(lib().nuosc_set_kernel(self._h, kind))
+
+    def _geometry(self):
+        g = _lib.Geometry()
+        check(lib().nuosc_get_geometry(self._h, C.byref(g)))
+        return g
+
+    @property
+    def phy_time(self):
+        return self._geometry().phy_time
+
+    @phy_time.setter
+    def phy_time(self, t):
+        check(lib().nuosc_set_time(self._h, t))
+
+    @property
+    def n_nue0(self):
+        return tuple(self._geometry().n_nue0)
+
+    @property
+    def device_bytes(self):
+        return self._geometry().device_bytes
+
+    def get_lpts(self):
+        return self.grid.lpts
+
+    def get_nv(self):
+        return self.grid.nv
+
+    @property
+    def G0(self):
+        a, b = np.zeros(self.grid.nv), np.zeros(self.grid.nv)
+        check(lib().nuosc_get_spectra(self._h, _dp(a), _dp(b)))
+        return a
+
+    @property
+    def G0b(self):
+        a, b = np.zeros(self.grid.nv), np.zeros(self.grid.nv)
+        check(lib().nuosc_get_spectra(self._h, _dp(a), _dp(b)))
+        return b
+
+    def set_spectra(self, G0, G0b, n_nue0, n_nueb0):
+        G0 = np.ascontiguousarray(G0, dtype=np.float64)
+        G0b = np.ascontiguousarray(G0b, dtype=np.float64)
+        check(lib().nuosc_set_spectra(self._h, _dp(G0), _dp(G0b), n_nue0, n_nueb0))
+
+    # ------------------------------------------------------------ init / state
+    def fillInitValue(self, ipt, alpha, eps0, sigma, lnue, lnueb, lnuex=0.0, lnuebx=0.0, seed=0):
+        """nuosc_init.cpp:17-137 (generic branch); ipt=1 draws eps0*U(-1,1) per (x,z) from `seed`.
+        lnuex/lnuebx <= 0 (or inf) mean unbounded, the reference default."""
+        lnuex = 0.0 if (lnuex is None or math.isinf(lnuex) or lnuex >= 1e300) else lnuex
+        lnuebx = 0.0 if (lnuebx is None or math.isinf(lnuebx) or lnuebx >= 1e300) else lnuebx
+        check(lib().nuosc_fill_init(self._h, int(ipt), alpha, eps0, sigma, lnue, lnueb, lnuex, lnuebx, int(seed)))
+
+    def get_field(self, field, reg=REG_STAT, layout=LAYOUT_COMPACT):
+        g = self.grid
+        if layout == LAYOUT_COMPACT:
+            out = np.zeros((g.nx, g.nz, g.nv))
+        else:
+            out = np.zeros(g.lpts)
+        check(lib().nuosc_get_state(self._h, reg, field, _dp(out), layout))
+        return out
+
+    def get_state(self, reg=REG_STAT):
+        """All 8 fields of a register as a (8, nx, nz, nv) float64 array."""
+        return np.stack([self.get_field(f, reg) for f in range(8)])
+
+    def set_field(self, field, arr, reg=REG_STAT, layout=LAYOUT_COMPACT):
+        arr = np.ascontiguousarray(arr, dtype=np.float64)
+        check(lib().nuosc_set_state(self._h, reg, field, _dp(arr), layout))
+
+    def set_state(self, arr, reg=REG_STAT):
+        for f in range(8):
+            self.set_field(f, arr[f], reg)
+
+    # ------------------------------------------------------------ hot path
+    def updatePeriodicBoundary(self, reg=REG_STAT):
+        check(lib().nuosc_update_periodic_boundary(self._h, reg))
+
+    def calRHS(self, out=REG_RHS, inp=REG_STAT):
+        check(lib().nuosc_calrhs(self._h, out, inp))
+
+    def vectorize(self, dst, src1, a, src2, src3=None):
+        if src3 is None:
+            check(lib().nuosc_vectorize(self._h, dst, src1, a, src2))
+        else:
+            check(lib().nuosc_vectorize2(self._h, dst, src1, a, src2, src3))
+
+    def step_rk4(self, nsteps=1):
+        check(lib().nuosc_step_rk4(self._h, int(nsteps)))
+
+    def synchronize(self):
+        check(lib().nuosc_synchronize(self._h))
+
+    @property
+    def kernel_launches(self):
+        return lib().nuosc_kernel_launches(self._h)
+
+    def set_profiling(self, on=True):
+        check(lib().nuosc_set_profiling(self._h, int(bool(on))))
+
+    def get_profile(self):
+        """{kind: (total_ms, launches)} since the last call (CUDA events on the handle's stream)."""
+        n = len(_lib.PROF_KINDS)
+        ms = np.zeros(n)
+        cnt = (C.c_longlong * n)()
+        check(lib().nuosc_get_profile(self._h, _dp(ms), cnt, n))
+        return {k: (float(ms[i]), int(cnt[i])) for i, k in enumerate(_lib.PROF_KINDS)}
+
+    # ------------------------------------------------------------ analysis / output
+    def analysis(self):
+        d = _lib.Diag()
+        check(lib().nuosc_analysis(self._h, C.byref(d)))
+        return d.as_dict()
+
+    def open_analysis_file(self, path="analysis.dat"):
+        check(lib().nuosc_open_analysis_file(self._h, path.encode()))
+
+    def addSnapShotAtV(self, var, fntpl, dumpstep, vidx):
+        """var: field ids or names (FIELDS)."""
+        f = [FIELDS.index(v) if isinstance(v, str) else int(v) for v in var]
+        check(lib().nuosc_add_snapshot_at_v(self._h, _ip(f), len(f), fntpl.encode(), dumpstep, _ip(vidx),
+                                            len(vidx)))
+
+    def addSnapShotAtXV(self, var, fntpl, dumpstep, xidx, vidx):
+        f = [FIELDS.index(v) if isinstance(v, str) else int(v) for v in var]
+        check(lib().nuosc_add_snapshot_at_xv(self._h, _ip(f), len(f), fntpl.encode(), dumpstep, _ip(xidx),
+                                             len(xidx), _ip(vidx), len(vidx)))
+
+    def checkSnapShot(self, t=0):
+        check(lib().nuosc_check_snapshot(self._h, int(t)))
+
+    def gather(self, field, xidx, vidx):
+        f = FIELDS.index(field) if isinstance(field, str) else int(field)
+        out = np.zeros((len(xidx), self.grid.nz, len(vidx)))
+        check(lib().nuosc_gather(self._h, f, _ip(xidx), len(xidx), _ip(vidx), len(vidx), _dp(out)))
+        return out

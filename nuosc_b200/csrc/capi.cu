@@ -1,0 +1,898 @@
+// capi.cu -- the C ABI of include/nuosc_b200.h: handle, device memory,
+// stage sequencing of step_rk4, analysis and snapshot I/O.
+//
+// Register roles inside step_rk4 (classic RK4 of nuosc_class.cpp:374-427,
+// rearranged so each stage is one fused pass):
+//   U = v_stat, A = v_rhs (accumulator), Ya = v_pre, Yb = v_cor
+//   S1: k1 = L(U)  ; A = U + dt/6 k1 ; Ya = U + dt/2 k1
+//   S2: k2 = L(Ya) ; A = A + dt/3 k2 ; Yb = U + dt/2 k2
+//   S3: k3 = L(Yb) ; A = A + dt/3 k3 ; Ya = U + dt   k3
+//   S4: k4 = L(Ya) ; U = A + dt/6 k4
+// which is U + dt/6 (k1 + 2k2 + 2k3 + k4), the reference's update, with
+// 16 state passes per step instead of the reference's 4 calRHS + 6 vectorize.
+#include "../../include/nuosc_b200.h"
+#include "internal.cuh"
+
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <iomanip>
+#include <list>
+#include <string>
+#include <vector>
+
+namespace nuosc {
+void icosahedron(int nn, std::vector<double> &vx, std::vector<double> &vy, std::vector<double> &vz,
+                 std::vector<double> &vw);
+int icosahedron_count(int nn);
+XTile autotune_lookup(int nv, int precision);
+}  // namespace nuosc
+
+using namespace nuosc;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+#define CUDA_TRY(expr)                                                                                    \
+    do {                                                                                                  \
+        cudaError_t e_ = (expr);                                                                          \
+        if (e_ != cudaSuccess) return fail(NUOSC_ERR_CUDA, "%s: %s (%s:%d)", #expr, cudaGetErrorString(e_), \
+                                           __FILE__, __LINE__);                                           \
+    } while (0)
+
+struct Snapshot {
+    std::vector<int> fields;
+    std::string fntpl;
+    int every;
+    std::vector<int> xidx, vidx;
+};
+
+}  // namespace
+
+struct nuosc_handle {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int precision = NUOSC_FP64;
+    size_t esize = 8;
+    int gx = 3, gz = 3;
+    bool ko6 = true;
+    Geom g{};
+    double x0 = 0, x1 = 0, z0 = 0, z1 = 0, dx = 0, dz = 0, cfl = 0, ko = 0;
+    double dt = 0, ds_L = 0, phy_time = 0;
+    double mu = 1.0, pmo = 0.1;  // NuOsc's defaults (nuosc_class.h:124-125)
+    bool renorm = false;
+    double n_nue0[2] = {0, 0};
+    int kernel = NUOSC_KERNEL_AUTO;
+    XTile tile{16, 64, 32};
+    long long launches = 0;
+    bool mom_valid = false;  // d_mom holds the moments of v_stat
+
+    std::vector<double> vx, vy, vz, vw, G0, G0b;  // host copies (length nv)
+    void *reg[4] = {nullptr, nullptr, nullptr, nullptr};
+    double *d_quad = nullptr;  // vx | vy | vz | vw | G0 | G0b, each nvs
+    double *d_mom = nullptr;   // [ncell][12]
+    double *d_part = nullptr;  // x-march partial moments
+    size_t part_bytes = 0;
+    double *d_ana = nullptr;   // analysis partials + final
+    double *h_ana = nullptr;   // pinned
+    int *d_status = nullptr;
+    double *d_stage = nullptr; // host-layout staging
+    size_t stage_bytes = 0;
+    int *d_idx = nullptr;      // snapshot index staging
+    size_t idx_cap = 0;
+    double *d_gather = nullptr;
+    size_t gather_bytes = 0;
+    size_t device_bytes = 0;
+
+    std::ofstream anafile;
+    std::list<Snapshot> snapshots;
+
+    // event-pair profiling of the step kernels (nuosc_set_profiling)
+    bool prof_on = false;
+    std::vector<cudaEvent_t> ev_pool;
+    std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev_pending;
+    double prof_ms[NUOSC_PROF_KINDS] = {0};
+    long long prof_n[NUOSC_PROF_KINDS] = {0};
+
+    cudaEvent_t take_event() {
+        if (ev_pool.empty()) {
+            cudaEvent_t e;
+            cudaEventCreate(&e);
+            return e;
+        }
+        cudaEvent_t e = ev_pool.back();
+        ev_pool.pop_back();
+        return e;
+    }
+    // record a begin event; returns the pending slot (or -1 when profiling is off)
+    int prof_begin(int kind) {
+        if (!prof_on) return -1;
+        cudaEvent_t a = take_event(), b = take_event();
+        cudaEventRecord(a, stream);
+        ev_pending.push_back({kind, {a, b}});
+        return (int)ev_pending.size() - 1;
+    }
+    void prof_end(int slot) {
+        if (slot >= 0) cudaEventRecord(ev_pending[slot].second.second, stream);
+    }
+    void prof_collect() {
+        for (auto &p : ev_pending) {
+            float ms = 0;
+            cudaEventSynchronize(p.second.second);
+            cudaEventElapsedTime(&ms, p.second.first, p.second.second);
+            prof_ms[p.first] += ms;
+            prof_n[p.first] += 1;
+            ev_pool.push_back(p.second.first);
+            ev_pool.push_back(p.second.second);
+        }
+        ev_pending.clear();
+    }
+
+    Quad quad() const {
+        const int s = g.nvs;
+        return Quad{d_quad, d_quad + s, d_quad + 2 * s, d_quad + 3 * s};
+    }
+    const double *dG0() const { return d_quad + 4 * g.nvs; }
+    const double *dG0b() const { return d_quad + 5 * g.nvs; }
+    Coeffs coeffs() const {
+        Coeffs c;
+        c.fxs = -1.0 / (12 * dx);
+        c.fzs = -1.0 / (12 * dz);
+        c.kx = ko6 ? -ko / dx / 64.0 : -ko / dx / 16.0;
+        c.kz = ko6 ? -ko / dz / 64.0 : -ko / dz / 16.0;
+        const double theta = 37 * M_PI / 180.;  // nuosc_class.h:120
+        c.ct = std::cos(2 * theta);
+        c.st = std::sin(2 * theta);
+        c.mu = mu;
+        c.pmo = pmo;
+        return c;
+    }
+};
+
+namespace {
+
+bool valid_reg(int r) { return r >= 0 && r < 4; }
+
+int ensure(void **p, size_t *cap, size_t bytes, nuosc_handle *h) {
+    if (*cap >= bytes) return 0;
+    if (*p) {
+        cudaFree(*p);
+        h->device_bytes -= *cap;
+    }
+    *p = nullptr;
+    *cap = 0;
+    CUDA_TRY(cudaMalloc(p, bytes));
+    *cap = bytes;
+    h->device_bytes += bytes;
+    return 0;
+}
+
+int prof_kind(int mode) {
+    switch (mode) {
+    case MODE_S1: return 0;
+    case MODE_S23: return 1;
+    case MODE_S4: return 2;
+    default: return 3;
+    }
+}
+
+// one RK4 stage in the direct path: moments of `in`, then the fused stencil
+template <typename T>
+int run_stage_direct(nuosc_handle *h, int mode, int in, int u, int acc_src, int acc_dst, int y_dst, double cA,
+                     double cY) {
+    StageArgs<T> a{};
+    a.in = (const T *)h->reg[in];
+    a.u = u >= 0 ? (const T *)h->reg[u] : nullptr;
+    a.acc_src = acc_src >= 0 ? (const T *)h->reg[acc_src] : nullptr;
+    a.acc_dst = (T *)h->reg[acc_dst];
+    a.y_dst = y_dst >= 0 ? (T *)h->reg[y_dst] : nullptr;
+    a.mom_in = h->d_mom;
+    a.q = h->quad();
+    a.g = h->g;
+    a.c = h->coeffs();
+    a.cA = cA;
+    a.cY = cY;
+    a.status = h->d_status;
+    if (!(mode == MODE_S1 && in == NUOSC_REG_STAT && h->mom_valid)) {
+        const int ps = h->prof_begin(4);
+        CUDA_TRY(launch_moments<T>((const T *)h->reg[in], h->d_mom, a.q, h->g, h->stream));
+        h->prof_end(ps);
+        h->launches++;
+    }
+    const int ps = h->prof_begin(prof_kind(mode));
+    CUDA_TRY(launch_stage_direct<T>(a, mode, h->ko6, h->stream));
+    h->prof_end(ps);
+    h->launches++;
+    return 0;
+}
+
+// one RK4 stage in the x-march path (moments of the stage output fused)
+template <typename T>
+int run_stage_xmarch(nuosc_handle *h, int mode, int in, int u, int acc_src, int acc_dst, int y_dst, double cA,
+                     double cY) {
+    StageArgs<T> a{};
+    a.in = (const T *)h->reg[in];
+    a.u = u >= 0 ? (const T *)h->reg[u] : nullptr;
+    a.acc_src = acc_src >= 0 ? (const T *)h->reg[acc_src] : nullptr;
+    a.acc_dst = (T *)h->reg[acc_dst];
+    a.y_dst = y_dst >= 0 ? (T *)h->reg[y_dst] : nullptr;
+    a.mom_in = h->d_mom;
+    a.mom_part = h->d_part;
+    a.q = h->quad();
+    a.g = h->g;
+    a.c = h->coeffs();
+    a.cA = cA;
+    a.cY = cY;
+    a.status = h->d_status;
+    if (!h->mom_valid) {
+        const int ps = h->prof_begin(4);
+        CUDA_TRY(launch_moments<T>((const T *)h->reg[in], h->d_mom, a.q, h->g, h->stream));
+        h->prof_end(ps);
+        h->launches++;
+    }
+    int ps = h->prof_begin(prof_kind(mode));
+    CUDA_TRY(launch_stage_xmarch<T>(a, mode, h->ko6, h->tile, h->stream));
+    h->prof_end(ps);
+    ps = h->prof_begin(5);
+    CUDA_TRY(launch_moment_finalize(h->d_part, h->d_mom, h->g, xmarch_num_vblocks(h->g, h->tile), h->stream));
+    h->prof_end(ps);
+    h->launches += 2;
+    h->mom_valid = true;  // d_mom now holds the moments of the register this stage wrote
+    return 0;
+}
+
+template <typename T>
+bool use_xmarch(nuosc_handle *h) {
+    if (h->kernel == NUOSC_KERNEL_DIRECT) return false;
+    return xmarch_supported<T>(h->g, h->ko6, h->tile);
+}
+
+template <typename T>
+int step_impl(nuosc_handle *h, int nsteps) {
+    const double dt = h->dt;
+    const bool xm = use_xmarch<T>(h);
+    if (h->kernel == NUOSC_KERNEL_XMARCH && !xm)
+        return fail(NUOSC_ERR_UNSUPPORTED, "x-march kernel does not support this geometry");
+    if (xm) {
+        const size_t need = (size_t)h->g.ncell * xmarch_num_vblocks(h->g, h->tile) * 2 * NMOM * sizeof(double);
+        if (int rc = ensure((void **)&h->d_part, &h->part_bytes, need, h)) return rc;
+    }
+    for (int n = 0; n < nsteps; ++n) {
+        int rc;
+        if (xm) {
+            if ((rc = run_stage_xmarch<T>(h, MODE_S1, 0, -1, -1, 1, 2, dt / 6.0, 0.5 * dt))) return rc;
+            if ((rc = run_stage_xmarch<T>(h, MODE_S23, 2, 0, 1, 1, 3, dt / 3.0, 0.5 * dt))) return rc;
+            if ((rc = run_stage_xmarch<T>(h, MODE_S23, 3, 0, 1, 1, 2, dt / 3.0, dt))) return rc;
+            if ((rc = run_stage_xmarch<T>(h, MODE_S4, 2, -1, 1, 0, -1, dt / 6.0, 0.0))) return rc;
+        } else {
+            if ((rc = run_stage_direct<T>(h, MODE_S1, 0, -1, -1, 1, 2, dt / 6.0, 0.5 * dt))) return rc;
+            h->mom_valid = false;
+            if ((rc = run_stage_direct<T>(h, MODE_S23, 2, 0, 1, 1, 3, dt / 3.0, 0.5 * dt))) return rc;
+            if ((rc = run_stage_direct<T>(h, MODE_S23, 3, 0, 1, 1, 2, dt / 3.0, dt))) return rc;
+            if ((rc = run_stage_direct<T>(h, MODE_S4, 2, -1, 1, 0, -1, dt / 6.0, 0.0))) return rc;
+        }
+        if (h->renorm) {
+            CUDA_TRY(launch_renormalize<T>((T *)h->reg[0], h->dG0(), h->dG0b(), h->g, h->stream));
+            h->launches++;
+            h->mom_valid = false;
+        }
+        h->phy_time += dt;
+    }
+    return 0;
+}
+
+template <typename T>
+int calrhs_impl(nuosc_handle *h, int out, int in) {
+    h->mom_valid = false;
+    int rc = run_stage_direct<T>(h, MODE_RHS, in, -1, -1, out, -1, 1.0, 0.0);
+    h->mom_valid = false;
+    return rc;
+}
+
+int check_status(nuosc_handle *h) {
+    int st = 0;
+    CUDA_TRY(cudaMemcpyAsync(&st, h->d_status, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    if (st != 0) {
+        CUDA_TRY(cudaMemsetAsync(h->d_status, 0, sizeof(int), h->stream));
+        return fail(NUOSC_ERR_TIMEOUT, "a bounded in-kernel wait expired (status %d)", st);
+    }
+    return 0;
+}
+
+// host spectra G0/G0b (nuosc_init.cpp:74-96)
+void compute_spectra(nuosc_handle *h, double alpha, double lnue, double lnueb, double lnuex, double lnuebx) {
+    if (lnuex <= 0) lnuex = DBL_MAX;
+    if (lnuebx <= 0) lnuebx = DBL_MAX;
+    const int nv = h->g.nv;
+    std::vector<double> ng(nv), ngb(nv);
+    double ing0 = 0, ing1 = 0;
+    for (int v = 0; v < nv; ++v) {
+        ng[v] = std::exp(-(h->vx[v] - 1.0) * (h->vx[v] - 1.0) / (2.0 * lnuex * lnuex) -
+                         (h->vz[v] - 1.0) * (h->vz[v] - 1.0) / (2.0 * lnue * lnue));
+        ngb[v] = std::exp(-(h->vx[v] - 1.0) * (h->vx[v] - 1.0) / (2.0 * lnuebx * lnuebx) -
+                          (h->vz[v] - 1.0) * (h->vz[v] - 1.0) / (2.0 * lnueb * lnueb));
+        ing0 += h->vw[v] * ng[v];
+        ing1 += h->vw[v] * ngb[v];
+    }
+    ing0 = 1.0 / ing0;
+    ing1 = 1.0 / ing1;
+    h->G0.resize(nv);
+    h->G0b.resize(nv);
+    for (int v = 0; v < nv; ++v) {
+        h->G0[v] = ng[v] * ing0;
+        h->G0b[v] = alpha * ngb[v] * ing1;
+    }
+}
+
+int upload_spectra(nuosc_handle *h) {
+    const int s = h->g.nvs;
+    CUDA_TRY(cudaMemsetAsync(h->d_quad + 4 * s, 0, 2 * s * sizeof(double), h->stream));
+    CUDA_TRY(cudaMemcpyAsync(h->d_quad + 4 * s, h->G0.data(), h->g.nv * sizeof(double), cudaMemcpyHostToDevice,
+                             h->stream));
+    CUDA_TRY(cudaMemcpyAsync(h->d_quad + 5 * s, h->G0b.data(), h->g.nv * sizeof(double), cudaMemcpyHostToDevice,
+                             h->stream));
+    return 0;
+}
+
+template <typename T>
+int analysis_raw(nuosc_handle *h, double *q) {
+    CUDA_TRY(launch_analysis<T>((const T *)h->reg[0], h->dG0(), h->dG0b(), h->quad().vw, h->g, h->d_ana,
+                                h->d_ana + ANA_BLOCKS * ANA_NQ, h->stream));
+    CUDA_TRY(cudaMemcpyAsync(h->h_ana, h->d_ana + ANA_BLOCKS * ANA_NQ, ANA_NQ * sizeof(double),
+                             cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    memcpy(q, h->h_ana, ANA_NQ * sizeof(double));
+    return 0;
+}
+
+int analysis_dispatch(nuosc_handle *h, double *q) {
+    return h->precision == NUOSC_FP64 ? analysis_raw<double>(h, q) : analysis_raw<float>(h, q);
+}
+
+bool host_layout_ok(int layout) { return layout == NUOSC_LAYOUT_COMPACT || layout == NUOSC_LAYOUT_GHOSTED; }
+size_t host_field_elems(const nuosc_handle *h, int layout) {
+    if (layout == NUOSC_LAYOUT_COMPACT) return (size_t)h->g.ncell * h->g.nv;
+    return (size_t)(h->g.nx + 2 * h->gx) * (h->g.nz + 2 * h->gz) * h->g.nv;
+}
+
+template <typename T>
+int set_state_impl(nuosc_handle *h, int reg, int field, const double *host, int layout) {
+    T *dst = (T *)h->reg[reg] + (size_t)field * h->g.fs;
+    const size_t n = host_field_elems(h, layout);
+    if (sizeof(T) == 8 && layout == NUOSC_LAYOUT_COMPACT && h->g.nvs == h->g.nv) {
+        CUDA_TRY(cudaMemcpyAsync(dst, host, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    } else {
+        if (int rc = ensure((void **)&h->d_stage, &h->stage_bytes, n * sizeof(double), h)) return rc;
+        CUDA_TRY(cudaMemcpyAsync(h->d_stage, host, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+        CUDA_TRY(launch_import<T>(dst, h->d_stage, h->g, layout, h->gx, h->gz, h->stream));
+    }
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return 0;
+}
+
+template <typename T>
+int get_state_impl(nuosc_handle *h, int reg, int field, double *host, int layout) {
+    const T *src = (const T *)h->reg[reg] + (size_t)field * h->g.fs;
+    const size_t n = host_field_elems(h, layout);
+    if (sizeof(T) == 8 && layout == NUOSC_LAYOUT_COMPACT && h->g.nvs == h->g.nv) {
+        CUDA_TRY(cudaMemcpyAsync(host, src, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    } else {
+        if (int rc = ensure((void **)&h->d_stage, &h->stage_bytes, n * sizeof(double), h)) return rc;
+        if (layout == NUOSC_LAYOUT_GHOSTED) {
+            // ghost entries are copied back as they were given (zeros for a fresh buffer)
+            CUDA_TRY(cudaMemcpyAsync(h->d_stage, host, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+        }
+        CUDA_TRY(launch_export<T>(src, h->d_stage, h->g, layout, h->gx, h->gz, h->stream));
+        CUDA_TRY(cudaMemcpyAsync(host, h->d_stage, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    }
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return 0;
+}
+
+int write_meta(nuosc_handle *h, const Snapshot &s, bool at_xv) {
+    char filename[4096];
+    std::string tmp = s.fntpl + ".meta";
+    snprintf(filename, sizeof filename, tmp.c_str(), 0);
+    std::ofstream out(filename, std::ofstream::out | std::ofstream::trunc);
+    if (!out) return fail(NUOSC_ERR_INVALID, "cannot open %s", filename);
+    // text layout of addSnapShotAtV / addSnapShotAtXV (nuosc_snapshot.cpp:31-39, 64-72)
+    const int sx = (int)s.xidx.size(), sv = (int)s.vidx.size();
+    out << h->dt << " " << sx << " " << h->g.nz << " " << sv << std::endl;
+    out << h->x0 << " " << h->x1 << std::endl;
+    out << h->z0 << " " << h->z1 << std::endl;
+    if (at_xv) {
+        for (int j = 0; j < h->g.nz; ++j) out << h->z0 + (j + 0.5) * h->dz << " ";
+        out << std::endl;
+        for (int x : s.xidx) out << h->x0 + (x + 0.5) * h->dx << " ";
+        out << std::endl;
+    } else {
+        for (int i = 0; i < h->g.nx; ++i) out << h->x0 + (i + 0.5) * h->dx << " ";
+        out << std::endl;
+        for (int j = 0; j < h->g.nz; ++j) out << h->z0 + (j + 0.5) * h->dz << " ";
+        out << std::endl;
+    }
+    for (int v : s.vidx) out << h->vx[v] << " ";
+    out << std::endl;
+    for (int v : s.vidx) out << h->vy[v] << " ";
+    out << std::endl;
+    for (int v : s.vidx) out << h->vz[v] << " ";
+    out << std::endl;
+    return 0;
+}
+
+template <typename T>
+int gather_impl(nuosc_handle *h, int field, const int *xidx, int sx, const int *vidx, int sv, double *host) {
+    const size_t nidx = (size_t)sx + sv;
+    if (int rc = ensure((void **)&h->d_idx, &h->idx_cap, nidx * sizeof(int), h)) return rc;
+    const size_t n = (size_t)sx * h->g.nz * sv;
+    if (int rc = ensure((void **)&h->d_gather, &h->gather_bytes, n * sizeof(double), h)) return rc;
+    CUDA_TRY(cudaMemcpyAsync(h->d_idx, xidx, sx * sizeof(int), cudaMemcpyHostToDevice, h->stream));
+    CUDA_TRY(cudaMemcpyAsync(h->d_idx + sx, vidx, sv * sizeof(int), cudaMemcpyHostToDevice, h->stream));
+    CUDA_TRY(launch_gather<T>((const T *)h->reg[0], field, h->d_idx, sx, h->d_idx + sx, sv, h->dG0(), h->dG0b(),
+                              h->g, h->d_gather, h->stream));
+    CUDA_TRY(cudaMemcpyAsync(host, h->d_gather, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return 0;
+}
+
+int gather_dispatch(nuosc_handle *h, int field, const int *xidx, int sx, const int *vidx, int sv, double *host) {
+    return h->precision == NUOSC_FP64 ? gather_impl<double>(h, field, xidx, sx, vidx, sv, host)
+                                      : gather_impl<float>(h, field, xidx, sx, vidx, sv, host);
+}
+
+int check_indices(const nuosc_handle *h, const int *fields, int nfields, const int *xidx, int nx_, const int *vidx,
+                  int nv_) {
+    if (nfields <= 0 || !fields) return fail(NUOSC_ERR_INVALID, "no fields");
+    for (int k = 0; k < nfields; ++k)
+        if (fields[k] < 0 || fields[k] > 15) return fail(NUOSC_ERR_INVALID, "field id %d out of range", fields[k]);
+    for (int k = 0; k < nx_; ++k)
+        if (xidx[k] < 0 || xidx[k] >= h->g.nx) return fail(NUOSC_ERR_INVALID, "x index %d out of range", xidx[k]);
+    if (nv_ <= 0 || !vidx) return fail(NUOSC_ERR_INVALID, "no velocity indices");
+    for (int k = 0; k < nv_; ++k)
+        if (vidx[k] < 0 || vidx[k] >= h->g.nv) return fail(NUOSC_ERR_INVALID, "v index %d out of range", vidx[k]);
+    return 0;
+}
+
+#define HANDLE_CHECK(h)                                                           \
+    do {                                                                          \
+        if (!(h)) return fail(NUOSC_ERR_INVALID, "null handle");                  \
+        cudaError_t e_ = cudaSetDevice((h)->device);                              \
+        if (e_ != cudaSuccess) return fail(NUOSC_ERR_CUDA, "cudaSetDevice: %s", cudaGetErrorString(e_)); \
+    } while (0)
+
+#define DISPATCH(h, fn, ...) ((h)->precision == NUOSC_FP64 ? fn<double>(__VA_ARGS__) : fn<float>(__VA_ARGS__))
+
+}  // namespace
+
+extern "C" {
+
+const char *nuosc_last_error(void) { return g_err.c_str(); }
+
+int nuosc_velocity_quadrature(int nn, double *vx, double *vy, double *vz, double *vw, int *n_out) {
+    if (nn < 1 || nn > 64) return fail(NUOSC_ERR_INVALID, "icosahedron subdivision nn=%d out of range", nn);
+    std::vector<double> x, y, z, w;
+    icosahedron(nn, x, y, z, w);
+    const size_t n = x.size() * sizeof(double);
+    if (vx) memcpy(vx, x.data(), n);
+    if (vy) memcpy(vy, y.data(), n);
+    if (vz) memcpy(vz, z.data(), n);
+    if (vw) memcpy(vw, w.data(), n);
+    if (n_out) *n_out = (int)x.size();
+    return NUOSC_OK;
+}
+
+int nuosc_create(const nuosc_params *p, nuosc_handle **out) {
+    g_err.clear();
+    if (!p || !out) return fail(NUOSC_ERR_INVALID, "null argument");
+    *out = nullptr;
+    if (p->px != 1 || p->pz != 1)
+        return fail(NUOSC_ERR_UNSUPPORTED, "px=%d pz=%d: one solve lives on one GPU (px = pz = 1)", p->px, p->pz);
+    if (p->nv < 1 || p->nv > 64) return fail(NUOSC_ERR_INVALID, "icosahedron subdivision nv=%d out of range", p->nv);
+    if (p->gx != p->gz || (p->gx != 2 && p->gx != 3))
+        return fail(NUOSC_ERR_INVALID, "ghost width gx=%d gz=%d: must be equal and 2 or 3", p->gx, p->gz);
+    if (!(p->dx > 0) || !(p->dz > 0) || !(p->x1 > p->x0) || !(p->z1 > p->z0))
+        return fail(NUOSC_ERR_INVALID, "bad box or spacing");
+    if (p->precision != NUOSC_FP64 && p->precision != NUOSC_FP32)
+        return fail(NUOSC_ERR_INVALID, "precision %d", p->precision);
+    nuosc_handle *h = new nuosc_handle;
+    h->device = p->device;
+    h->precision = p->precision;
+    h->esize = p->precision == NUOSC_FP64 ? 8 : 4;
+    h->gx = p->gx;
+    h->gz = p->gz;
+    h->ko6 = p->gx == 3;
+    h->x0 = p->x0; h->x1 = p->x1; h->z0 = p->z0; h->z1 = p->z1;
+    h->dx = p->dx; h->dz = p->dz; h->cfl = p->cfl; h->ko = p->ko;
+    const int nx = (int)((p->x1 - p->x0) / p->dx), nz = (int)((p->z1 - p->z0) / p->dz);
+    if (nx < 4 || nz < 4) {
+        delete h;
+        return fail(NUOSC_ERR_INVALID, "grid %dx%d too small (need at least 4x4)", nx, nz);
+    }
+    h->dt = p->dz * p->cfl;
+    h->ds_L = p->dx * p->dz / (p->z1 - p->z0) / (p->x1 - p->x0);
+    icosahedron(p->nv, h->vx, h->vy, h->vz, h->vw);
+    const int nv = (int)h->vx.size();
+    const int align = (int)(16 / h->esize);
+    const int nvs = (nv + align - 1) / align * align;
+    h->g.nx = nx;
+    h->g.nz = nz;
+    h->g.nv = nv;
+    h->g.nvs = nvs;
+    h->g.ncell = (long long)nx * nz;
+    h->g.fs = h->g.ncell * nvs;
+    h->tile = autotune_lookup(nv, h->precision);
+
+    auto bail = [&](int rc) {
+        nuosc_destroy(h);
+        return rc;
+    };
+    cudaError_t e = cudaSetDevice(h->device);
+    if (e != cudaSuccess) return bail(fail(NUOSC_ERR_CUDA, "cudaSetDevice(%d): %s", h->device, cudaGetErrorString(e)));
+    e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return bail(fail(NUOSC_ERR_CUDA, "cudaStreamCreate: %s", cudaGetErrorString(e)));
+    const size_t reg_bytes = (size_t)h->g.fs * NF * h->esize;
+    size_t free_b = 0, total_b = 0;
+    cudaMemGetInfo(&free_b, &total_b);
+    const size_t need = 4 * reg_bytes + (size_t)h->g.ncell * NMOM * 8;
+    if (need > free_b)
+        return bail(fail(NUOSC_ERR_OOM, "need %.2f GB for 4 state registers, %.2f GB free", need / 1e9, free_b / 1e9));
+    for (int r = 0; r < 4; ++r) {
+        e = cudaMalloc(&h->reg[r], reg_bytes);
+        if (e != cudaSuccess) return bail(fail(NUOSC_ERR_OOM, "cudaMalloc register %d (%.2f GB): %s", r, reg_bytes / 1e9,
+                                               cudaGetErrorString(e)));
+        h->device_bytes += reg_bytes;
+        cudaMemsetAsync(h->reg[r], 0, reg_bytes, h->stream);
+    }
+    const size_t small = 6 * (size_t)nvs * sizeof(double) + (size_t)h->g.ncell * NMOM * sizeof(double) +
+                         (ANA_BLOCKS + 1) * ANA_NQ * sizeof(double) + 256;
+    char *blk = nullptr;
+    e = cudaMalloc(&blk, small);
+    if (e != cudaSuccess) return bail(fail(NUOSC_ERR_OOM, "cudaMalloc work buffers: %s", cudaGetErrorString(e)));
+    h->device_bytes += small;
+    cudaMemsetAsync(blk, 0, small, h->stream);
+    h->d_status = (int *)blk;
+    h->d_quad = (double *)(blk + 256);
+    h->d_mom = h->d_quad + 6 * nvs;
+    h->d_ana = h->d_mom + h->g.ncell * NMOM;
+    e = cudaMallocHost(&h->h_ana, ANA_NQ * sizeof(double));
+    if (e != cudaSuccess) return bail(fail(NUOSC_ERR_CUDA, "cudaMallocHost: %s", cudaGetErrorString(e)));
+    cudaMemcpyAsync(h->d_quad, h->vx.data(), nv * 8, cudaMemcpyHostToDevice, h->stream);
+    cudaMemcpyAsync(h->d_quad + nvs, h->vy.data(), nv * 8, cudaMemcpyHostToDevice, h->stream);
+    cudaMemcpyAsync(h->d_quad + 2 * nvs, h->vz.data(), nv * 8, cudaMemcpyHostToDevice, h->stream);
+    cudaMemcpyAsync(h->d_quad + 3 * nvs, h->vw.data(), nv * 8, cudaMemcpyHostToDevice, h->stream);
+    h->G0.assign(nv, 0.0);
+    h->G0b.assign(nv, 0.0);
+    e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) return bail(fail(NUOSC_ERR_CUDA, "create: %s", cudaGetErrorString(e)));
+    *out = h;
+    return NUOSC_OK;
+}
+
+int nuosc_destroy(nuosc_handle *h) {
+    if (!h) return NUOSC_OK;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    h->prof_collect();
+    for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
+    for (int r = 0; r < 4; ++r)
+        if (h->reg[r]) cudaFree(h->reg[r]);
+    if (h->d_status) cudaFree(h->d_status);
+    if (h->d_part) cudaFree(h->d_part);
+    if (h->d_stage) cudaFree(h->d_stage);
+    if (h->d_idx) cudaFree(h->d_idx);
+    if (h->d_gather) cudaFree(h->d_gather);
+    if (h->h_ana) cudaFreeHost(h->h_ana);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    if (h->anafile.is_open()) h->anafile.close();
+    delete h;
+    return NUOSC_OK;
+}
+
+int nuosc_set_mu(nuosc_handle *h, double mu) {
+    if (!h) return fail(NUOSC_ERR_INVALID, "null handle");
+    h->mu = mu;
+    return NUOSC_OK;
+}
+int nuosc_set_pmo(nuosc_handle *h, double pmo) {
+    if (!h) return fail(NUOSC_ERR_INVALID, "null handle");
+    h->pmo = pmo;
+    return NUOSC_OK;
+}
+int nuosc_set_renorm(nuosc_handle *h, int renorm) {
+    if (!h) return fail(NUOSC_ERR_INVALID, "null handle");
+    h->renorm = renorm != 0;
+    return NUOSC_OK;
+}
+int nuosc_set_kernel(nuosc_handle *h, int kind) {
+    if (!h) return fail(NUOSC_ERR_INVALID, "null handle");
+    if (kind < NUOSC_KERNEL_AUTO || kind > NUOSC_KERNEL_XMARCH) return fail(NUOSC_ERR_INVALID, "kernel kind %d", kind);
+    h->kernel = kind;
+    h->mom_valid = false;
+    return NUOSC_OK;
+}
+int nuosc_set_time(nuosc_handle *h, double t) {
+    if (!h) return fail(NUOSC_ERR_INVALID, "null handle");
+    h->phy_time = t;
+    return NUOSC_OK;
+}
+
+int nuosc_get_geometry(const nuosc_handle *h, nuosc_geometry *o) {
+    if (!h || !o) return fail(NUOSC_ERR_INVALID, "null argument");
+    o->nx = h->g.nx; o->nz = h->g.nz; o->nv = h->g.nv; o->nv_stride = h->g.nvs;
+    o->gx = h->gx; o->gz = h->gz; o->precision = h->precision;
+    o->dt = h->dt; o->ds_L = h->ds_L; o->phy_time = h->phy_time;
+    o->x0 = h->x0; o->x1 = h->x1; o->z0 = h->z0; o->z1 = h->z1; o->dx = h->dx; o->dz = h->dz;
+    o->n_nue0[0] = h->n_nue0[0]; o->n_nue0[1] = h->n_nue0[1];
+    o->device_bytes = h->device_bytes;
+    return NUOSC_OK;
+}
+
+int nuosc_get_velocities(const nuosc_handle *h, double *vx, double *vy, double *vz, double *vw) {
+    if (!h) return fail(NUOSC_ERR_INVALID, "null handle");
+    const size_t n = h->vx.size() * sizeof(double);
+    if (vx) memcpy(vx, h->vx.data(), n);
+    if (vy) memcpy(vy, h->vy.data(), n);
+    if (vz) memcpy(vz, h->vz.data(), n);
+    if (vw) memcpy(vw, h->vw.data(), n);
+    return NUOSC_OK;
+}
+
+int nuosc_get_spectra(const nuosc_handle *h, double *G0, double *G0b) {
+    if (!h) return fail(NUOSC_ERR_INVALID, "null handle");
+    if (G0) memcpy(G0, h->G0.data(), h->G0.size() * sizeof(double));
+    if (G0b) memcpy(G0b, h->G0b.data(), h->G0b.size() * sizeof(double));
+    return NUOSC_OK;
+}
+
+int nuosc_set_spectra(nuosc_handle *h, const double *G0, const double *G0b, double n0, double n1) {
+    HANDLE_CHECK(h);
+    if (!G0 || !G0b) return fail(NUOSC_ERR_INVALID, "null spectra");
+    h->G0.assign(G0, G0 + h->g.nv);
+    h->G0b.assign(G0b, G0b + h->g.nv);
+    h->n_nue0[0] = n0;
+    h->n_nue0[1] = n1;
+    if (int rc = upload_spectra(h)) return rc;
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return NUOSC_OK;
+}
+
+int nuosc_fill_init(nuosc_handle *h, int ipt, double alpha, double eps0, double sigma, double lnue, double lnueb,
+                    double lnuex, double lnuebx, uint64_t seed) {
+    HANDLE_CHECK(h);
+    if (ipt < 0 || ipt > 3)
+        return fail(NUOSC_ERR_UNSUPPORTED, "ipt=%d: supported initial data are ipt 0..3", ipt);
+    compute_spectra(h, alpha, lnue, lnueb, lnuex, lnuebx);
+    if (int rc = upload_spectra(h)) return rc;
+    if (h->precision == NUOSC_FP64)
+        CUDA_TRY(launch_init<double>((double *)h->reg[0], h->dG0(), h->dG0b(), h->g, ipt, eps0, sigma, h->z0, h->dz,
+                                     seed, h->stream));
+    else
+        CUDA_TRY(launch_init<float>((float *)h->reg[0], h->dG0(), h->dG0b(), h->g, ipt, eps0, sigma, h->z0, h->dz,
+                                    seed, h->stream));
+    h->mom_valid = false;
+    h->phy_time = 0.0;
+    double q[ANA_NQ];
+    if (int rc = analysis_dispatch(h, q)) return rc;
+    h->n_nue0[0] = q[1] * h->ds_L;  // nuosc_init.cpp:116-130
+    h->n_nue0[1] = q[2] * h->ds_L;
+    return NUOSC_OK;
+}
+
+int nuosc_set_state(nuosc_handle *h, int reg, int field, const double *host, int layout) {
+    HANDLE_CHECK(h);
+    if (!valid_reg(reg) || field < 0 || field >= NF || !host || !host_layout_ok(layout))
+        return fail(NUOSC_ERR_INVALID, "set_state: bad register/field/layout");
+    if (reg == NUOSC_REG_STAT) h->mom_valid = false;
+    return DISPATCH(h, set_state_impl, h, reg, field, host, layout);
+}
+
+int nuosc_get_state(nuosc_handle *h, int reg, int field, double *host, int layout) {
+    HANDLE_CHECK(h);
+    if (!valid_reg(reg) || field < 0 || field >= NF || !host || !host_layout_ok(layout))
+        return fail(NUOSC_ERR_INVALID, "get_state: bad register/field/layout");
+    return DISPATCH(h, get_state_impl, h, reg, field, host, layout);
+}
+
+int nuosc_update_periodic_boundary(nuosc_handle *h, int reg) {
+    if (!h) return fail(NUOSC_ERR_INVALID, "null handle");
+    if (!valid_reg(reg)) return fail(NUOSC_ERR_INVALID, "register %d", reg);
+    return NUOSC_OK;
+}
+
+int nuosc_calrhs(nuosc_handle *h, int out, int in) {
+    HANDLE_CHECK(h);
+    if (!valid_reg(out) || !valid_reg(in) || out == in)
+        return fail(NUOSC_ERR_INVALID, "calrhs: registers must be distinct and in 0..3");
+    int rc = DISPATCH(h, calrhs_impl, h, out, in);
+    if (rc) return rc;
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return NUOSC_OK;
+}
+
+int nuosc_vectorize(nuosc_handle *h, int dst, int src1, double a, int src2) {
+    HANDLE_CHECK(h);
+    if (!valid_reg(dst) || !valid_reg(src1) || !valid_reg(src2)) return fail(NUOSC_ERR_INVALID, "vectorize: register");
+    if (h->precision == NUOSC_FP64)
+        CUDA_TRY(launch_vectorize<double>((double *)h->reg[dst], (const double *)h->reg[src1], a,
+                                          (const double *)h->reg[src2], nullptr, h->g, h->stream));
+    else
+        CUDA_TRY(launch_vectorize<float>((float *)h->reg[dst], (const float *)h->reg[src1], a,
+                                         (const float *)h->reg[src2], nullptr, h->g, h->stream));
+    if (dst == NUOSC_REG_STAT) h->mom_valid = false;
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return NUOSC_OK;
+}
+
+int nuosc_vectorize2(nuosc_handle *h, int dst, int src1, double a, int src2, int src3) {
+    HANDLE_CHECK(h);
+    if (!valid_reg(dst) || !valid_reg(src1) || !valid_reg(src2) || !valid_reg(src3))
+        return fail(NUOSC_ERR_INVALID, "vectorize2: register");
+    if (h->precision == NUOSC_FP64)
+        CUDA_TRY(launch_vectorize<double>((double *)h->reg[dst], (const double *)h->reg[src1], a,
+                                          (const double *)h->reg[src2], (const double *)h->reg[src3], h->g,
+                                          h->stream));
+    else
+        CUDA_TRY(launch_vectorize<float>((float *)h->reg[dst], (const float *)h->reg[src1], a,
+                                         (const float *)h->reg[src2], (const float *)h->reg[src3], h->g, h->stream));
+    if (dst == NUOSC_REG_STAT) h->mom_valid = false;
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return NUOSC_OK;
+}
+
+int nuosc_step_rk4(nuosc_handle *h, int nsteps) {
+    HANDLE_CHECK(h);
+    if (nsteps < 0) return fail(NUOSC_ERR_INVALID, "nsteps %d", nsteps);
+    int rc = DISPATCH(h, step_impl, h, nsteps);
+    if (rc) return rc;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(NUOSC_ERR_CUDA, "step_rk4: %s", cudaGetErrorString(e));
+    return NUOSC_OK;
+}
+
+int nuosc_analysis(nuosc_handle *h, nuosc_diag *o) {
+    HANDLE_CHECK(h);
+    if (int rc = check_status(h)) return rc;
+    double q[ANA_NQ];
+    if (int rc = analysis_dispatch(h, q)) return rc;
+    // nuosc_ana.cpp:110-117
+    nuosc_diag d;
+    d.phy_time = h->phy_time;
+    d.maxdP = q[0];
+    d.surv = q[1] / q[8];
+    d.survb = q[2] / q[9];
+    d.avgP = q[3] / q[8];
+    d.avgPb = q[4] / q[9];
+    d.aM0 = std::sqrt(q[5] * q[5] + q[6] * q[6] + q[7] * q[7]) * h->ds_L;
+    d.Lex = q[7] * h->ds_L;
+    d.ELNe = std::fabs(h->n_nue0[0] * (1.0 - d.surv) - h->n_nue0[1] * (1.0 - d.survb)) / (h->n_nue0[0] + h->n_nue0[1]);
+    d.nonfinite = (long long)q[10];
+    if (o) *o = d;
+    if (h->anafile.is_open()) {
+        // nuosc_ana.cpp:126-129 (precision 13 sticks after the first record)
+        h->anafile << d.phy_time << std::setprecision(13) << " " << d.maxdP << " " << d.surv << " " << d.survb << " "
+                   << d.avgP << " " << d.avgPb << " " << d.aM0 << " " << d.Lex << " " << d.ELNe << " " << std::endl;
+    }
+    if (d.nonfinite > 0 || !(d.maxdP < 10))
+        return fail(NUOSC_ERR_NUMERIC, "state blew up: max||P|-1| = %g, %lld non-finite values", d.maxdP, d.nonfinite);
+    return NUOSC_OK;
+}
+
+int nuosc_open_analysis_file(nuosc_handle *h, const char *path) {
+    if (!h || !path) return fail(NUOSC_ERR_INVALID, "null argument");
+    if (h->anafile.is_open()) h->anafile.close();
+    h->anafile.open(path, std::ofstream::out | std::ofstream::trunc);
+    if (!h->anafile) return fail(NUOSC_ERR_INVALID, "cannot open %s", path);
+    h->anafile << "### [ phy_time,   1:maxrelP,    2:surv, survb,    4:avgP, avgPb,      6:aM0    7:Lem   8:ELNe]"
+               << std::endl;
+    return NUOSC_OK;
+}
+
+int nuosc_add_snapshot_at_v(nuosc_handle *h, const int *fields, int nfields, const char *fntpl, int every,
+                            const int *vidx, int n_vidx) {
+    if (!h || !fntpl) return fail(NUOSC_ERR_INVALID, "null argument");
+    if (int rc = check_indices(h, fields, nfields, nullptr, 0, vidx, n_vidx)) return rc;
+    Snapshot s;
+    s.fields.assign(fields, fields + nfields);
+    s.fntpl = fntpl;
+    s.every = every;
+    for (int i = 0; i < h->g.nx; ++i) s.xidx.push_back(i);
+    s.vidx.assign(vidx, vidx + n_vidx);
+    if (int rc = write_meta(h, s, false)) return rc;
+    h->snapshots.push_back(s);
+    return NUOSC_OK;
+}
+
+int nuosc_add_snapshot_at_xv(nuosc_handle *h, const int *fields, int nfields, const char *fntpl, int every,
+                             const int *xidx, int n_xidx, const int *vidx, int n_vidx) {
+    if (!h || !fntpl) return fail(NUOSC_ERR_INVALID, "null argument");
+    if (n_xidx <= 0 || !xidx) return fail(NUOSC_ERR_INVALID, "no x indices");
+    if (int rc = check_indices(h, fields, nfields, xidx, n_xidx, vidx, n_vidx)) return rc;
+    Snapshot s;
+    s.fields.assign(fields, fields + nfields);
+    s.fntpl = fntpl;
+    s.every = every;
+    s.xidx.assign(xidx, xidx + n_xidx);
+    s.vidx.assign(vidx, vidx + n_vidx);
+    if (int rc = write_meta(h, s, true)) return rc;
+    h->snapshots.push_back(s);
+    return NUOSC_OK;
+}
+
+int nuosc_check_snapshot(nuosc_handle *h, int t) {
+    HANDLE_CHECK(h);
+    // like the reference, every registered snapshot is written on each call
+    // (the `every` test is commented out at nuosc_snapshot.cpp:89)
+    for (const Snapshot &s : h->snapshots) {
+        char filename[4096];
+        snprintf(filename, sizeof filename, s.fntpl.c_str(), t);
+        std::ofstream out(filename, std::ofstream::out | std::ofstream::trunc | std::ofstream::binary);
+        if (!out) return fail(NUOSC_ERR_INVALID, "cannot open %s", filename);
+        const unsigned tt = (unsigned)t;
+        out.write((const char *)&tt, sizeof(unsigned));
+        out.write((const char *)&h->phy_time, sizeof(double));
+        std::vector<double> buf((size_t)s.xidx.size() * h->g.nz * s.vidx.size());
+        for (int f : s.fields) {
+            if (int rc = gather_dispatch(h, f, s.xidx.data(), (int)s.xidx.size(), s.vidx.data(), (int)s.vidx.size(),
+                                         buf.data()))
+                return rc;
+            out.write((const char *)buf.data(), buf.size() * sizeof(double));
+        }
+    }
+    return NUOSC_OK;
+}
+
+int nuosc_gather(nuosc_handle *h, int field, const int *xidx, int n_xidx, const int *vidx, int n_vidx, double *host) {
+    HANDLE_CHECK(h);
+    if (!host || n_xidx <= 0 || !xidx) return fail(NUOSC_ERR_INVALID, "gather: bad arguments");
+    if (int rc = check_indices(h, &field, 1, xidx, n_xidx, vidx, n_vidx)) return rc;
+    return gather_dispatch(h, field, xidx, n_xidx, vidx, n_vidx, host);
+}
+
+int nuosc_synchronize(nuosc_handle *h) {
+    HANDLE_CHECK(h);
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return check_status(h);
+}
+
+void *nuosc_stream(nuosc_handle *h) { return h ? (void *)h->stream : nullptr; }
+
+long long nuosc_kernel_launches(const nuosc_handle *h) { return h ? h->launches : 0; }
+
+int nuosc_set_profiling(nuosc_handle *h, int on) {
+    HANDLE_CHECK(h);
+    h->prof_collect();
+    h->prof_on = on != 0;
+    return NUOSC_OK;
+}
+
+int nuosc_get_profile(nuosc_handle *h, double *ms, long long *launches, int nkinds) {
+    HANDLE_CHECK(h);
+    h->prof_collect();
+    for (int k = 0; k < nkinds && k < NUOSC_PROF_KINDS; ++k) {
+        if (ms) ms[k] = h->prof_ms[k];
+        if (launches) launches[k] = h->prof_n[k];
+    }
+    for (int k = 0; k < NUOSC_PROF_KINDS; ++k) {
+        h->prof_ms[k] = 0;
+        h->prof_n[k] = 0;
+    }
+    return NUOSC_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,100 @@
+// internal.cuh -- device-side data layout, kernel argument blocks and launch
+// entry points shared by the CUDA kernels and the C-ABI host layer.
+//
+// HBM layout of one register (a FieldVar of the reference): 8 fields, each
+// [x][z][v] with the velocity innermost and `nvs` velocities per (x,z) row
+// (nv rounded up so every row starts on a 16-byte boundary).  No ghost cells
+// are stored: the stencils wrap x and z periodically in-kernel, which is what
+// updatePeriodicBoundary's ghost fill amounts to for the plus-shaped stencil
+// (nuosc_boundary.cpp:4-52).  Padding velocities carry zero weight, zero
+// velocity and zero state, so every kernel may process them and they stay 0.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace nuosc {
+
+constexpr int NF = 8;  // ee, mm, emr, emi, bee, bmm, bemr, bemi
+constexpr int NMOM = 12;  // emRm[4], emIp[4], eemm[4] (nuosc_class.cpp:28-31)
+
+struct Geom {
+    int nx, nz, nv, nvs;
+    long long fs;     // elements per field = nx*nz*nvs
+    long long ncell;  // nx*nz
+};
+
+// Physics coefficients of calRHS (nuosc_class.cpp:112-183, nuosc_class.h:120-122).
+struct Coeffs {
+    double fxs, fzs;  // advection: factor_x = vx * fxs, fxs = -1/(12 dx) (same for z)
+    double kx, kz;    // KO strength: -ko/dx/64 (6th difference) or -ko/dx/16 (4th)
+    double mu, pmo, ct, st;
+};
+
+struct Quad {
+    const double *vx, *vy, *vz, *vw;  // [nvs], zero in the padding
+};
+
+// One RK stage: k = L(in); then, by mode,
+//   MODE_RHS : acc_dst = k
+//   MODE_S1  : acc_dst = in + cA*k ;          y_dst = in + cY*k
+//   MODE_S23 : acc_dst = acc_src + cA*k ;     y_dst = u  + cY*k
+//   MODE_S4  : acc_dst = acc_src + cA*k
+enum StageMode { MODE_RHS = 0, MODE_S1 = 1, MODE_S23 = 2, MODE_S4 = 3 };
+
+template <typename T>
+struct StageArgs {
+    const T *in;
+    const T *u;
+    const T *acc_src;
+    T *acc_dst;
+    T *y_dst;
+    const double *mom_in;  // [ncell][12] moments of `in`
+    double *mom_part;      // x-march: per-(cell, v-block, half) partial moments of the new state
+    Quad q;
+    Geom g;
+    Coeffs c;
+    double cA, cY;
+    int *status;           // device status word (bounded waits)
+};
+
+// ---------------------------------------------------------------- launches
+template <typename T>
+cudaError_t launch_moments(const T *reg, double *mom, Quad q, Geom g, cudaStream_t s);
+template <typename T>
+cudaError_t launch_stage_direct(const StageArgs<T> &a, int mode, bool ko6, cudaStream_t s);
+
+// x-march kernel: tile shape chosen by the autotuner (tile.cu)
+struct XTile {
+    int tz;      // z rows per CTA
+    int lx;      // x planes marched per CTA
+    int vb;      // velocities per CTA (32)
+};
+template <typename T>
+bool xmarch_supported(const Geom &g, bool ko6, XTile t);
+template <typename T>
+cudaError_t launch_stage_xmarch(const StageArgs<T> &a, int mode, bool ko6, XTile t, cudaStream_t s);
+int xmarch_num_vblocks(const Geom &g, XTile t);
+cudaError_t launch_moment_finalize(const double *part, double *mom, Geom g, int nvb, cudaStream_t s);
+
+template <typename T>
+cudaError_t launch_init(T *reg, const double *G0, const double *G0b, Geom g, int ipt, double eps0,
+                        double sigma, double z0, double dz, uint64_t seed, cudaStream_t s);
+// Analysis partial sums; `part` holds ANA_BLOCKS * ANA_NQ doubles, `out` ANA_NQ.
+constexpr int ANA_NQ = 12;
+constexpr int ANA_BLOCKS = 296;
+template <typename T>
+cudaError_t launch_analysis(const T *reg, const double *G0, const double *G0b, const double *vw, Geom g,
+                            double *part, double *out, cudaStream_t s);
+template <typename T>
+cudaError_t launch_gather(const T *reg, int field, const int *xidx, int sx, const int *vidx, int sv,
+                          const double *G0, const double *G0b, Geom g, double *out, cudaStream_t s);
+template <typename T>
+cudaError_t launch_import(T *reg_field, const double *src, Geom g, int layout, int gx, int gz, cudaStream_t s);
+template <typename T>
+cudaError_t launch_export(const T *reg_field, double *dst, Geom g, int layout, int gx, int gz, cudaStream_t s);
+template <typename T>
+cudaError_t launch_vectorize(T *dst, const T *a, double c, const T *b, const T *d, Geom g, cudaStream_t s);
+template <typename T>
+cudaError_t launch_renormalize(T *reg, const double *G0, const double *G0b, Geom g, cudaStream_t s);
+
+}  // namespace nuosc

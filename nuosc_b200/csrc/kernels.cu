@@ -1,0 +1,441 @@
+// kernels.cu -- direct stage kernel, velocity moments, and the auxiliary
+// kernels (seeded initial data, analysis reduction, snapshot gather, layout
+// conversion, vectorize, renormalize).  All are HBM-bound streaming kernels.
+#include "internal.cuh"
+#include "physics.cuh"
+
+namespace nuosc {
+
+// ----------------------------------------------------------------------------
+// Velocity moments of one register (nuosc_class.cpp:62-82): one warp per
+// (x,z) cell, lanes stride over v, FP64 accumulation, butterfly warp
+// reduction (fixed order, so the result is deterministic).
+// ----------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(256) k_moments(const T *__restrict__ in, double *__restrict__ mom, Quad q, Geom g) {
+    const int lane = threadIdx.x & 31;
+    const long long cell = (long long)blockIdx.x * 8 + (threadIdx.x >> 5);
+    if (cell >= g.ncell) return;
+    double m[NMOM];
+#pragma unroll
+    for (int k = 0; k < NMOM; ++k) m[k] = 0.0;
+    const T *row = in + cell * g.nvs;
+    for (int v = lane; v < g.nv; v += 32) {
+        const double ee = row[v], mm = row[v + g.fs], emr = row[v + 2 * g.fs], emi = row[v + 3 * g.fs];
+        const double bee = row[v + 4 * g.fs], bmm = row[v + 5 * g.fs], bemr = row[v + 6 * g.fs],
+                     bemi = row[v + 7 * g.fs];
+        const double w = q.vw[v];
+        const double v4[4] = {1.0, q.vx[v], q.vy[v], q.vz[v]};
+        const double d0 = bemr - emr, d1 = bemi + emi, d2 = bee - bmm - ee + mm;
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+            const double vw4 = v4[s] * w;
+            m[s] += vw4 * d0;
+            m[4 + s] += vw4 * d1;
+            m[8 + s] += vw4 * d2;
+        }
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1)
+#pragma unroll
+        for (int k = 0; k < NMOM; ++k) m[k] += __shfl_xor_sync(0xffffffffu, m[k], off);
+    if (lane == 0) {
+#pragma unroll
+        for (int k = 0; k < NMOM; ++k) mom[cell * NMOM + k] = m[k];
+    }
+}
+
+template <typename T>
+cudaError_t launch_moments(const T *reg, double *mom, Quad q, Geom g, cudaStream_t s) {
+    const long long blocks = (g.ncell + 7) / 8;
+    k_moments<T><<<(unsigned)blocks, 256, 0, s>>>(reg, mom, q, g);
+    return cudaGetLastError();
+}
+
+// ----------------------------------------------------------------------------
+// Direct stage kernel: one thread per (cell, velocity), all 8 fields, the
+// 13-point (KO6) or 9-point (KO4) plus-shaped stencil read through the
+// read-only cache with periodic wrap, fused RK-stage epilogue.  Used for
+// calRHS, for geometries the x-march kernel does not cover, and as the
+// simple reference path on the device.
+// ----------------------------------------------------------------------------
+template <typename T, bool KO6, int MODE>
+__global__ void __launch_bounds__(256) k_stage_direct(StageArgs<T> a) {
+    const Geom g = a.g;
+    const int v = blockIdx.x * 32 + threadIdx.x;
+    const long long cell = (long long)blockIdx.y * 8 + threadIdx.y;
+    if (cell >= g.ncell || v >= g.nvs) return;
+    const int i = (int)(cell / g.nz), j = (int)(cell - (long long)i * g.nz);
+    constexpr int R = KO6 ? 3 : 2;
+    long long oz[7], ox[7];
+#pragma unroll
+    for (int k = -3; k <= 3; ++k) {
+        const int kk = (k < -R || k > R) ? 0 : k;
+        oz[k + 3] = ((long long)i * g.nz + wrap_index(j + kk, g.nz)) * g.nvs + v;
+        ox[k + 3] = ((long long)wrap_index(i + kk, g.nx) * g.nz + j) * g.nvs + v;
+    }
+    const double vxd = a.q.vx[v], vyd = a.q.vy[v], vzd = a.q.vz[v];
+    const T fx = T(vxd * a.c.fxs), fz = T(vzd * a.c.fzs);
+    const T kx = T(a.c.kx), kz = T(a.c.kz);
+    const double *m = a.mom_in + cell * NMOM;
+    const T ia = T(inp(m, vxd, vyd, vzd)), ib = T(inp(m + 4, vxd, vyd, vzd)), ie = T(inp(m + 8, vxd, vyd, vzd));
+
+    T cen[NF], adv[NF], ko[NF];
+#pragma unroll
+    for (int f = 0; f < NF; ++f) {
+        const T *F = a.in + f * g.fs;
+        T zs[7], xs[7];
+#pragma unroll
+        for (int k = 0; k < 7; ++k) {
+            zs[k] = __ldg(F + oz[k]);
+            xs[k] = __ldg(F + ox[k]);
+        }
+        cen[f] = zs[3];
+        adv[f] = adv_axis(zs, fz) + adv_axis(xs, fx);
+        ko[f] = ko_axis<T, KO6>(zs, kz) + ko_axis<T, KO6>(xs, kx);
+    }
+    T k[NF];
+    {
+        T c4[4] = {cen[0], cen[1], cen[2], cen[3]}, a4[4] = {adv[0], adv[1], adv[2], adv[3]},
+          k4[4] = {ko[0], ko[1], ko[2], ko[3]}, o4[4];
+        commutator_half(c4, ia, ib, ie, a.c, o4, a4, k4);
+#pragma unroll
+        for (int f = 0; f < 4; ++f) k[f] = o4[f];
+    }
+    {
+        T c4[4] = {cen[4], cen[5], cen[6], cen[7]}, a4[4] = {adv[4], adv[5], adv[6], adv[7]},
+          k4[4] = {ko[4], ko[5], ko[6], ko[7]}, o4[4];
+        commutator_half(c4, ia, ib, ie, a.c, o4, a4, k4);
+#pragma unroll
+        for (int f = 0; f < 4; ++f) k[4 + f] = o4[f];
+    }
+    const long long o = oz[3];
+    const T cA = T(a.cA), cY = T(a.cY);
+#pragma unroll
+    for (int f = 0; f < NF; ++f) {
+        const long long idx = o + f * g.fs;
+        if (MODE == MODE_RHS) {
+            a.acc_dst[idx] = k[f];
+        } else if (MODE == MODE_S1) {
+            a.acc_dst[idx] = cen[f] + cA * k[f];
+            a.y_dst[idx] = cen[f] + cY * k[f];
+        } else if (MODE == MODE_S23) {
+            a.acc_dst[idx] = a.acc_src[idx] + cA * k[f];
+            a.y_dst[idx] = a.u[idx] + cY * k[f];
+        } else {
+            a.acc_dst[idx] = a.acc_src[idx] + cA * k[f];
+        }
+    }
+}
+
+template <typename T, bool KO6>
+static cudaError_t launch_direct_ko(const StageArgs<T> &a, int mode, cudaStream_t s) {
+    dim3 block(32, 8);
+    dim3 grid((a.g.nvs + 31) / 32, (unsigned)((a.g.ncell + 7) / 8));
+    switch (mode) {
+    case MODE_RHS: k_stage_direct<T, KO6, MODE_RHS><<<grid, block, 0, s>>>(a); break;
+    case MODE_S1: k_stage_direct<T, KO6, MODE_S1><<<grid, block, 0, s>>>(a); break;
+    case MODE_S23: k_stage_direct<T, KO6, MODE_S23><<<grid, block, 0, s>>>(a); break;
+    default: k_stage_direct<T, KO6, MODE_S4><<<grid, block, 0, s>>>(a); break;
+    }
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_stage_direct(const StageArgs<T> &a, int mode, bool ko6, cudaStream_t s) {
+    return ko6 ? launch_direct_ko<T, true>(a, mode, s) : launch_direct_ko<T, false>(a, mode, s);
+}
+
+// ----------------------------------------------------------------------------
+// Seeded initial data (nuosc_init.cpp:70-127), one thread per (cell, v).
+// The perturbation of cell (i,j) is a counter-based hash of (seed, i, j), so
+// it is independent of the launch shape and identical to the host oracle's.
+// ----------------------------------------------------------------------------
+__device__ __forceinline__ uint64_t mix64(uint64_t z) {
+    z += 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+template <typename T>
+__global__ void k_init(T *reg, const double *G0, const double *G0b, Geom g, int ipt, double eps0, double sigma,
+                       double z0, double dz, uint64_t seed) {
+    const int v = blockIdx.x * 32 + threadIdx.x;
+    const long long cell = (long long)blockIdx.y * 8 + threadIdx.y;
+    if (cell >= g.ncell || v >= g.nvs) return;
+    const int i = (int)(cell / g.nz), j = (int)(cell - (long long)i * g.nz);
+    const long long o = cell * g.nvs + v;
+    if (v >= g.nv) {
+#pragma unroll
+        for (int f = 0; f < NF; ++f) reg[o + f * g.fs] = T(0);
+        return;
+    }
+    const double Zj = __dadd_rn(z0, __dmul_rn(j + 0.5, dz));
+    double t;
+    if (ipt == 0) {
+        t = eps0 * exp(-Zj * Zj / (2.0 * sigma * sigma));
+    } else if (ipt == 1) {
+        const uint64_t key = ((uint64_t)(uint32_t)i << 32) | (uint64_t)(uint32_t)j;
+        const double u = (double)(mix64(mix64(seed) ^ key) >> 11) * 0x1.0p-53;
+        t = __dmul_rn(eps0, __dadd_rn(__dmul_rn(2.0, u), -1.0));
+    } else if (ipt == 2) {
+        t = eps0 * (1.0 + cos(2 * 3.14159265358979323846 * Zj / (2.0 * sigma * sigma))) * 0.5;
+    } else {
+        t = eps0;
+    }
+    const double p3o = __dsqrt_rn(__dadd_rn(1.0, -__dmul_rn(t, t)));
+    const double G = G0[v], Gb = G0b[v];
+    const double hG = __dmul_rn(0.5, G), hGb = __dmul_rn(0.5, Gb);
+    reg[o + 0 * g.fs] = T(__dmul_rn(hG, __dadd_rn(1.0, p3o)));
+    reg[o + 1 * g.fs] = T(__dmul_rn(hG, __dadd_rn(1.0, -p3o)));
+    reg[o + 2 * g.fs] = T(__dmul_rn(hG, t));
+    reg[o + 3 * g.fs] = T(0);
+    reg[o + 4 * g.fs] = T(__dmul_rn(hGb, __dadd_rn(1.0, p3o)));
+    reg[o + 5 * g.fs] = T(__dmul_rn(hGb, __dadd_rn(1.0, -p3o)));
+    reg[o + 6 * g.fs] = T(__dmul_rn(hGb, t));
+    reg[o + 7 * g.fs] = T(0);
+}
+
+template <typename T>
+cudaError_t launch_init(T *reg, const double *G0, const double *G0b, Geom g, int ipt, double eps0, double sigma,
+                        double z0, double dz, uint64_t seed, cudaStream_t s) {
+    dim3 block(32, 8);
+    dim3 grid((g.nvs + 31) / 32, (unsigned)((g.ncell + 7) / 8));
+    k_init<T><<<grid, block, 0, s>>>(reg, G0, G0b, g, ipt, eps0, sigma, z0, dz, seed);
+    return cudaGetLastError();
+}
+
+// ----------------------------------------------------------------------------
+// analysis() reduction (nuosc_ana.cpp:34-137) in FP64 without the reference's
+// ten full-size temporaries: each block reduces a fixed, strided set of cells
+// to ANA_NQ partials; a one-block pass sums the partials in block order.
+// Quantities: 0 maxdP, 1 sum w ee, 2 sum w bee, 3 sum w G dP, 4 sum w Gb dPb,
+// 5..7 aM01..aM03, 8 sum w G, 9 sum w Gb, 10 non-finite count.
+// ----------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(256) k_analysis(const T *__restrict__ st, const double *__restrict__ G0,
+                                                  const double *__restrict__ G0b, const double *__restrict__ vw,
+                                                  Geom g, double *__restrict__ part) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    double q[ANA_NQ];
+#pragma unroll
+    for (int k = 0; k < ANA_NQ; ++k) q[k] = 0.0;
+    for (long long cell = (long long)blockIdx.x * 8 + warp; cell < g.ncell; cell += (long long)gridDim.x * 8) {
+        const T *row = st + cell * g.nvs;
+        for (int v = lane; v < g.nv; v += 32) {
+            const double ee = row[v], mm = row[v + g.fs], emr = row[v + 2 * g.fs], emi = row[v + 3 * g.fs];
+            const double bee = row[v + 4 * g.fs], bmm = row[v + 5 * g.fs], bemr = row[v + 6 * g.fs],
+                         bemi = row[v + 7 * g.fs];
+            const double G = G0[v], Gb = G0b[v], w = vw[v];
+            const double iG = 1.0 / G, iGb = 1.0 / Gb;
+            const double P1 = 2.0 * emr * iG, P2 = -2.0 * emi * iG, P3 = (ee - mm) * iG;
+            const double P1b = 2.0 * bemr * iGb, P2b = 2.0 * bemi * iGb, P3b = (bee - bmm) * iGb;
+            const double dP = fabs(1.0 - sqrt(P1 * P1 + P2 * P2 + P3 * P3));
+            const double dPb = fabs(1.0 - sqrt(P1b * P1b + P2b * P2b + P3b * P3b));
+            q[0] = fmax(q[0], fmax(dP, dPb));
+            q[1] += w * ee;
+            q[2] += w * bee;
+            q[3] += w * G * dP;
+            q[4] += w * Gb * dPb;
+            q[5] += w * (emr - bemr);
+            q[6] += w * (-emi - bemi);
+            q[7] += w * 0.5 * (ee - mm - bee + bmm);
+            q[8] += w * G;
+            q[9] += w * Gb;
+            const double chk = ee + mm + emr + emi + bee + bmm + bemr + bemi;
+            if (!isfinite(chk)) q[10] += 1.0;
+        }
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        q[0] = fmax(q[0], __shfl_xor_sync(0xffffffffu, q[0], off));
+#pragma unroll
+        for (int k = 1; k < ANA_NQ; ++k) q[k] += __shfl_xor_sync(0xffffffffu, q[k], off);
+    }
+    __shared__ double sm[8][ANA_NQ];
+    if (lane == 0)
+#pragma unroll
+        for (int k = 0; k < ANA_NQ; ++k) sm[warp][k] = q[k];
+    __syncthreads();
+    if (threadIdx.x < ANA_NQ) {
+        const int k = threadIdx.x;
+        double r = sm[0][k];
+        for (int w = 1; w < 8; ++w) r = (k == 0) ? fmax(r, sm[w][k]) : r + sm[w][k];
+        part[blockIdx.x * ANA_NQ + k] = r;
+    }
+}
+
+__global__ void k_analysis_final(const double *__restrict__ part, int nblocks, double *__restrict__ out) {
+    const int k = threadIdx.x;
+    if (k >= ANA_NQ) return;
+    double r = part[k];
+    for (int b = 1; b < nblocks; ++b) r = (k == 0) ? fmax(r, part[b * ANA_NQ + k]) : r + part[b * ANA_NQ + k];
+    out[k] = r;
+}
+
+template <typename T>
+cudaError_t launch_analysis(const T *reg, const double *G0, const double *G0b, const double *vw, Geom g,
+                            double *part, double *out, cudaStream_t s) {
+    k_analysis<T><<<ANA_BLOCKS, 256, 0, s>>>(reg, G0, G0b, vw, g, part);
+    k_analysis_final<<<1, 32, 0, s>>>(part, ANA_BLOCKS, out);
+    return cudaGetLastError();
+}
+
+// ----------------------------------------------------------------------------
+// Snapshot gather (nuosc_snapshot.cpp:82-122): out[(ii*nz + j)*sv + vv] =
+// field(xidx[ii], j, vidx[vv]); fields 8..15 are the eval_conserved derived
+// quantities (nuosc_ana.cpp:8-28) of the current state.
+// ----------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ double derived_value(const T *st, long long o, long long fs, int field, double G,
+                                                double Gb) {
+    if (field < 8) return (double)st[o + field * fs];
+    const double ee = st[o], mm = st[o + fs], emr = st[o + 2 * fs], emi = st[o + 3 * fs];
+    const double bee = st[o + 4 * fs], bmm = st[o + 5 * fs], bemr = st[o + 6 * fs], bemi = st[o + 7 * fs];
+    const double iG = 1.0 / G, iGb = 1.0 / Gb;
+    const double P1 = 2.0 * emr * iG, P2 = -2.0 * emi * iG, P3 = (ee - mm) * iG;
+    const double P1b = 2.0 * bemr * iGb, P2b = 2.0 * bemi * iGb, P3b = (bee - bmm) * iGb;
+    switch (field) {
+    case 8: return P1;
+    case 9: return P2;
+    case 10: return P3;
+    case 11: return P1b;
+    case 12: return P2b;
+    case 13: return P3b;
+    case 14: return fabs(1.0 - sqrt(P1 * P1 + P2 * P2 + P3 * P3));
+    default: return fabs(1.0 - sqrt(P1b * P1b + P2b * P2b + P3b * P3b));
+    }
+}
+
+template <typename T>
+__global__ void k_gather(const T *st, int field, const int *xidx, int sx, const int *vidx, int sv, const double *G0,
+                         const double *G0b, Geom g, double *out) {
+    const long long n = (long long)sx * g.nz * sv;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const int vv = (int)(t % sv);
+        const long long r = t / sv;
+        const int j = (int)(r % g.nz), ii = (int)(r / g.nz);
+        const int v = vidx[vv], i = xidx[ii];
+        const long long o = ((long long)i * g.nz + j) * g.nvs + v;
+        out[t] = derived_value(st, o, g.fs, field, G0[v], G0b[v]);
+    }
+}
+
+template <typename T>
+cudaError_t launch_gather(const T *reg, int field, const int *xidx, int sx, const int *vidx, int sv,
+                          const double *G0, const double *G0b, Geom g, double *out, cudaStream_t s) {
+    const long long n = (long long)sx * g.nz * sv;
+    const unsigned blocks = (unsigned)((n + 255) / 256 < 148 * 16 ? (n + 255) / 256 : 148 * 16);
+    k_gather<T><<<blocks > 0 ? blocks : 1, 256, 0, s>>>(reg, field, xidx, sx, vidx, sv, G0, G0b, g, out);
+    return cudaGetLastError();
+}
+
+// ----------------------------------------------------------------------------
+// Host-layout conversion of one field: compact [x][z][v] or the reference's
+// ghosted array ((i+gx)(nz+2gz) + j+gz) nv + v  <->  device [x][z][nvs] in T.
+// ----------------------------------------------------------------------------
+__device__ __forceinline__ long long host_index(int layout, int i, int j, int v, const Geom &g, int gx, int gz) {
+    if (layout == 0) return ((long long)i * g.nz + j) * g.nv + v;
+    return ((long long)(i + gx) * (g.nz + 2 * gz) + j + gz) * g.nv + v;
+}
+
+template <typename T>
+__global__ void k_import(T *dst, const double *src, Geom g, int layout, int gx, int gz) {
+    const int v = blockIdx.x * 32 + threadIdx.x;
+    const long long cell = (long long)blockIdx.y * 8 + threadIdx.y;
+    if (cell >= g.ncell || v >= g.nvs) return;
+    const int i = (int)(cell / g.nz), j = (int)(cell - (long long)i * g.nz);
+    dst[cell * g.nvs + v] = v < g.nv ? T(src[host_index(layout, i, j, v, g, gx, gz)]) : T(0);
+}
+template <typename T>
+__global__ void k_export(const T *src, double *dst, Geom g, int layout, int gx, int gz) {
+    const int v = blockIdx.x * 32 + threadIdx.x;
+    const long long cell = (long long)blockIdx.y * 8 + threadIdx.y;
+    if (cell >= g.ncell || v >= g.nv) return;
+    const int i = (int)(cell / g.nz), j = (int)(cell - (long long)i * g.nz);
+    dst[host_index(layout, i, j, v, g, gx, gz)] = (double)src[cell * g.nvs + v];
+}
+
+template <typename T>
+cudaError_t launch_import(T *reg_field, const double *src, Geom g, int layout, int gx, int gz, cudaStream_t s) {
+    dim3 block(32, 8), grid((g.nvs + 31) / 32, (unsigned)((g.ncell + 7) / 8));
+    k_import<T><<<grid, block, 0, s>>>(reg_field, src, g, layout, gx, gz);
+    return cudaGetLastError();
+}
+template <typename T>
+cudaError_t launch_export(const T *reg_field, double *dst, Geom g, int layout, int gx, int gz, cudaStream_t s) {
+    dim3 block(32, 8), grid((g.nvs + 31) / 32, (unsigned)((g.ncell + 7) / 8));
+    k_export<T><<<grid, block, 0, s>>>(reg_field, dst, g, layout, gx, gz);
+    return cudaGetLastError();
+}
+
+// ----------------------------------------------------------------------------
+// vectorize (nuosc_class.cpp:313-351): dst = a + c*b, or dst = a + c*(b + d)
+// over all 8 fields of a register (element-wise, padding included).
+// ----------------------------------------------------------------------------
+template <typename T>
+__global__ void k_vectorize(T *dst, const T *a, T c, const T *b, const T *d, long long n) {
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+        dst[t] = d ? a[t] + c * (b[t] + d[t]) : a[t] + c * b[t];
+}
+template <typename T>
+cudaError_t launch_vectorize(T *dst, const T *a, double c, const T *b, const T *d, Geom g, cudaStream_t s) {
+    k_vectorize<T><<<148 * 8, 256, 0, s>>>(dst, a, T(c), b, d, g.fs * NF);
+    return cudaGetLastError();
+}
+
+// ----------------------------------------------------------------------------
+// renormalize (nuosc_ana.cpp:140-166), kept exactly as the reference writes it
+// (including its ee = G0 + tmp convention) so set_renorm(1) behaves the same.
+// ----------------------------------------------------------------------------
+template <typename T>
+__global__ void k_renormalize(T *st, const double *G0, const double *G0b, Geom g) {
+    const int v = blockIdx.x * 32 + threadIdx.x;
+    const long long cell = (long long)blockIdx.y * 8 + threadIdx.y;
+    if (cell >= g.ncell || v >= g.nv) return;
+    const long long o = cell * g.nvs + v, fs = g.fs;
+    const double G = G0[v], Gb = G0b[v];
+    const double iG = 1.0 / G, iGb = 1.0 / Gb;
+    const double ee = st[o], mm = st[o + fs], emr = st[o + 2 * fs], emi = st[o + 3 * fs];
+    const double bee = st[o + 4 * fs], bmm = st[o + 5 * fs], bemr = st[o + 6 * fs], bemi = st[o + 7 * fs];
+    const double P1 = emr * iG, P2 = -emi * iG, P3 = (ee - mm) * iG;
+    const double P1b = bemr * iGb, P2b = bemi * iGb, P3b = (bee - bmm) * iGb;
+    const double iP = 1.0 / sqrt(P1 * P1 + P2 * P2 + P3 * P3);
+    const double iPb = 1.0 / sqrt(P1b * P1b + P2b * P2b + P3b * P3b);
+    const double tmp = iP * (P3)*G, tmpb = iPb * (P3b)*Gb;
+    st[o] = T(G + tmp);
+    st[o + fs] = T(G - tmp);
+    st[o + 2 * fs] = T(emr * iP);
+    st[o + 3 * fs] = T(emi * iP);
+    st[o + 4 * fs] = T(Gb + tmpb);
+    st[o + 5 * fs] = T(Gb - tmpb);
+    st[o + 6 * fs] = T(bemr * iPb);
+    st[o + 7 * fs] = T(bemi * iPb);
+}
+template <typename T>
+cudaError_t launch_renormalize(T *reg, const double *G0, const double *G0b, Geom g, cudaStream_t s) {
+    dim3 block(32, 8), grid((g.nvs + 31) / 32, (unsigned)((g.ncell + 7) / 8));
+    k_renormalize<T><<<grid, block, 0, s>>>(reg, G0, G0b, g);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------- instances
+#define NUOSC_INSTANTIATE(T)                                                                                   \
+    template cudaError_t launch_moments<T>(const T *, double *, Quad, Geom, cudaStream_t);                    \
+    template cudaError_t launch_stage_direct<T>(const StageArgs<T> &, int, bool, cudaStream_t);              \
+    template cudaError_t launch_init<T>(T *, const double *, const double *, Geom, int, double, double, double, \
+                                        double, uint64_t, cudaStream_t);                                      \
+    template cudaError_t launch_analysis<T>(const T *, const double *, const double *, const double *, Geom,   \
+                                            double *, double *, cudaStream_t);                                \
+    template cudaError_t launch_gather<T>(const T *, int, const int *, int, const int *, int, const double *,  \
+                                          const double *, Geom, double *, cudaStream_t);                      \
+    template cudaError_t launch_import<T>(T *, const double *, Geom, int, int, int, cudaStream_t);            \
+    template cudaError_t launch_export<T>(const T *, double *, Geom, int, int, int, cudaStream_t);            \
+    template cudaError_t launch_vectorize<T>(T *, const T *, double, const T *, const T *, Geom, cudaStream_t); \
+    template cudaError_t launch_renormalize<T>(T *, const double *, const double *, Geom, cudaStream_t);
+
+NUOSC_INSTANTIATE(double)
+NUOSC_INSTANTIATE(float)
+
+}  // namespace nuosc

@@ -1,0 +1,249 @@
+// ref_capi.cpp -- C API over the reference's own NuOsc class (TEST INFRASTRUCTURE ONLY).
+//
+// Linked with the reference's unmodified CPU sources (nuosc_class.cpp,
+// nuosc_boundary.cpp, nuosc_ana.cpp, nuosc_init.cpp, CartGrid.cpp,
+// nuosc_snapshot.cpp) by oracle/Makefile into oracle/_ref/libnuosc_ref_ko{6,4}.so.
+// Tests use it to pin the C oracle and to generate the golden fixtures; bench.py
+// times it as the reference CPU baseline.  The product never loads it.
+//
+// The only thing this file adds to the reference is the initial-data
+// injection: the reference draws its perturbation with rand() per (x,z,v)
+// (nuosc_init.cpp:5,100), which is not reproducible under OpenMP, so the
+// harness lets the reference compute G0/G0b itself (fillInitValue with a
+// constant perturbation, nuosc_init.cpp:70-127) and then overwrites v_stat
+// with the seeded per-(x,z) perturbation using the same formulas.
+#include "nuosc_class.h"
+
+#include <cfloat>
+#include <cstdint>
+#include <cstdio>
+#include <fcntl.h>
+#include <unistd.h>
+
+namespace {
+
+struct RefSim {
+    NuOsc *s = nullptr;
+    std::string workdir, anapath;
+};
+
+// Run f inside the simulation's working directory (the reference writes
+// analysis.dat and snapshot files relative to the current directory, into
+// 32-byte filename buffers, nuosc_snapshot.cpp:26,94).
+template <class F> void in_dir(const std::string &dir, F &&f) {
+    char cwd[4096];
+    if (!getcwd(cwd, sizeof cwd)) cwd[0] = 0;
+    if (!dir.empty() && chdir(dir.c_str()) != 0) return;
+    f();
+    if (cwd[0] && chdir(cwd) != 0) { /* keep going */ }
+}
+
+// Run f with stdout sent to /dev/null (the reference prints on every call).
+template <class F> void quiet(F &&f) {
+    fflush(stdout);
+    int saved = dup(1);
+    int devnull = open("/dev/null", O_WRONLY);
+    if (devnull >= 0) { dup2(devnull, 1); close(devnull); }
+    f();
+    fflush(stdout);
+    if (saved >= 0) { dup2(saved, 1); close(saved); }
+}
+
+uint64_t mix64(uint64_t z) {
+    z += 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+double uniform01(uint64_t seed, int i, int j) {
+    uint64_t key = ((uint64_t)(uint32_t)i << 32) | (uint64_t)(uint32_t)j;
+    return (double)(mix64(mix64(seed) ^ key) >> 11) * 0x1.0p-53;
+}
+
+FieldVar *reg_of(NuOsc *s, int reg) {
+    switch (reg) {
+    case 0: return s->v_stat;
+    case 1: return s->v_rhs;
+    case 2: return s->v_pre;
+    default: return s->v_cor;
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+void *ref_create(int nn, double x0, double x1, double z0, double z1, double dx, double dz, double cfl,
+                 double ko, int ghost, double mu, double pmo, const char *workdir) {
+    RefSim *r = new RefSim;
+    char cwd[4096];
+    if (!getcwd(cwd, sizeof cwd)) cwd[0] = 0;
+    if (workdir && chdir(workdir) != 0) { delete r; return nullptr; }
+    quiet([&] {
+        r->s = new NuOsc(1, 1, nn, 0, ghost, ghost, x0, x1, z0, z1, dx, dz, cfl, ko);
+        r->s->set_mu(mu);
+        r->s->set_pmo(pmo);
+        r->s->set_renorm(false);
+    });
+    r->workdir = workdir ? workdir : ".";
+    r->anapath = r->workdir + "/analysis.dat";
+    if (cwd[0] && chdir(cwd) != 0) { /* keep going */ }
+    return r;
+}
+
+void ref_destroy(void *h) {
+    RefSim *r = (RefSim *)h;
+    if (!r) return;
+    quiet([&] { delete r->s; });
+    delete r;
+}
+
+// ints: nx, nz, nv, gx ; dbls: dt, ds_L, phy_time, n_nue0[0], n_nue0[1]
+void ref_info(void *h, int *ints, double *dbls) {
+    NuOsc *s = ((RefSim *)h)->s;
+    ints[0] = s->grid.nx; ints[1] = s->grid.nz; ints[2] = s->grid.nv; ints[3] = s->grid.gx;
+    dbls[0] = s->dt; dbls[1] = s->ds_L; dbls[2] = s->phy_time; dbls[3] = s->n_nue0[0]; dbls[4] = s->n_nue0[1];
+}
+
+// Quadrature and the spectra G0/G0b at (x,z) cell (0,0) (they are x,z independent).
+void ref_velocities(void *h, double *vx, double *vy, double *vz, double *vw, double *G0, double *G0b) {
+    NuOsc *s = ((RefSim *)h)->s;
+    const int nv = s->grid.nv;
+    for (int v = 0; v < nv; ++v) {
+        vx[v] = s->grid.vx.data()[v];
+        vy[v] = s->grid.vy.data()[v];
+        vz[v] = s->grid.vz.data()[v];
+        vw[v] = s->grid.vw.data()[v];
+        G0[v] = s->G0[s->grid.idx(0, 0, v)];
+        G0b[v] = s->G0b[s->grid.idx(0, 0, v)];
+    }
+}
+
+// Seeded initial data (see the file comment).  ipt as in fillInitValue with
+// ipt==1 replaced by eps0*U(-1,1) per (x,z) drawn from `seed`.
+void ref_fill_init(void *h, int ipt, double alpha, double eps0, double sigma, double lnue, double lnueb,
+                   double lnuex, double lnuebx, uint64_t seed) {
+    NuOsc *s = ((RefSim *)h)->s;
+    if (lnuex <= 0) lnuex = DBL_MAX;
+    if (lnuebx <= 0) lnuebx = DBL_MAX;
+    if (ipt != 1) {
+        quiet([&] { s->fillInitValue(ipt, alpha, eps0, sigma, lnue, lnueb, lnuex, lnuebx); });
+        return;
+    }
+    quiet([&] { s->fillInitValue(3, alpha, 0.0, sigma, lnue, lnueb, lnuex, lnuebx); });
+    double n00 = 0, n01 = 0;
+    for (int i = 0; i < s->grid.nx; ++i)
+        for (int j = 0; j < s->grid.nz; ++j) {
+            const double tmpr = eps0 * (2.0 * uniform01(seed, i, j) - 1.0);
+            const double p3o = sqrt(1.0 - tmpr * tmpr);
+            for (int v = 0; v < s->grid.nv; ++v) {
+                const auto ijv = s->grid.idx(i, j, v);
+                s->v_stat->ee[ijv] = 0.5 * s->G0[ijv] * (1.0 + p3o);
+                s->v_stat->mm[ijv] = 0.5 * s->G0[ijv] * (1.0 - p3o);
+                s->v_stat->emr[ijv] = 0.5 * s->G0[ijv] * tmpr;
+                s->v_stat->emi[ijv] = 0.0;
+                s->v_stat->bee[ijv] = 0.5 * s->G0b[ijv] * (1.0 + p3o);
+                s->v_stat->bmm[ijv] = 0.5 * s->G0b[ijv] * (1.0 - p3o);
+                s->v_stat->bemr[ijv] = 0.5 * s->G0b[ijv] * tmpr;
+                s->v_stat->bemi[ijv] = 0.0;
+                n00 += s->grid.vw.data()[v] * s->v_stat->ee[ijv];
+                n01 += s->grid.vw.data()[v] * s->v_stat->bee[ijv];
+            }
+        }
+    s->n_nue0[0] = n00 * s->ds_L;
+    s->n_nue0[1] = n01 * s->ds_L;
+}
+
+// Interior of one field of one register, compact (x, z, v) order.
+void ref_get_state(void *h, int reg, int field, double *out) {
+    NuOsc *s = ((RefSim *)h)->s;
+    real *a = reg_of(s, reg)->getAllFields()[field];
+    const int nx = s->grid.nx, nz = s->grid.nz, nv = s->grid.nv;
+    for (int i = 0; i < nx; ++i)
+        for (int j = 0; j < nz; ++j)
+            for (int v = 0; v < nv; ++v) out[((long)i * nz + j) * nv + v] = a[s->grid.idx(i, j, v)];
+}
+void ref_set_state(void *h, int reg, int field, const double *in) {
+    NuOsc *s = ((RefSim *)h)->s;
+    real *a = reg_of(s, reg)->getAllFields()[field];
+    const int nx = s->grid.nx, nz = s->grid.nz, nv = s->grid.nv;
+    for (int i = 0; i < nx; ++i)
+        for (int j = 0; j < nz; ++j)
+            for (int v = 0; v < nv; ++v) a[s->grid.idx(i, j, v)] = in[((long)i * nz + j) * nv + v];
+}
+// Whole ghosted array of one field (lpts doubles), for boundary checks.
+void ref_get_ghosted(void *h, int reg, int field, double *out) {
+    NuOsc *s = ((RefSim *)h)->s;
+    real *a = reg_of(s, reg)->getAllFields()[field];
+    memcpy(out, a, sizeof(double) * s->grid.get_lpts());
+}
+
+void ref_update_boundary(void *h, int reg) {
+    NuOsc *s = ((RefSim *)h)->s;
+    s->updatePeriodicBoundary(reg_of(s, reg));
+}
+
+// calRHS(v_rhs, v_stat) after the periodic ghost fill of v_stat.
+void ref_calrhs(void *h) {
+    NuOsc *s = ((RefSim *)h)->s;
+    s->updatePeriodicBoundary(s->v_stat);
+    s->calRHS(s->v_rhs, s->v_stat);
+}
+
+void ref_step(void *h, int nsteps) {
+    NuOsc *s = ((RefSim *)h)->s;
+    for (int t = 0; t < nsteps; ++t) s->step_rk4();
+}
+
+// analysis(); the sums are locals of the reference, so the values are read
+// back from the analysis.dat line it appends (13 significant digits).
+// out: phy_time maxdP surv survb avgP avgPb aM0 Lex ELNe
+int ref_analysis(void *h, double *out) {
+    RefSim *r = (RefSim *)h;
+    quiet([&] { r->s->analysis(); });
+    FILE *f = fopen(r->anapath.c_str(), "r");
+    if (!f) return -1;
+    char line[1024], last[1024] = {0};
+    while (fgets(line, sizeof line, f))
+        if (line[0] != '#') memcpy(last, line, sizeof line);
+    fclose(f);
+    int n = sscanf(last, "%lf %lf %lf %lf %lf %lf %lf %lf %lf", out, out + 1, out + 2, out + 3, out + 4, out + 5,
+                   out + 6, out + 7, out + 8);
+    return n == 9 ? 0 : -2;
+}
+
+// Snapshot registration over fields of v_stat as it is now, then write step t.
+void ref_snapshot_at_v(void *h, const char *fntpl, int every, int nvidx, const int *vidx, int nfields,
+                       const int *fields, int t) {
+    RefSim *r = (RefSim *)h;
+    NuOsc *s = r->s;
+    std::list<real *> vars;
+    auto all = s->v_stat->getAllFields();
+    for (int k = 0; k < nfields; ++k) vars.push_back(all[fields[k]]);
+    std::vector<int> vi(vidx, vidx + nvidx);
+    in_dir(r->workdir, [&] {
+        quiet([&] {
+            s->snapshots.clear();
+            s->addSnapShotAtV(vars, (char *)fntpl, every, vi);
+            s->checkSnapShot(t);
+        });
+    });
+}
+void ref_snapshot_at_xv(void *h, const char *fntpl, int every, int nxidx, const int *xidx, int nvidx,
+                        const int *vidx, int nfields, const int *fields, int t) {
+    RefSim *r = (RefSim *)h;
+    NuOsc *s = r->s;
+    std::list<real *> vars;
+    auto all = s->v_stat->getAllFields();
+    for (int k = 0; k < nfields; ++k) vars.push_back(all[fields[k]]);
+    std::vector<int> xi(xidx, xidx + nxidx), vi(vidx, vidx + nvidx);
+    in_dir(r->workdir, [&] {
+        quiet([&] {
+            s->snapshots.clear();
+            s->addSnapShotAtXV(vars, (char *)fntpl, every, xi, vi);
+            s->checkSnapShot(t);
+        });
+    });
+}
+
+}  // extern "C"

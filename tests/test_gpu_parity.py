@@ -1,0 +1,306 @@
+"""Parity of the CUDA path (through the C ABI) with the reference.
+
+Fixtures in tests/golden/ come from the reference's own build; the oracle
+(oracle/nuosc_oracle.c, pinned against that build by test_oracle.py) checks
+larger cases.  The FP64 bar is the norm-wise relative error
+    max|gpu - ref| / max|ref|  per field
+after the stated number of RK4 steps:
+    FP64_TOL = 1e-12 (state), CALRHS_TOL = 1e-13 (one right-hand side).
+"""
+import os
+
+import numpy as np
+import pytest
+
+import pyoracle as po
+from conftest import golden
+
+pytestmark = pytest.mark.gpu
+
+FP64_TOL = 1e-12
+CALRHS_TOL = 1e-13
+PHYS = dict(alpha=0.9, eps0=1e-6, sigma=1.0, lnue=0.6, lnueb=0.5)
+
+
+@pytest.fixture(scope="module")
+def nb(gpu):
+    import nuosc_b200
+    return nuosc_b200
+
+
+def make(nb, params, ko_order, precision=0, kernel=None):
+    x0, x1, dx, cfl, ko, mu, pmo, nn = [float(p) for p in params]
+    g = 3 if ko_order == 6 else 2
+    s = nb.NuOsc(1, 1, int(nn), 0, g, g, x0, x1, x0, x1, dx, dx, cfl, ko, precision=precision)
+    s.set_mu(mu)
+    s.set_pmo(pmo)
+    if kernel is not None:
+        s.set_kernel(kernel)
+    return s
+
+
+def box_params(n, nn, dx=0.1, cfl=0.4, ko=0.1, mu=1.0, pmo=0.0):
+    x0, x1 = po.box(n, dx)
+    return (x0, x1, dx, cfl, ko, mu, pmo, nn)
+
+
+def diag_vec(d):
+    return np.array([d[k] for k in po.DIAG_NAMES])
+
+
+def assert_diag_close(a, ref):
+    np.testing.assert_allclose(a[[0, 2, 3, 6, 7]], ref[[0, 2, 3, 6, 7]], rtol=1e-12)
+    np.testing.assert_allclose(a[[1, 4, 5, 8]], ref[[1, 4, 5, 8]], atol=1e-13, rtol=1e-4)
+
+
+KERNELS = [1, 2]  # direct, x-march
+
+
+def _kernel_ok(nb, s, kernel):
+    if kernel == nb.KERNEL_DIRECT:
+        s.set_kernel(kernel)
+    if kernel == nb.KERNEL_XMARCH:
+        try:
+            s.step_rk4(0)
+            s.set_kernel(kernel)
+            s.step_rk4(0)
+        except nb.NuoscError as e:
+            if e.code == 6:
+                pytest.skip("x-march kernel not available for this geometry")
+            raise
+
+
+@pytest.mark.parametrize("ko_order", [6, 4])
+def test_init_matches_reference(nb, ko_order):
+    g = golden(f"run_ko{ko_order}.npz")
+    s = make(nb, g["params"], ko_order)
+    s.fillInitValue(1, seed=int(g["seed"]), **PHYS)
+    st = s.get_state()
+    assert po.relerr(st, g["state0"]) < 1e-15
+    np.testing.assert_allclose(s.n_nue0, g["n_nue0"], rtol=1e-13)
+    np.testing.assert_allclose(s.G0, g["G0"], rtol=1e-15)
+    np.testing.assert_allclose(s.G0b, g["G0b"], rtol=1e-15)
+
+
+@pytest.mark.parametrize("ko_order", [6, 4])
+def test_calrhs_matches_reference(nb, ko_order):
+    g = golden(f"calrhs_ko{ko_order}.npz")
+    s = make(nb, g["params"], ko_order)
+    s.set_state(g["inp"], nb.REG_STAT)
+    s.updatePeriodicBoundary(nb.REG_STAT)
+    s.calRHS(nb.REG_RHS, nb.REG_STAT)
+    rhs = s.get_state(nb.REG_RHS)
+    for f in range(8):
+        assert po.relerr(rhs[f], g["rhs"][f]) < CALRHS_TOL, f
+
+
+@pytest.mark.parametrize("kernel", KERNELS)
+@pytest.mark.parametrize("ko_order", [6, 4])
+def test_ten_steps_match_reference(nb, ko_order, kernel):
+    g = golden(f"run_ko{ko_order}.npz")
+    s = make(nb, g["params"], ko_order)
+    s.fillInitValue(1, seed=int(g["seed"]), **PHYS)
+    _kernel_ok(nb, s, kernel)
+    a0 = diag_vec(s.analysis())
+    s.step_rk4(10)
+    st = s.get_state()
+    for f in range(8):
+        assert po.relerr(st[f], g["state10"][f]) < FP64_TOL, f
+    a1 = diag_vec(s.analysis())
+    assert_diag_close(a0, g["ana0"])
+    assert_diag_close(a1, g["ana10"])
+
+
+@pytest.mark.parametrize("kernel", KERNELS)
+def test_c0_config_100_steps(nb, kernel):
+    """64x64 cells x 162 velocities, 100 steps, analysis every 10 (config 0):
+    diagnostics against the reference's series, state against the oracle."""
+    g = golden("c0_series.npz")
+    p = box_params(64, 4)
+    s = make(nb, p, 6)
+    s.fillInitValue(1, seed=int(g["seed"]), **PHYS)
+    _kernel_ok(nb, s, kernel)
+    series = [diag_vec(s.analysis())]
+    for _ in range(10):
+        s.step_rk4(10)
+        series.append(diag_vec(s.analysis()))
+    series = np.array(series)
+    ref = g["series"]
+    np.testing.assert_allclose(series[:, [0, 2, 3, 6, 7]], ref[:, [0, 2, 3, 6, 7]], rtol=1e-12)
+    np.testing.assert_allclose(series[:, 1], ref[:, 1], rtol=1e-4, atol=1e-14)
+    flat = s.get_state().reshape(8, -1)
+    np.testing.assert_allclose(flat.sum(axis=1), g["fsum"], rtol=1e-12, atol=1e-12 * g["fmax"].max())
+    o = po.Oracle(nn=4, x0=p[0], x1=p[1], z0=p[0], z1=p[1], dx=0.1, dz=0.1, cfl=0.4, ko=0.1, ko_order=6)
+    o.fill_init(ipt=1, seed=int(g["seed"]), **PHYS)
+    o.step(100)
+    ref_state = o.get_state(0).reshape(8, -1)
+    for f in range(8):
+        assert po.relerr(flat[f], ref_state[f]) < FP64_TOL, f
+
+
+@pytest.mark.slow
+@pytest.mark.parametrize("kernel", KERNELS)
+def test_128_cells_162_velocities_100_steps(nb, kernel):
+    """The parity size of the production configuration (128^2 x 162)."""
+    p = box_params(128, 4)
+    s = make(nb, p, 6)
+    s.fillInitValue(1, seed=77, **PHYS)
+    _kernel_ok(nb, s, kernel)
+    s.step_rk4(100)
+    st = s.get_state()
+    o = po.Oracle(nn=4, x0=p[0], x1=p[1], z0=p[0], z1=p[1], dx=0.1, dz=0.1, cfl=0.4, ko=0.1, ko_order=6)
+    o.fill_init(ipt=1, seed=77, **PHYS)
+    o.step(100)
+    ref = o.get_state(0)
+    for f in range(8):
+        assert po.relerr(st[f], ref[f]) < FP64_TOL, f
+    assert_diag_close(diag_vec(s.analysis()), o.analysis())
+
+
+@pytest.mark.parametrize("kernel", KERNELS)
+@pytest.mark.parametrize("n,nn", [(8, 1), (12, 2), (20, 2), (24, 4)])
+def test_odd_sizes_against_oracle(nb, n, nn, kernel):
+    """Sizes that do not divide the tile shapes, nv with a partial velocity block."""
+    p = box_params(n, nn, mu=1.3, pmo=0.2)
+    s = make(nb, p, 6)
+    s.fillInitValue(1, seed=3, alpha=1.2, eps0=1e-3, sigma=1.0, lnue=0.6, lnueb=0.4)
+    _kernel_ok(nb, s, kernel)
+    s.step_rk4(7)
+    o = po.Oracle(nn=nn, x0=p[0], x1=p[1], z0=p[0], z1=p[1], dx=0.1, dz=0.1, cfl=0.4, ko=0.1, ko_order=6, mu=1.3,
+                  pmo=0.2)
+    o.fill_init(ipt=1, seed=3, alpha=1.2, eps0=1e-3, sigma=1.0, lnue=0.6, lnueb=0.4)
+    o.step(7)
+    a, b = s.get_state(), o.get_state(0)
+    for f in range(8):
+        assert po.relerr(a[f], b[f]) < FP64_TOL, f
+
+
+def test_state_roundtrip_layouts(nb):
+    p = box_params(8, 2)
+    for prec in (nb.FP64, nb.FP32):
+        s = make(nb, p, 6, precision=prec)
+        rng = np.random.default_rng(0)
+        st = rng.standard_normal((8, 8, 8, 42))
+        s.set_state(st, nb.REG_PRE)
+        back = s.get_state(nb.REG_PRE)
+        if prec == nb.FP64:
+            assert np.array_equal(back, st)
+        else:
+            assert np.array_equal(back, st.astype(np.float32).astype(np.float64))
+        gh = s.get_field(3, nb.REG_PRE, layout=1)
+        gxz = gh.reshape(8 + 6, 8 + 6, 42)[3:-3, 3:-3]
+        np.testing.assert_array_equal(gxz, back[3])
+        gh2 = np.zeros_like(gh)
+        gh2.reshape(14, 14, 42)[3:-3, 3:-3] = st[5]
+        s.set_field(5, gh2, nb.REG_COR, layout=1)
+        np.testing.assert_array_equal(s.get_field(5, nb.REG_COR), back[5])
+
+
+def test_vectorize(nb):
+    p = box_params(8, 2)
+    s = make(nb, p, 6)
+    rng = np.random.default_rng(1)
+    a, b, c = (rng.standard_normal((8, 8, 8, 42)) for _ in range(3))
+    s.set_state(a, 1)
+    s.set_state(b, 2)
+    s.set_state(c, 3)
+    s.vectorize(0, 1, 0.25, 2)
+    np.testing.assert_allclose(s.get_state(0), a + 0.25 * b, rtol=0, atol=1e-15)
+    s.vectorize(0, 1, 0.5, 2, 3)
+    np.testing.assert_allclose(s.get_state(0), a + 0.5 * (b + c), rtol=0, atol=1e-15)
+
+
+def test_snapshot_files_match_reference(nb, tmp_path):
+    g = golden("snapshot.npz")
+    s = make(nb, box_params(8, 2), 6)
+    s.fillInitValue(1, seed=5, **PHYS)
+    assert po.relerr(s.get_state(), g["state0"]) < 1e-15
+    cwd = os.getcwd()
+    os.chdir(tmp_path)
+    try:
+        s.addSnapShotAtV([0, 2], "ee%06d.bin", 1, [0, 21, 41])
+        s.addSnapShotAtXV([4, 6, 3], "xv%06d.bin", 1, [1, 4], [3, 7, 40])
+        s.checkSnapShot(0)
+    finally:
+        os.chdir(cwd)
+    for name in ("ee000000.bin", "ee000000.bin.meta", "xv000000.bin", "xv000000.bin.meta"):
+        mine = (tmp_path / name).read_bytes()
+        assert mine == g[name.replace(".", "_")].tobytes(), name
+
+
+def test_gather_derived_fields(nb):
+    p = box_params(8, 2)
+    s = make(nb, p, 6)
+    s.fillInitValue(1, seed=9, alpha=1.1, eps0=1e-2, sigma=1.0, lnue=0.6, lnueb=0.5)
+    s.step_rk4(3)
+    st = s.get_state()
+    G0, G0b = s.G0, s.G0b
+    P3 = (st[0] - st[1]) / G0
+    P2b = 2 * st[7] / G0b
+    xi, vi = [0, 5], [1, 17, 40]
+    np.testing.assert_allclose(s.gather("P3", xi, vi), P3[xi][:, :, vi], rtol=1e-14, atol=1e-15)
+    np.testing.assert_allclose(s.gather("P2b", xi, vi), P2b[xi][:, :, vi], rtol=1e-14, atol=1e-15)
+    P = np.sqrt((2 * st[2] / G0) ** 2 + (2 * st[3] / G0) ** 2 + P3 ** 2)
+    np.testing.assert_allclose(s.gather("dP", xi, vi), np.abs(1 - P)[xi][:, :, vi], atol=1e-15)
+
+
+def test_analysis_file_format(nb, tmp_path):
+    s = make(nb, box_params(8, 2), 6)
+    s.fillInitValue(1, seed=1, **PHYS)
+    path = str(tmp_path / "analysis.dat")
+    s.open_analysis_file(path)
+    s.analysis()
+    s.step_rk4(2)
+    d = s.analysis()
+    lines = open(path).read().splitlines()
+    assert lines[0].startswith("### [ phy_time")
+    vals = [float(x) for x in lines[-1].split()]
+    assert len(vals) == 9
+    np.testing.assert_allclose(vals[1:], [d[k] for k in po.DIAG_NAMES[1:]], rtol=1e-12, atol=1e-25)
+
+
+def test_error_paths(nb):
+    s = make(nb, box_params(8, 2), 6)
+    with pytest.raises(nb.NuoscError) as e:
+        s.calRHS(nb.REG_STAT, nb.REG_STAT)
+    assert e.value.code == 1
+    with pytest.raises(nb.NuoscError):
+        s.updatePeriodicBoundary(7)
+    with pytest.raises(nb.NuoscError) as e:
+        s.fillInitValue(4, **PHYS)
+    assert e.value.code == 6
+    # a non-finite state is reported by analysis() as a numeric error
+    s.fillInitValue(1, seed=1, **PHYS)
+    st = s.get_state()
+    st[2, 3, 4, 5] = np.nan
+    s.set_state(st)
+    with pytest.raises(nb.NuoscError) as e:
+        s.analysis()
+    assert e.value.code == 4
+
+
+def test_fp32_tracks_fp64(nb):
+    """FP32 state with FP64 moments and diagnostics stays close to FP64 on
+    config 0 over 100 steps."""
+    p = box_params(64, 4)
+    runs = {}
+    for prec in (nb.FP64, nb.FP32):
+        s = make(nb, p, 6, precision=prec)
+        s.fillInitValue(1, seed=2024, **PHYS)
+        series = [diag_vec(s.analysis())]
+        for _ in range(10):
+            s.step_rk4(10)
+            series.append(diag_vec(s.analysis()))
+        runs[prec] = np.array(series)
+    d = np.abs(runs[nb.FP32] - runs[nb.FP64])
+    assert d[:, 2].max() < 1e-6      # Pee
+    assert d[:, 4].max() < 1e-6      # <|P|-1>
+    assert d[:, 6].max() < 1e-6      # |M0|
+
+
+def test_launch_count(nb):
+    s = make(nb, box_params(16, 2), 6)
+    s.fillInitValue(1, seed=1, **PHYS)
+    n0 = s.kernel_launches
+    s.step_rk4(3)
+    assert s.kernel_launches - n0 >= 3 * 4

@@ -1,0 +1,97 @@
+"""The C oracle against the golden fixtures made by the reference's own build.
+
+These pin the restatement in oracle/nuosc_oracle.c before it is trusted as the
+checker of the CUDA path (CPU only).
+"""
+import numpy as np
+import pytest
+
+import pyoracle as po
+from conftest import golden
+
+PHYS = dict(alpha=0.9, eps0=1e-6, lnue=0.6, lnueb=0.5)
+
+
+def _kw(params, ko_order):
+    x0, x1, dx, cfl, ko, mu, pmo, nn = params
+    return dict(nn=int(nn), x0=x0, x1=x1, z0=x0, z1=x1, dx=dx, dz=dx, cfl=cfl, ko=ko, ko_order=ko_order, mu=mu,
+                pmo=pmo)
+
+
+@pytest.mark.parametrize("nn", [1, 2, 4, 8])
+def test_quadrature_bit_exact(nn):
+    g = golden("quadrature.npz")
+    vx, vy, vz, vw = po.icosahedron(nn)
+    for name, a in zip(("vx", "vy", "vz", "vw"), (vx, vy, vz, vw)):
+        assert np.array_equal(a, g[f"{name}_{nn}"]), name
+    assert len(vw) == 10 * nn * nn + 2
+
+
+def test_quadrature_known_answers():
+    """Sphere integrals of test_vint2d.cpp:33-47: 4*pi for f=1 converges from
+    below (flat-triangle areas) and x^2 y^2 z^2 integrates towards 4*pi/105."""
+    prev = 0.0
+    for nn in (1, 2, 4, 8, 16):
+        vx, vy, vz, vw = po.icosahedron(nn)
+        s0 = vw.sum()
+        assert prev < s0 < 4 * np.pi
+        prev = s0
+    vx, vy, vz, vw = po.icosahedron(16)
+    assert abs(vw.sum() - 4 * np.pi) / (4 * np.pi) < 2e-3
+    s2 = (vw * (vx * vy * vz) ** 2).sum()
+    assert abs(s2 - 4 * np.pi / 105) / (4 * np.pi / 105) < 2e-2
+
+
+@pytest.mark.parametrize("ko_order", [6, 4])
+def test_run_matches_reference(ko_order):
+    g = golden(f"run_ko{ko_order}.npz")
+    o = po.Oracle(**_kw(g["params"], ko_order))
+    o.fill_init(ipt=1, seed=int(g["seed"]), **PHYS)
+    s0 = o.get_state(0)
+    assert po.relerr(s0, g["state0"]) < 1e-15
+    np.testing.assert_allclose(o.info()["n_nue0"], g["n_nue0"], rtol=1e-14)
+    a0 = o.analysis()
+    o.step(10)
+    s1 = o.get_state(0)
+    for f in range(8):
+        assert po.relerr(s1[f], g["state10"][f]) < 1e-13, f
+    a1 = o.analysis()
+    for a, ref in ((a0, g["ana0"]), (a1, g["ana10"])):
+        # surv/survb/aM0/Lex are O(1) sums: relative; maxdP/avgP/ELNe are
+        # cancellation-limited O(1e-12) quantities: absolute
+        np.testing.assert_allclose(a[[0, 2, 3, 6, 7]], ref[[0, 2, 3, 6, 7]], rtol=1e-12)
+        np.testing.assert_allclose(a[[1, 4, 5, 8]], ref[[1, 4, 5, 8]], atol=1e-13)
+
+
+@pytest.mark.parametrize("ko_order", [6, 4])
+def test_calrhs_matches_reference(ko_order):
+    g = golden(f"calrhs_ko{ko_order}.npz")
+    o = po.Oracle(**_kw(g["params"], ko_order))
+    o.set_state(g["inp"], 0)
+    o.calrhs()
+    rhs = o.get_state(1)
+    for f in range(8):
+        assert po.relerr(rhs[f], g["rhs"][f]) < 1e-14, f
+
+
+@pytest.mark.slow
+def test_c0_series_matches_reference():
+    """64x64 cells x 162 velocities, 100 RK4 steps, analysis every 10."""
+    g = golden("c0_series.npz")
+    x0, x1 = po.box(64, 0.1)
+    o = po.Oracle(nn=4, x0=x0, x1=x1, z0=x0, z1=x1, dx=0.1, dz=0.1, cfl=0.4, ko=0.1, ko_order=6, mu=1.0, pmo=0.0)
+    o.fill_init(ipt=1, seed=int(g["seed"]), **PHYS)
+    series = [o.analysis()]
+    for _ in range(10):
+        o.step(10)
+        series.append(o.analysis())
+    series = np.array(series)
+    ref = g["series"]
+    np.testing.assert_allclose(series[:, [0, 2, 3, 6, 7]], ref[:, [0, 2, 3, 6, 7]], rtol=1e-12)
+    # max||P|-1| grows by 5 orders through the instability; compare relative to its size
+    np.testing.assert_allclose(series[:, 1], ref[:, 1], rtol=1e-4, atol=1e-14)
+    flat = o.get_state(0).reshape(8, -1)
+    np.testing.assert_allclose(flat.sum(axis=1), g["fsum"], rtol=1e-12, atol=1e-12 * g["fmax"].max())
+    for f in range(8):
+        assert po.relerr(flat[f, g["sample_idx"]], g["sample"][f]) < 1e-12 * max(1.0, g["fmax"][f] / np.abs(
+            g["sample"][f]).max())
