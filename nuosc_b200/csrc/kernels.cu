@@ -62,8 +62,8 @@ cudaError_t launch_moments(const T *reg, double *mom, Quad q, Geom g, cudaStream
 template <typename T, bool KO6, int MODE>
 __global__ void __launch_bounds__(256) k_stage_direct(StageArgs<T> a) {
     const Geom g = a.g;
-    const int v = blockIdx.x * 32 + threadIdx.x;
-    const long long cell = (long long)blockIdx.y * 8 + threadIdx.y;
+    const int v = blockIdx.y * 32 + threadIdx.x;
+    const long long cell = (long long)blockIdx.x * 8 + threadIdx.y;
     if (cell >= g.ncell || v >= g.nvs) return;
     const int i = (int)(cell / g.nz), j = (int)(cell - (long long)i * g.nz);
     constexpr int R = KO6 ? 3 : 2;
@@ -131,7 +131,7 @@ __global__ void __launch_bounds__(256) k_stage_direct(StageArgs<T> a) {
 template <typename T, bool KO6>
 static cudaError_t launch_direct_ko(const StageArgs<T> &a, int mode, cudaStream_t s) {
     dim3 block(32, 8);
-    dim3 grid((a.g.nvs + 31) / 32, (unsigned)((a.g.ncell + 7) / 8));
+    dim3 grid((unsigned)((a.g.ncell + 7) / 8), (a.g.nvs + 31) / 32);
     switch (mode) {
     case MODE_RHS: k_stage_direct<T, KO6, MODE_RHS><<<grid, block, 0, s>>>(a); break;
     case MODE_S1: k_stage_direct<T, KO6, MODE_S1><<<grid, block, 0, s>>>(a); break;
@@ -161,8 +161,8 @@ __device__ __forceinline__ uint64_t mix64(uint64_t z) {
 template <typename T>
 __global__ void k_init(T *reg, const double *G0, const double *G0b, Geom g, int ipt, double eps0, double sigma,
                        double z0, double dz, uint64_t seed) {
-    const int v = blockIdx.x * 32 + threadIdx.x;
-    const long long cell = (long long)blockIdx.y * 8 + threadIdx.y;
+    const int v = blockIdx.y * 32 + threadIdx.x;
+    const long long cell = (long long)blockIdx.x * 8 + threadIdx.y;
     if (cell >= g.ncell || v >= g.nvs) return;
     const int i = (int)(cell / g.nz), j = (int)(cell - (long long)i * g.nz);
     const long long o = cell * g.nvs + v;
@@ -201,7 +201,7 @@ template <typename T>
 cudaError_t launch_init(T *reg, const double *G0, const double *G0b, Geom g, int ipt, double eps0, double sigma,
                         double z0, double dz, uint64_t seed, cudaStream_t s) {
     dim3 block(32, 8);
-    dim3 grid((g.nvs + 31) / 32, (unsigned)((g.ncell + 7) / 8));
+    dim3 grid((unsigned)((g.ncell + 7) / 8), (g.nvs + 31) / 32);
     k_init<T><<<grid, block, 0, s>>>(reg, G0, G0b, g, ipt, eps0, sigma, z0, dz, seed);
     return cudaGetLastError();
 }
@@ -342,16 +342,16 @@ __device__ __forceinline__ long long host_index(int layout, int i, int j, int v,
 
 template <typename T>
 __global__ void k_import(T *dst, const double *src, Geom g, int layout, int gx, int gz) {
-    const int v = blockIdx.x * 32 + threadIdx.x;
-    const long long cell = (long long)blockIdx.y * 8 + threadIdx.y;
+    const int v = blockIdx.y * 32 + threadIdx.x;
+    const long long cell = (long long)blockIdx.x * 8 + threadIdx.y;
     if (cell >= g.ncell || v >= g.nvs) return;
     const int i = (int)(cell / g.nz), j = (int)(cell - (long long)i * g.nz);
     dst[cell * g.nvs + v] = v < g.nv ? T(src[host_index(layout, i, j, v, g, gx, gz)]) : T(0);
 }
 template <typename T>
 __global__ void k_export(const T *src, double *dst, Geom g, int layout, int gx, int gz) {
-    const int v = blockIdx.x * 32 + threadIdx.x;
-    const long long cell = (long long)blockIdx.y * 8 + threadIdx.y;
+    const int v = blockIdx.y * 32 + threadIdx.x;
+    const long long cell = (long long)blockIdx.x * 8 + threadIdx.y;
     if (cell >= g.ncell || v >= g.nv) return;
     const int i = (int)(cell / g.nz), j = (int)(cell - (long long)i * g.nz);
     dst[host_index(layout, i, j, v, g, gx, gz)] = (double)src[cell * g.nvs + v];
@@ -359,13 +359,13 @@ __global__ void k_export(const T *src, double *dst, Geom g, int layout, int gx, 
 
 template <typename T>
 cudaError_t launch_import(T *reg_field, const double *src, Geom g, int layout, int gx, int gz, cudaStream_t s) {
-    dim3 block(32, 8), grid((g.nvs + 31) / 32, (unsigned)((g.ncell + 7) / 8));
+    dim3 block(32, 8), grid((unsigned)((g.ncell + 7) / 8), (g.nvs + 31) / 32);
     k_import<T><<<grid, block, 0, s>>>(reg_field, src, g, layout, gx, gz);
     return cudaGetLastError();
 }
 template <typename T>
 cudaError_t launch_export(const T *reg_field, double *dst, Geom g, int layout, int gx, int gz, cudaStream_t s) {
-    dim3 block(32, 8), grid((g.nvs + 31) / 32, (unsigned)((g.ncell + 7) / 8));
+    dim3 block(32, 8), grid((unsigned)((g.ncell + 7) / 8), (g.nvs + 31) / 32);
     k_export<T><<<grid, block, 0, s>>>(reg_field, dst, g, layout, gx, gz);
     return cudaGetLastError();
 }
@@ -391,8 +391,8 @@ cudaError_t launch_vectorize(T *dst, const T *a, double c, const T *b, const T *
 // ----------------------------------------------------------------------------
 template <typename T>
 __global__ void k_renormalize(T *st, const double *G0, const double *G0b, Geom g) {
-    const int v = blockIdx.x * 32 + threadIdx.x;
-    const long long cell = (long long)blockIdx.y * 8 + threadIdx.y;
+    const int v = blockIdx.y * 32 + threadIdx.x;
+    const long long cell = (long long)blockIdx.x * 8 + threadIdx.y;
     if (cell >= g.ncell || v >= g.nv) return;
     const long long o = cell * g.nvs + v, fs = g.fs;
     const double G = G0[v], Gb = G0b[v];
@@ -415,7 +415,7 @@ __global__ void k_renormalize(T *st, const double *G0, const double *G0b, Geom g
 }
 template <typename T>
 cudaError_t launch_renormalize(T *reg, const double *G0, const double *G0b, Geom g, cudaStream_t s) {
-    dim3 block(32, 8), grid((g.nvs + 31) / 32, (unsigned)((g.ncell + 7) / 8));
+    dim3 block(32, 8), grid((unsigned)((g.ncell + 7) / 8), (g.nvs + 31) / 32);
     k_renormalize<T><<<grid, block, 0, s>>>(reg, G0, G0b, g);
     return cudaGetLastError();
 }

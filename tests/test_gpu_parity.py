@@ -6,6 +6,9 @@ larger cases.  The FP64 bar is the norm-wise relative error
     max|gpu - ref| / max|ref|  per field
 after the stated number of RK4 steps:
     FP64_TOL = 1e-12 (state), CALRHS_TOL = 1e-13 (one right-hand side).
+Diagnostics are sums over 10^4..10^7 terms; their summation order differs
+(tree reduction on the device, sequential or OpenMP on the host), which alone
+moves the O(1) sums by up to ~1e-11 relative, so DIAG_RTOL = 1e-10 there.
 """
 import os
 
@@ -19,6 +22,7 @@ pytestmark = pytest.mark.gpu
 
 FP64_TOL = 1e-12
 CALRHS_TOL = 1e-13
+DIAG_RTOL = 1e-10
 PHYS = dict(alpha=0.9, eps0=1e-6, sigma=1.0, lnue=0.6, lnueb=0.5)
 
 
@@ -49,8 +53,11 @@ def diag_vec(d):
 
 
 def assert_diag_close(a, ref):
-    np.testing.assert_allclose(a[[0, 2, 3, 6, 7]], ref[[0, 2, 3, 6, 7]], rtol=1e-12)
-    np.testing.assert_allclose(a[[1, 4, 5, 8]], ref[[1, 4, 5, 8]], atol=1e-13, rtol=1e-4)
+    np.testing.assert_allclose(a[[0, 2, 3, 6, 7]], ref[[0, 2, 3, 6, 7]], rtol=DIAG_RTOL)
+    np.testing.assert_allclose(a[[1, 4, 5]], ref[[1, 4, 5]], atol=1e-13, rtol=1e-4)
+    # ELNe = |n0 (1 - surv) - n1 (1 - survb)| / (n0 + n1) with 1 - surv ~ 1e-12:
+    # pure cancellation, set by the last bits of surv
+    np.testing.assert_allclose(a[8], ref[8], atol=1e-11)
 
 
 KERNELS = [1, 2]  # direct, x-march
@@ -126,7 +133,7 @@ def test_c0_config_100_steps(nb, kernel):
         series.append(diag_vec(s.analysis()))
     series = np.array(series)
     ref = g["series"]
-    np.testing.assert_allclose(series[:, [0, 2, 3, 6, 7]], ref[:, [0, 2, 3, 6, 7]], rtol=1e-12)
+    np.testing.assert_allclose(series[:, [0, 2, 3, 6, 7]], ref[:, [0, 2, 3, 6, 7]], rtol=DIAG_RTOL)
     np.testing.assert_allclose(series[:, 1], ref[:, 1], rtol=1e-4, atol=1e-14)
     flat = s.get_state().reshape(8, -1)
     np.testing.assert_allclose(flat.sum(axis=1), g["fsum"], rtol=1e-12, atol=1e-12 * g["fmax"].max())
