@@ -124,6 +124,14 @@ class NuOsc:
     def set_kernel(self, kind):
         check(lib().nuosc_set_kernel(self._h, kind))
 
+    def set_tile(self, tz, lx):
+        check(lib().nuosc_set_tile(self._h, int(tz), int(lx)))
+
+    def get_tile(self):
+        tz, lx = C.c_int(), C.c_int()
+        check(lib().nuosc_get_tile(self._h, C.byref(tz), C.byref(lx)))
+        return tz.value, lx.value
+
     def _geometry(self):
         g = _lib.Geometry()
         check(lib().nuosc_get_geometry(self._h, C.byref(g)))

@@ -64,6 +64,8 @@ _SIGS = {
     "nuosc_set_pmo": [_P, _D],
     "nuosc_set_renorm": [_P, _I],
     "nuosc_set_kernel": [_P, _I],
+    "nuosc_set_tile": [_P, _I, _I],
+    "nuosc_get_tile": [_P, _IP, _IP],
     "nuosc_set_time": [_P, _D],
     "nuosc_get_geometry": [_P, C.POINTER(Geometry)],
     "nuosc_get_velocities": [_P, _DP, _DP, _DP, _DP],

@@ -160,6 +160,15 @@ struct nuosc_handle {
         c.st = std::sin(2 * theta);
         c.mu = mu;
         c.pmo = pmo;
+        if (ko6) {
+            c.kz3 = c.kz; c.kz2 = -6 * c.kz; c.kz1 = 15 * c.kz;
+            c.kx3 = c.kx; c.kx2 = -6 * c.kx; c.kx1 = 15 * c.kx;
+            c.kc = -20 * (c.kz + c.kx);
+        } else {
+            c.kz3 = 0; c.kz2 = c.kz; c.kz1 = -4 * c.kz;
+            c.kx3 = 0; c.kx2 = c.kx; c.kx1 = -4 * c.kx;
+            c.kc = 6 * (c.kz + c.kx);
+        }
         return c;
     }
 };
@@ -626,6 +635,23 @@ int nuosc_set_kernel(nuosc_handle *h, int kind) {
     h->mom_valid = false;
     return NUOSC_OK;
 }
+int nuosc_set_tile(nuosc_handle *h, int tz, int lx) {
+    if (!h) return fail(NUOSC_ERR_INVALID, "null handle");
+    if ((tz != 8 && tz != 16) || lx < 1) return fail(NUOSC_ERR_INVALID, "tile tz=%d lx=%d (tz 8 or 16, lx >= 1)", tz, lx);
+    const int nvb_old = xmarch_num_vblocks(h->g, h->tile);
+    h->tile.tz = tz;
+    h->tile.lx = lx;
+    if (xmarch_num_vblocks(h->g, h->tile) != nvb_old) h->mom_valid = false;
+    return NUOSC_OK;
+}
+
+int nuosc_get_tile(const nuosc_handle *h, int *tz, int *lx) {
+    if (!h) return fail(NUOSC_ERR_INVALID, "null handle");
+    if (tz) *tz = h->tile.tz;
+    if (lx) *lx = h->tile.lx;
+    return NUOSC_OK;
+}
+
 int nuosc_set_time(nuosc_handle *h, double t) {
     if (!h) return fail(NUOSC_ERR_INVALID, "null handle");
     h->phy_time = t;

@@ -28,6 +28,11 @@ struct Coeffs {
     double fxs, fzs;  // advection: factor_x = vx * fxs, fxs = -1/(12 dx) (same for z)
     double kx, kz;    // KO strength: -ko/dx/64 (6th difference) or -ko/dx/16 (4th)
     double mu, pmo, ct, st;
+    // KO weights of the symmetric sums s_k = x[-k] + x[+k] and of the centre,
+    // per axis, for the fused stencil of the x-march kernel:
+    //   6th difference: k3 = eps, k2 = -6 eps, k1 = 15 eps, centre -20 (eps_x + eps_z)
+    //   4th difference: k3 = 0,   k2 = eps,    k1 = -4 eps, centre   6 (eps_x + eps_z)
+    double kz3, kz2, kz1, kx3, kx2, kx1, kc;
 };
 
 struct Quad {

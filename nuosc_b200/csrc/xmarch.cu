@@ -1,23 +1,35 @@
 // xmarch.cu -- fused RK4 stage kernel that marches along x.
 //
 // One CTA owns TZ consecutive z rows x 32 consecutive velocities x one flavour
-// half (fields ee,mm,emr,emi or their barred partners) and walks a segment
-// of x planes.  Per thread (one (z, v) column):
-//   * a (2R+1)-deep register queue in x per field holds the stencil in x, so
-//     every state value is read from HBM once per stage (plus the z halo and
+// half (fields ee,mm,emr,emi or their barred partners) and walks a segment of
+// LX x planes.  Per thread (one (z, v) column):
+//   * a (2R+1)-deep register queue in x per field holds the x stencil, so each
+//     state value is read from HBM once per stage (plus the z halo rows and
 //     the 2R planes that prime each segment);
 //   * the centre plane goes through shared memory for the z stencil;
-//   * the inputs of the next plane (queue front, z-halo rows, U and A
-//     registers, cell moments) are staged into a double-buffered shared
-//     pipeline with cp.async while the current plane computes;
+//   * the inputs of the planes ahead (queue front, z-halo rows, the U and A
+//     registers, cell moments) are staged by cp.async into an NS-deep
+//     shared-memory ring, NS-1 planes ahead, with one barrier per plane;
 //   * the epilogue applies the RK-stage update and accumulates the velocity
-//     moments of the state it writes (warp butterfly over the 32 velocities,
-//     one partial per (cell, velocity block, half)); moment_finalize sums the
-//     partials in a fixed order, so the next stage needs no moment pass.
-// The physics is the same as k_stage_direct (physics.cuh); only the data
-// movement differs.  Periodic wrap in x and z is index arithmetic.
+//     moments of the state it writes: a reduce-scatter over the 32
+//     velocities of the warp gives one partial per (cell, velocity block,
+//     half); moment_finalize sums the partials in a fixed order, so the next
+//     stage needs no separate moment pass and results are deterministic.
+// ADV and KO of one field are accumulated as one FMA chain over the symmetric
+// sums x[-k]+x[+k] and differences x[-k]-x[+k]; this reassociates the
+// reference's ADV_FD + KO_FD (nuosc_class.cpp:112-183) at the last-bit level.
+// Periodic wrap in x and z is index arithmetic.
 #include "internal.cuh"
 #include "physics.cuh"
+
+#include <dlfcn.h>
+
+#include <array>
+#include <cstdio>
+#include <cstdlib>
+#include <mutex>
+#include <string>
+#include <vector>
 
 namespace nuosc {
 
@@ -25,9 +37,11 @@ namespace {
 
 constexpr int VB = 32;
 
-__device__ __forceinline__ void cp_async_elem(void *smem, const void *gmem, int bytes) {
+__device__ __forceinline__ void cp_async(void *smem, const void *gmem, int bytes) {
     const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    if (bytes == 8)
+    if (bytes == 16)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+    else if (bytes == 8)
         asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
     else
         asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
@@ -38,30 +52,74 @@ __device__ __forceinline__ void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
-// shared-memory layout of one pipeline stage
+// shared-memory layout of one pipeline stage (all offsets 16-byte aligned)
 template <typename T, int TZ, int R>
 struct Stage {
     static constexpr int ZR = TZ + 2 * R;
-    static constexpr size_t zb = 0;                                   // [4][ZR][VB]  centre plane + z halo
-    static constexpr size_t fr = zb + sizeof(T) * 4 * ZR * VB;        // [4][TZ][VB]  queue front
-    static constexpr size_t ub = fr + sizeof(T) * 4 * TZ * VB;        // [4][TZ][VB]  U
-    static constexpr size_t ab = ub + sizeof(T) * 4 * TZ * VB;        // [4][TZ][VB]  A (accumulator)
-    static constexpr size_t mb = ab + sizeof(T) * 4 * TZ * VB;        // [TZ][12] double, cell moments
+    static constexpr size_t zb = 0;                             // [4][ZR][VB]  centre plane + z halo
+    static constexpr size_t fr = zb + sizeof(T) * 4 * ZR * VB;  // [4][TZ][VB]  queue front
+    static constexpr size_t ub = fr + sizeof(T) * 4 * TZ * VB;  // [4][TZ][VB]  U
+    static constexpr size_t ab = ub + sizeof(T) * 4 * TZ * VB;  // [4][TZ][VB]  A (accumulator)
+    static constexpr size_t mb = ab + sizeof(T) * 4 * TZ * VB;  // [TZ][12] double, cell moments
     static constexpr size_t bytes = mb + sizeof(double) * TZ * NMOM;
+    static_assert(fr % 16 == 0 && mb % 16 == 0 && bytes % 16 == 0, "stage alignment");
 };
 
+// ADV + KO along one axis, accumulated into acc; s[0..2R] = x[-R..+R].
+template <typename T, int R>
+__device__ __forceinline__ T axis_terms(const T (&s)[2 * R + 1], T f, T k3, T k2, T k1, T acc) {
+    constexpr int C = R;
+    const T t2 = s[C - 2] + s[C + 2], t1 = s[C - 1] + s[C + 1];
+    const T d2 = s[C - 2] - s[C + 2], d1 = s[C - 1] - s[C + 1];
+    if (R == 3) acc = fma(k3, s[0] + s[6], acc);
+    acc = fma(k2, t2, acc);
+    acc = fma(k1, t1, acc);
+    return fma(f, fma(T(-8), d1, d2), acc);
+}
+
+// commutator + vacuum terms of one flavour half on top of the stencil sum
 template <typename T>
-__device__ __forceinline__ long long off3(int x, int z, int v, const Geom &g) {
-    return ((long long)x * g.nz + z) * g.nvs + v;
+__device__ __forceinline__ void rhs_half(const T (&c)[4], T a, T b, T e, T mu, T pmo, T ct, T st, T (&sten)[4],
+                                         T (&out)[4]) {
+    const T ee = c[0], mm = c[1], emr = c[2], emi = c[3];
+    const T Iee = T(2) * mu * (emi * a + emr * b);
+    const T Iemr = -mu * ((ee - mm) * b + e * emi);
+    const T Iemi = mu * ((mm - ee) * a + e * emr);
+    out[0] = Iee + sten[0] - pmo * T(2) * st * emi;
+    out[1] = -Iee + sten[1] + pmo * T(2) * st * emi;
+    out[2] = Iemr + sten[2] - pmo * T(2) * ct * emi;
+    out[3] = Iemi + sten[3] + pmo * (T(2) * ct * emr + st * (ee - mm));
+}
+
+// one reduce-scatter step over lane pairs (lane, lane^O): N values -> N/2
+template <int N, int O>
+__device__ __forceinline__ void rs_step(double (&m)[16], int lane) {
+    const bool up = (lane & O) != 0;
+#pragma unroll
+    for (int i = 0; i < N / 2; ++i) {
+        const double send = up ? m[i] : m[i + N / 2];
+        const double keep = up ? m[i + N / 2] : m[i];
+        m[i] = keep + __shfl_xor_sync(0xffffffffu, send, O);
+    }
 }
 
 }  // namespace
 
-template <typename T, int R, int MODE, int TZ>
-__global__ void __launch_bounds__(VB *TZ, 1) k_xmarch(StageArgs<T> a, int LX) {
+// CTAs per SM the tile is built for: 8-row tiles run two independent CTAs per
+// SM so one computes while the other waits at its per-plane barrier.
+template <int TZ>
+constexpr int ctas_per_sm() {
+    return TZ == 8 ? 2 : 1;
+}
+
+template <typename T, int R, int MODE, int TZ, int NS>
+__global__ void __launch_bounds__(VB *TZ, ctas_per_sm<TZ>()) k_xmarch(StageArgs<T> a, int LX) {
     using S = Stage<T, TZ, R>;
     constexpr int W = 2 * R + 1;
     constexpr int ZR = S::ZR;
+    constexpr int D = NS - 1;                 // planes staged ahead
+    constexpr int NHR = 4 * 2 * R;            // z-halo rows per plane (4 fields)
+    constexpr int NH = (NHR + TZ - 1) / TZ;   // halo rows per warp
     extern __shared__ __align__(16) unsigned char smem[];
 
     const Geom g = a.g;
@@ -72,184 +130,195 @@ __global__ void __launch_bounds__(VB *TZ, 1) k_xmarch(StageArgs<T> a, int LX) {
     const bool vact = v < g.nvs;
     const int seg = blockIdx.z >> 1, half = blockIdx.z & 1;
     const int xs = seg * LX;
-    const int xe = min(xs + LX, g.nx);
     if (xs >= g.nx) return;
+    const int xe = min(xs + LX, g.nx);
     const int zr = z0 + r;
     const bool zact = zr < g.nz;
-    const int zl = wrap_index(zr, g.nz);
+    const bool act = vact && zact;
     const long long fs = g.fs;
+    const long long P = (long long)g.nz * g.nvs;  // elements per x plane of one field
     const long long hoff = (long long)half * 4 * fs;
     const T *in = a.in + hoff;
-    const T *u = a.u ? a.u + hoff : nullptr;
-    const T *accs = a.acc_src ? a.acc_src + hoff : nullptr;
-    T *accd = a.acc_dst + hoff;
-    T *yd = a.y_dst ? a.y_dst + hoff : nullptr;
+    const int vc = vact ? v : 0;
+    const long long own_ld = (long long)wrap_index(zr, g.nz) * g.nvs + vc;  // this column (wrapped) for loads
+    const long long own_st = (long long)(zact ? zr : 0) * g.nvs + vc;       // this column for U/A and stores
     const int nvb = gridDim.y;
 
+    // z-halo rows staged by this warp (plane-independent part of the address)
+    long long h_off[NH];
+    int h_sm[NH];
+    bool h_ok[NH];
+#pragma unroll
+    for (int k = 0; k < NH; ++k) {
+        const int hrow = r + k * TZ;
+        h_ok[k] = vact && hrow < NHR;
+        const int f = hrow / (2 * R), hr = hrow - f * (2 * R);
+        const int kb = hr < R ? hr : TZ + hr;
+        h_off[k] = f * fs + (long long)wrap_index(z0 - R + kb, g.nz) * g.nvs + vc;
+        h_sm[k] = (f * ZR + kb) * VB + lane;
+    }
+    // cell moments of the TZ rows: threads tid < TZ*6 copy 16 bytes each
+    const bool m_ok = tid < TZ * NMOM / 2 && z0 + (2 * tid) / NMOM < g.nz;
+    const long long m_off = (long long)z0 * NMOM + 2 * tid;
+
     // per-velocity constants (constant along the march)
-    const int vc = vact ? v : 0;
     const double vxd = a.q.vx[vc], vyd = a.q.vy[vc], vzd = a.q.vz[vc], wd = vact ? a.q.vw[vc] : 0.0;
     const T fx = T(vxd * a.c.fxs), fz = T(vzd * a.c.fzs);
-    const T kx = T(a.c.kx), kz = T(a.c.kz);
-    const double v4w[4] = {wd, vxd * wd, vyd * wd, vzd * wd};
+    const T kz3 = T(a.c.kz3), kz2 = T(a.c.kz2), kz1 = T(a.c.kz1);
+    const T kx3 = T(a.c.kx3), kx2 = T(a.c.kx2), kx1 = T(a.c.kx1), kc = T(a.c.kc);
+    const T mu = T(a.c.mu), pmo = T(a.c.pmo), ct = T(a.c.ct), st = T(a.c.st);
     const T cA = T(a.cA), cY = T(a.cY);
 
-    auto stage_ptr = [&](int b) { return smem + (size_t)b * S::bytes; };
-
-    // issue the copies for the plane with centre xn into buffer b
     auto issue = [&](int xn, int b) {
-        unsigned char *st = stage_ptr(b);
-        T *zb = (T *)(st + S::zb);
-        T *fr = (T *)(st + S::fr);
-        T *ubuf = (T *)(st + S::ub);
-        T *abuf = (T *)(st + S::ab);
-        double *mb = (double *)(st + S::mb);
-        const int xf = wrap_index(xn + R, g.nx);
+        unsigned char *sp = smem + (size_t)b * S::bytes;
+        T *zb = (T *)(sp + S::zb);
+        T *fr = (T *)(sp + S::fr);
+        T *ubuf = (T *)(sp + S::ub);
+        T *abuf = (T *)(sp + S::ab);
+        double *mb = (double *)(sp + S::mb);
+        const int xf = xn + R < g.nx ? xn + R : xn + R - g.nx;
+        const long long xo = (long long)xn * P;
         if (vact) {
-            const long long of = off3<T>(xf, zl, v, g);
+            const T *pf = in + (long long)xf * P + own_ld;
 #pragma unroll
-            for (int f = 0; f < 4; ++f) cp_async_elem(&fr[(f * TZ + r) * VB + lane], in + f * fs + of, sizeof(T));
-            if (zact && MODE != MODE_S1) {
-                const long long oc = off3<T>(xn, zr, v, g);
+            for (int f = 0; f < 4; ++f) cp_async(&fr[(f * TZ + r) * VB + lane], pf + f * fs, sizeof(T));
+            if (MODE != MODE_S1 && zact) {
+                const long long oc = hoff + xo + own_st;
 #pragma unroll
                 for (int f = 0; f < 4; ++f) {
-                    if (MODE == MODE_S23) cp_async_elem(&ubuf[(f * TZ + r) * VB + lane], u + f * fs + oc, sizeof(T));
-                    cp_async_elem(&abuf[(f * TZ + r) * VB + lane], accs + f * fs + oc, sizeof(T));
+                    if (MODE == MODE_S23) cp_async(&ubuf[(f * TZ + r) * VB + lane], a.u + oc + f * fs, sizeof(T));
+                    cp_async(&abuf[(f * TZ + r) * VB + lane], a.acc_src + oc + f * fs, sizeof(T));
                 }
             }
         }
-        // z-halo rows of plane xn: buffer rows [0,R) and [R+TZ, ZR)
-        for (int h = tid; h < 4 * 2 * R * VB; h += VB * TZ) {
-            const int f = h / (2 * R * VB), rem = h - f * (2 * R * VB);
-            const int hr = rem / VB, hl = rem - hr * VB;
-            const int k = hr < R ? hr : TZ + hr;
-            const int vv = vb * VB + hl;
-            if (vv < g.nvs) {
-                const int zg = wrap_index(z0 - R + k, g.nz);
-                cp_async_elem(&zb[(f * ZR + k) * VB + hl], in + f * fs + off3<T>(xn, zg, vv, g), sizeof(T));
-            }
-        }
-        // moments of the TZ cells of plane xn
-        for (int e = tid; e < TZ * NMOM; e += VB * TZ) {
-            const int row = e / NMOM;
-            if (z0 + row < g.nz)
-                cp_async_elem(&mb[e], a.mom_in + ((long long)xn * g.nz + z0) * NMOM + e, 8);
-        }
+#pragma unroll
+        for (int k = 0; k < NH; ++k)
+            if (h_ok[k]) cp_async(&zb[h_sm[k]], in + h_off[k] + xo, sizeof(T));
+        if (m_ok) cp_async(&mb[2 * tid], a.mom_in + (long long)xn * g.nz * NMOM + m_off, 16);
     };
 
-    // prime the queue with planes xs-R .. xs+R-1 and stage the first plane
+    // prime the queue with planes xs-R .. xs+R-1 and stage the first D planes
     T q[4][W];
 #pragma unroll
     for (int p = 0; p < 2 * R; ++p) {
-        const int xp = wrap_index(xs - R + p, g.nx);
-        const long long o = off3<T>(xp, zl, v, g);
+        const long long o = (long long)wrap_index(xs - R + p, g.nx) * P + own_ld;
 #pragma unroll
         for (int f = 0; f < 4; ++f) q[f][p] = vact ? in[f * fs + o] : T(0);
     }
-    issue(xs, 0);
-    cp_async_commit();
-
-    for (int x = xs; x < xe; ++x) {
-        const int b = (x - xs) & 1;
-        if (x + 1 < xe) issue(x + 1, b ^ 1);
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+        if (xs + d < xe) issue(xs + d, d);
         cp_async_commit();
-        cp_async_wait<1>();
+    }
 
-        unsigned char *st = stage_ptr(b);
-        T *zb = (T *)(st + S::zb);
-        const T *fr = (const T *)(st + S::fr);
-        const T *ubuf = (const T *)(st + S::ub);
-        const T *abuf = (const T *)(st + S::ab);
-        const double *mb = (const double *)(st + S::mb);
+    int bi = 0;  // ring slot of plane x
+    for (int x = xs; x < xe; ++x) {
+        cp_async_wait<D - 1>();
+        unsigned char *sp = smem + (size_t)bi * S::bytes;
+        T *zb = (T *)(sp + S::zb);
+        const T *fr = (const T *)(sp + S::fr);
+        const T *ubuf = (const T *)(sp + S::ub);
+        const T *abuf = (const T *)(sp + S::ab);
+        const double *mb = (const double *)(sp + S::mb);
 #pragma unroll
         for (int f = 0; f < 4; ++f) {
             q[f][2 * R] = vact ? fr[(f * TZ + r) * VB + lane] : T(0);
             zb[(f * ZR + R + r) * VB + lane] = q[f][R];
         }
         __syncthreads();
+        {
+            int bn = bi + D;
+            if (bn >= NS) bn -= NS;
+            if (x + D < xe) issue(x + D, bn);
+            cp_async_commit();
+        }
 
-        // stencil: z from the shared centre plane, x from the register queue
-        T cen[4], adv[4], ko[4];
+        // stencil sums: z from the shared centre plane, x from the register queue
+        T sten[4], cen[4];
 #pragma unroll
         for (int f = 0; f < 4; ++f) {
-            T zs[7], xq[7];
+            T zs[W];
 #pragma unroll
-            for (int k = 0; k < 7; ++k) {
-                const int kk = k - 3;
-                if (kk >= -R && kk <= R) {
-                    zs[k] = zb[(f * ZR + r + R + kk) * VB + lane];
-                    xq[k] = q[f][R + kk];
-                } else {
-                    zs[k] = T(0);
-                    xq[k] = T(0);
-                }
-            }
+            for (int k = 0; k < W; ++k) zs[k] = zb[(f * ZR + r + k) * VB + lane];
             cen[f] = q[f][R];
-            adv[f] = adv_axis(zs, fz) + adv_axis(xq, fx);
-            ko[f] = ko_axis<T, R == 3>(zs, kz) + ko_axis<T, R == 3>(xq, kx);
+            T acc = kc * cen[f];
+            acc = axis_terms<T, R>(zs, fz, kz3, kz2, kz1, acc);
+            sten[f] = axis_terms<T, R>(q[f], fx, kx3, kx2, kx1, acc);
         }
-        const double *m = mb + r * NMOM;
+        double m[NMOM];
+        {
+            const double2 *m2 = (const double2 *)(mb + r * NMOM);
+#pragma unroll
+            for (int k = 0; k < NMOM / 2; ++k) {
+                const double2 t = m2[k];
+                m[2 * k] = t.x;
+                m[2 * k + 1] = t.y;
+            }
+        }
         const T ia = T(inp(m, vxd, vyd, vzd)), ib = T(inp(m + 4, vxd, vyd, vzd)), ie = T(inp(m + 8, vxd, vyd, vzd));
-        T kk4[4];
-        commutator_half(cen, ia, ib, ie, a.c, kk4, adv, ko);
+        T kk[4];
+        rhs_half(cen, ia, ib, ie, mu, pmo, ct, st, sten, kk);
 
         // RK-stage epilogue
         T outm[4];
-        const bool act = vact && zact;
-        const long long oc = off3<T>(x, zact ? zr : 0, v, g);
+        const long long oc = hoff + (long long)x * P + own_st;
 #pragma unroll
         for (int f = 0; f < 4; ++f) {
             if (MODE == MODE_S1) {
-                const T A = cen[f] + cA * kk4[f];
-                const T Y = cen[f] + cY * kk4[f];
+                const T A = cen[f] + cA * kk[f];
+                const T Y = cen[f] + cY * kk[f];
                 if (act) {
-                    accd[f * fs + oc] = A;
-                    yd[f * fs + oc] = Y;
+                    a.acc_dst[oc + f * fs] = A;
+                    a.y_dst[oc + f * fs] = Y;
                 }
                 outm[f] = Y;
             } else if (MODE == MODE_S23) {
-                const T A = abuf[(f * TZ + r) * VB + lane] + cA * kk4[f];
-                const T Y = ubuf[(f * TZ + r) * VB + lane] + cY * kk4[f];
+                const T A = abuf[(f * TZ + r) * VB + lane] + cA * kk[f];
+                const T Y = ubuf[(f * TZ + r) * VB + lane] + cY * kk[f];
                 if (act) {
-                    accd[f * fs + oc] = A;
-                    yd[f * fs + oc] = Y;
+                    a.acc_dst[oc + f * fs] = A;
+                    a.y_dst[oc + f * fs] = Y;
                 }
                 outm[f] = Y;
             } else {
-                const T A = abuf[(f * TZ + r) * VB + lane] + cA * kk4[f];
-                if (act) accd[f * fs + oc] = A;
+                const T A = abuf[(f * TZ + r) * VB + lane] + cA * kk[f];
+                if (act) a.acc_dst[oc + f * fs] = A;
                 outm[f] = A;
             }
         }
+
         // velocity-moment partials of the written state (nuosc_class.cpp:69-71)
-        double d0, d1, d2;
-        if (half == 0) moment_terms<false>(outm[0], outm[1], outm[2], outm[3], d0, d1, d2);
-        else moment_terms<true>(outm[0], outm[1], outm[2], outm[3], d0, d1, d2);
-        double mp[NMOM];
+        {
+            double d0, d1, d2;
+            if (half == 0) moment_terms<false>(outm[0], outm[1], outm[2], outm[3], d0, d1, d2);
+            else moment_terms<true>(outm[0], outm[1], outm[2], outm[3], d0, d1, d2);
+            if (!act) d0 = d1 = d2 = 0.0;
+            const double v4w[4] = {wd, vxd * wd, vyd * wd, vzd * wd};
+            double mp[16];
 #pragma unroll
-        for (int s = 0; s < 4; ++s) {
-            mp[s] = act ? v4w[s] * d0 : 0.0;
-            mp[4 + s] = act ? v4w[s] * d1 : 0.0;
-            mp[8 + s] = act ? v4w[s] * d2 : 0.0;
-        }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1)
-#pragma unroll
-            for (int k = 0; k < NMOM; ++k) mp[k] += __shfl_xor_sync(0xffffffffu, mp[k], o);
-        if (zact && lane < NMOM) {
-            double val = mp[0];
-#pragma unroll
-            for (int k = 1; k < NMOM; ++k)
-                if (lane == k) val = mp[k];
-            const long long cell = (long long)x * g.nz + zr;
-            a.mom_part[((cell * nvb + vb) * 2 + half) * NMOM + lane] = val;
+            for (int s = 0; s < 4; ++s) {
+                mp[s] = v4w[s] * d0;
+                mp[4 + s] = v4w[s] * d1;
+                mp[8 + s] = v4w[s] * d2;
+                mp[12 + s] = 0.0;
+            }
+            rs_step<16, 16>(mp, lane);
+            rs_step<8, 8>(mp, lane);
+            rs_step<4, 4>(mp, lane);
+            rs_step<2, 2>(mp, lane);
+            mp[0] += __shfl_xor_sync(0xffffffffu, mp[0], 1);
+            const int idx = lane >> 1;  // lanes 2k, 2k+1 hold moment k
+            if (zact && (lane & 1) == 0 && idx < NMOM) {
+                const long long cell = (long long)x * g.nz + zr;
+                a.mom_part[((cell * nvb + vb) * 2 + half) * NMOM + idx] = mp[0];
+            }
         }
 
 #pragma unroll
         for (int f = 0; f < 4; ++f)
 #pragma unroll
             for (int k = 0; k < 2 * R; ++k) q[f][k] = q[f][k + 1];
-        __syncthreads();
+        bi = bi + 1 == NS ? 0 : bi + 1;
     }
     cp_async_wait<0>();
 }
@@ -272,22 +341,28 @@ int xmarch_num_vblocks(const Geom &g, XTile) { return (g.nvs + VB - 1) / VB; }
 
 template <typename T>
 bool xmarch_supported(const Geom &g, bool, XTile t) {
-    return (t.tz == 8 || t.tz == 16) && t.lx >= 1 && t.vb == VB && g.nx >= 1 && g.nz >= 1;
+    return (t.tz == 8 || t.tz == 16) && t.lx >= 1 && t.vb == VB && g.nx >= 4 && g.nz >= 1;
 }
 
 namespace {
 
+// deepest ring (3 or 2 planes) that lets ctas_per_sm CTAs share the SM's 228 KB
+template <typename T, int TZ, int R>
+constexpr int ring_depth() {
+    return ctas_per_sm<TZ>() * (3 * Stage<T, TZ, R>::bytes + 1024) <= 228 * 1024 ? 3 : 2;
+}
+
 template <typename T, int R, int MODE, int TZ>
 cudaError_t launch_x(const StageArgs<T> &a, XTile t, cudaStream_t s) {
-    using St = Stage<T, TZ, R>;
-    const size_t smem = 2 * St::bytes;
-    cudaError_t e = cudaFuncSetAttribute(k_xmarch<T, R, MODE, TZ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    constexpr int NS = ring_depth<T, TZ, R>();
+    const size_t smem = NS * Stage<T, TZ, R>::bytes;
+    cudaError_t e = cudaFuncSetAttribute(k_xmarch<T, R, MODE, TZ, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e != cudaSuccess) return e;
     const int nseg = (a.g.nx + t.lx - 1) / t.lx;
     dim3 grid((a.g.nz + TZ - 1) / TZ, (a.g.nvs + VB - 1) / VB, nseg * 2);
     dim3 block(VB, TZ);
-    k_xmarch<T, R, MODE, TZ><<<grid, block, smem, s>>>(a, t.lx);
+    k_xmarch<T, R, MODE, TZ, NS><<<grid, block, smem, s>>>(a, t.lx);
     return cudaGetLastError();
 }
 
@@ -321,11 +396,35 @@ template bool xmarch_supported<float>(const Geom &, bool, XTile);
 template cudaError_t launch_stage_xmarch<double>(const StageArgs<double> &, int, bool, XTile, cudaStream_t);
 template cudaError_t launch_stage_xmarch<float>(const StageArgs<float> &, int, bool, XTile, cudaStream_t);
 
-// Tile table keyed on (velocity count, precision), written by the autotuner
-// (nuosc_b200/autotune.py); shapes not listed use the default.
+// Tile table keyed on (velocity count, precision): lines "nv precision tz lx"
+// in tiles.txt beside the library (or the file named by NUOSC_TILES), written
+// by the autotuner nuosc_b200/autotune.py.  Shapes not listed use 16 x 128.
 XTile autotune_lookup(int nv, int precision) {
-    (void)nv;
-    (void)precision;
+    static std::vector<std::array<int, 4>> table;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        std::string path;
+        if (const char *env = getenv("NUOSC_TILES")) {
+            path = env;
+        } else {
+            Dl_info info;
+            if (dladdr((void *)&autotune_lookup, &info) && info.dli_fname) {
+                path = info.dli_fname;
+                const size_t slash = path.rfind('/');
+                path = (slash == std::string::npos ? std::string(".") : path.substr(0, slash)) + "/tiles.txt";
+            }
+        }
+        FILE *f = path.empty() ? nullptr : fopen(path.c_str(), "r");
+        if (!f) return;
+        char line[256];
+        while (fgets(line, sizeof line, f)) {
+            std::array<int, 4> e;
+            if (line[0] != '#' && sscanf(line, "%d %d %d %d", &e[0], &e[1], &e[2], &e[3]) == 4) table.push_back(e);
+        }
+        fclose(f);
+    });
+    for (const auto &e : table)
+        if (e[0] == nv && e[1] == precision && (e[2] == 8 || e[2] == 16) && e[3] >= 1) return XTile{e[2], e[3], VB};
     return XTile{16, 128, VB};
 }
 

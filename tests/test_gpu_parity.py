@@ -182,6 +182,34 @@ def test_odd_sizes_against_oracle(nb, n, nn, kernel):
         assert po.relerr(a[f], b[f]) < FP64_TOL, f
 
 
+@pytest.mark.parametrize("ko_order", [6, 4])
+def test_xmarch_tiles_bit_identical(nb, ko_order):
+    """Every x-march tile shape gives the same bits (moment partials are reduced
+    per 32-velocity block in a fixed order, independent of the tile), and the
+    result matches the oracle."""
+    p = box_params(40, 4)
+    ref_bits = None
+    for tz, lx in ((16, 128), (8, 128), (16, 7), (8, 1), (16, 40), (8, 13)):
+        s = make(nb, p, ko_order)
+        s.fillInitValue(1, seed=5, alpha=1.2, eps0=1e-3, sigma=1.0, lnue=0.6, lnueb=0.4)
+        s.set_kernel(nb.KERNEL_XMARCH)
+        s.set_tile(tz, lx)
+        s.step_rk4(6)
+        st = s.get_state()
+        if ref_bits is None:
+            ref_bits = st
+            o = po.Oracle(nn=4, x0=p[0], x1=p[1], z0=p[0], z1=p[1], dx=0.1, dz=0.1, cfl=0.4, ko=0.1,
+                          ko_order=ko_order)
+            o.fill_init(ipt=1, seed=5, alpha=1.2, eps0=1e-3, sigma=1.0, lnue=0.6, lnueb=0.4)
+            o.step(6)
+            ref = o.get_state(0)
+            for f in range(8):
+                assert po.relerr(st[f], ref[f]) < FP64_TOL, f
+        else:
+            assert np.array_equal(st, ref_bits), (tz, lx)
+        s.close()
+
+
 def test_state_roundtrip_layouts(nb):
     p = box_params(8, 2)
     for prec in (nb.FP64, nb.FP32):
