@@ -124,7 +124,7 @@ int nuosc_set_pmo(nuosc_handle *h, double pmo);
 int nuosc_set_renorm(nuosc_handle *h, int renorm);
 /* stage-kernel choice (NUOSC_KERNEL_*); no counterpart in the reference */
 int nuosc_set_kernel(nuosc_handle *h, int kind);
-/* x-march tile: tz z-rows per CTA (8 or 16) and lx x-planes marched per CTA.
+/* x-march tile: tz z-rows per CTA (4, 8 or 16) and lx x-planes marched per CTA.
  * The default comes from the autotuner's table (tiles.txt beside the
  * library, keyed on velocity count and precision).  No reference counterpart. */
 int nuosc_set_tile(nuosc_handle *h, int tz, int lx);

@@ -3,7 +3,7 @@
     python -m nuosc_b200.autotune --nn 8 --precision 0 --size 1024 [--write]
 
 For one (velocity count, precision) it times full RK4 steps for every
-candidate tile (tz z-rows per CTA in {8, 16}, lx x-planes per CTA) with CUDA
+candidate tile (tz z-rows per CTA in {4, 8, 16}, lx x-planes per CTA) with CUDA
 events on the solver's stream, and with --write records the fastest in
 nuosc_b200/tiles.txt ("nv precision tz lx" per line), which the library reads
 when a handle is created.  The direct kernel is timed too, for reference.
@@ -48,7 +48,7 @@ def tune(nn, precision, size, steps=3, warmup=2, lx_list=DEFAULT_LX, device=0, k
     ms = time_steps(s, stream, steps, warmup)
     results.append({"kernel": "direct", "ms_per_step": ms, "cell_steps_per_s": cells / ms * 1e3})
     s.set_kernel(nb.KERNEL_XMARCH)
-    for tz in (8, 16):
+    for tz in (4, 8, 16):
         for lx in lx_list:
             lx = min(lx, s.grid.nx)
             if any(r.get("tz") == tz and r.get("lx") == lx for r in results):

@@ -637,7 +637,8 @@ int nuosc_set_kernel(nuosc_handle *h, int kind) {
 }
 int nuosc_set_tile(nuosc_handle *h, int tz, int lx) {
     if (!h) return fail(NUOSC_ERR_INVALID, "null handle");
-    if ((tz != 8 && tz != 16) || lx < 1) return fail(NUOSC_ERR_INVALID, "tile tz=%d lx=%d (tz 8 or 16, lx >= 1)", tz, lx);
+    if ((tz != 4 && tz != 8 && tz != 16) || lx < 1)
+        return fail(NUOSC_ERR_INVALID, "tile tz=%d lx=%d (tz 4, 8 or 16, lx >= 1)", tz, lx);
     const int nvb_old = xmarch_num_vblocks(h->g, h->tile);
     h->tile.tz = tz;
     h->tile.lx = lx;

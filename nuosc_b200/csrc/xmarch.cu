@@ -52,15 +52,17 @@ __device__ __forceinline__ void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
-// shared-memory layout of one pipeline stage (all offsets 16-byte aligned)
-template <typename T, int TZ, int R>
+// shared-memory layout of one pipeline stage (all offsets 16-byte aligned);
+// S1 stages no U or A, S4 no U
+template <typename T, int TZ, int R, int MODE>
 struct Stage {
     static constexpr int ZR = TZ + 2 * R;
-    static constexpr size_t zb = 0;                             // [4][ZR][VB]  centre plane + z halo
-    static constexpr size_t fr = zb + sizeof(T) * 4 * ZR * VB;  // [4][TZ][VB]  queue front
-    static constexpr size_t ub = fr + sizeof(T) * 4 * TZ * VB;  // [4][TZ][VB]  U
-    static constexpr size_t ab = ub + sizeof(T) * 4 * TZ * VB;  // [4][TZ][VB]  A (accumulator)
-    static constexpr size_t mb = ab + sizeof(T) * 4 * TZ * VB;  // [TZ][12] double, cell moments
+    static constexpr size_t plane = sizeof(T) * 4 * TZ * VB;
+    static constexpr size_t zb = 0;                                        // [4][ZR][VB] centre plane + z halo
+    static constexpr size_t fr = zb + sizeof(T) * 4 * ZR * VB;             // [4][TZ][VB] queue front
+    static constexpr size_t ub = fr + plane;                               // [4][TZ][VB] U       (S2/S3)
+    static constexpr size_t ab = ub + (MODE == MODE_S23 ? plane : 0);      // [4][TZ][VB] A       (S2/S3/S4)
+    static constexpr size_t mb = ab + (MODE != MODE_S1 ? plane : 0);       // [TZ][12] double, cell moments
     static constexpr size_t bytes = mb + sizeof(double) * TZ * NMOM;
     static_assert(fr % 16 == 0 && mb % 16 == 0 && bytes % 16 == 0, "stage alignment");
 };
@@ -105,16 +107,17 @@ __device__ __forceinline__ void rs_step(double (&m)[16], int lane) {
 
 }  // namespace
 
-// CTAs per SM the tile is built for: 8-row tiles run two independent CTAs per
-// SM so one computes while the other waits at its per-plane barrier.
+// CTAs per SM the tile is built for: 8-row tiles run two, 4-row tiles four
+// independent CTAs per SM, so some compute while others wait at their
+// per-plane barrier.
 template <int TZ>
 constexpr int ctas_per_sm() {
-    return TZ == 8 ? 2 : 1;
+    return TZ == 4 ? 4 : TZ == 8 ? 2 : 1;
 }
 
 template <typename T, int R, int MODE, int TZ, int NS>
 __global__ void __launch_bounds__(VB *TZ, ctas_per_sm<TZ>()) k_xmarch(StageArgs<T> a, int LX) {
-    using S = Stage<T, TZ, R>;
+    using S = Stage<T, TZ, R, MODE>;
     constexpr int W = 2 * R + 1;
     constexpr int ZR = S::ZR;
     constexpr int D = NS - 1;                 // planes staged ahead
@@ -341,21 +344,22 @@ int xmarch_num_vblocks(const Geom &g, XTile) { return (g.nvs + VB - 1) / VB; }
 
 template <typename T>
 bool xmarch_supported(const Geom &g, bool, XTile t) {
-    return (t.tz == 8 || t.tz == 16) && t.lx >= 1 && t.vb == VB && g.nx >= 4 && g.nz >= 1;
+    return (t.tz == 4 || t.tz == 8 || t.tz == 16) && t.lx >= 1 && t.vb == VB && g.nx >= 4 && g.nz >= 1;
 }
 
 namespace {
 
-// deepest ring (3 or 2 planes) that lets ctas_per_sm CTAs share the SM's 228 KB
-template <typename T, int TZ, int R>
+// deepest ring (4, 3 or 2 planes) that lets ctas_per_sm CTAs share the SM's 228 KB
+template <typename T, int TZ, int R, int MODE>
 constexpr int ring_depth() {
-    return ctas_per_sm<TZ>() * (3 * Stage<T, TZ, R>::bytes + 1024) <= 228 * 1024 ? 3 : 2;
+    constexpr size_t b = Stage<T, TZ, R, MODE>::bytes, cap = 228 * 1024;
+    return ctas_per_sm<TZ>() * (4 * b + 1024) <= cap ? 4 : ctas_per_sm<TZ>() * (3 * b + 1024) <= cap ? 3 : 2;
 }
 
 template <typename T, int R, int MODE, int TZ>
 cudaError_t launch_x(const StageArgs<T> &a, XTile t, cudaStream_t s) {
-    constexpr int NS = ring_depth<T, TZ, R>();
-    const size_t smem = NS * Stage<T, TZ, R>::bytes;
+    constexpr int NS = ring_depth<T, TZ, R, MODE>();
+    const size_t smem = NS * Stage<T, TZ, R, MODE>::bytes;
     cudaError_t e = cudaFuncSetAttribute(k_xmarch<T, R, MODE, TZ, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e != cudaSuccess) return e;
@@ -382,7 +386,8 @@ template <typename T>
 cudaError_t launch_stage_xmarch(const StageArgs<T> &a, int mode, bool ko6, XTile t, cudaStream_t s) {
     if (!a.mom_part) return cudaErrorInvalidValue;
     if (t.tz == 16) return ko6 ? launch_mode<T, 3, 16>(a, mode, t, s) : launch_mode<T, 2, 16>(a, mode, t, s);
-    return ko6 ? launch_mode<T, 3, 8>(a, mode, t, s) : launch_mode<T, 2, 8>(a, mode, t, s);
+    if (t.tz == 8) return ko6 ? launch_mode<T, 3, 8>(a, mode, t, s) : launch_mode<T, 2, 8>(a, mode, t, s);
+    return ko6 ? launch_mode<T, 3, 4>(a, mode, t, s) : launch_mode<T, 2, 4>(a, mode, t, s);
 }
 
 cudaError_t launch_moment_finalize(const double *part, double *mom, Geom g, int nvb, cudaStream_t s) {
@@ -424,7 +429,7 @@ XTile autotune_lookup(int nv, int precision) {
         fclose(f);
     });
     for (const auto &e : table)
-        if (e[0] == nv && e[1] == precision && (e[2] == 8 || e[2] == 16) && e[3] >= 1) return XTile{e[2], e[3], VB};
+        if (e[0] == nv && e[1] == precision && (e[2] == 4 || e[2] == 8 || e[2] == 16) && e[3] >= 1) return XTile{e[2], e[3], VB};
     return XTile{16, 128, VB};
 }
 
