@@ -68,9 +68,10 @@ extern "C" {
 #define NUOSC_LAYOUT_GHOSTED 1 /* the reference's array: [(i+gx)*(nz+2gz)+j+gz]*nv+v (CartGrid.h:91) */
 
 /* stage-kernel selection (nuosc_set_kernel) */
-#define NUOSC_KERNEL_AUTO 0   /* the fused x-march kernel when the geometry allows, else direct */
+#define NUOSC_KERNEL_AUTO 0   /* the TMA x-march kernel when the geometry allows, else the cp.async one */
 #define NUOSC_KERNEL_DIRECT 1 /* one thread per (cell, velocity), separate moment pass */
-#define NUOSC_KERNEL_XMARCH 2 /* bulk-copy staged x-march with fused moments */
+#define NUOSC_KERNEL_XMARCH 2 /* cp.async-staged x-march with fused moments (any geometry) */
+#define NUOSC_KERNEL_XTMA 3   /* TMA-fed x-march with mbarrier ring, fused moments (nz % tz == 0) */
 
 typedef struct nuosc_handle nuosc_handle;
 

@@ -21,11 +21,11 @@ import math
 import numpy as np
 
 from . import _lib
-from ._lib import (FP32, FP64, KERNEL_AUTO, KERNEL_DIRECT, KERNEL_XMARCH, LAYOUT_COMPACT, LAYOUT_GHOSTED,
-                   REG_COR, REG_PRE, REG_RHS, REG_STAT, FIELDS, NuoscError, check, lib)
+from ._lib import (FP32, FP64, KERNEL_AUTO, KERNEL_DIRECT, KERNEL_XMARCH, KERNEL_XTMA, LAYOUT_COMPACT,
+                   LAYOUT_GHOSTED, REG_COR, REG_PRE, REG_RHS, REG_STAT, FIELDS, NuoscError, check, lib)
 
 __all__ = ["NuOsc", "NuoscError", "FP32", "FP64", "REG_STAT", "REG_RHS", "REG_PRE", "REG_COR",
-           "KERNEL_AUTO", "KERNEL_DIRECT", "KERNEL_XMARCH", "FIELDS", "lib"]
+           "KERNEL_AUTO", "KERNEL_DIRECT", "KERNEL_XMARCH", "KERNEL_XTMA", "FIELDS", "lib"]
 
 lib()  # fail at import time if the CUDA library is missing
 

@@ -13,7 +13,7 @@ OK, ERR_INVALID, ERR_CUDA, ERR_OOM, ERR_NUMERIC, ERR_TIMEOUT, ERR_UNSUPPORTED = 
 FP64, FP32 = 0, 1
 REG_STAT, REG_RHS, REG_PRE, REG_COR = 0, 1, 2, 3
 LAYOUT_COMPACT, LAYOUT_GHOSTED = 0, 1
-KERNEL_AUTO, KERNEL_DIRECT, KERNEL_XMARCH = 0, 1, 2
+KERNEL_AUTO, KERNEL_DIRECT, KERNEL_XMARCH, KERNEL_XTMA = 0, 1, 2, 3
 FIELDS = ["ee", "mm", "emr", "emi", "bee", "bmm", "bemr", "bemi",
           "P1", "P2", "P3", "P1b", "P2b", "P3b", "dP", "dPb"]
 

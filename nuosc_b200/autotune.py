@@ -47,34 +47,39 @@ def tune(nn, precision, size, steps=3, warmup=2, lx_list=DEFAULT_LX, device=0, k
     s.set_kernel(nb.KERNEL_DIRECT)
     ms = time_steps(s, stream, steps, warmup)
     results.append({"kernel": "direct", "ms_per_step": ms, "cell_steps_per_s": cells / ms * 1e3})
-    s.set_kernel(nb.KERNEL_XMARCH)
-    for tz in (4, 8, 16):
-        for lx in lx_list:
-            lx = min(lx, s.grid.nx)
-            if any(r.get("tz") == tz and r.get("lx") == lx for r in results):
+    for kind, name, tzs in ((nb.KERNEL_XTMA, "xtma", (8, 16)), (nb.KERNEL_XMARCH, "xmarch", (4, 8, 16))):
+        s.set_kernel(kind)
+        for tz in tzs:
+            if kind == nb.KERNEL_XTMA and s.grid.nz % tz:
                 continue
-            s.set_tile(tz, lx)
-            ms = time_steps(s, stream, steps, warmup)
-            results.append({"kernel": "xmarch", "tz": tz, "lx": lx, "ms_per_step": ms,
-                            "cell_steps_per_s": cells / ms * 1e3})
+            for lx in lx_list:
+                lx = min(lx, s.grid.nx)
+                if any(r["kernel"] == name and r.get("tz") == tz and r.get("lx") == lx for r in results):
+                    continue
+                s.set_tile(tz, lx)
+                ms = time_steps(s, stream, steps, warmup)
+                results.append({"kernel": name, "kind": kind, "tz": tz, "lx": lx, "ms_per_step": ms,
+                                "cell_steps_per_s": cells / ms * 1e3})
     s.close()
-    best = min((r for r in results if r["kernel"] == "xmarch"), key=lambda r: r["ms_per_step"])
+    best = min((r for r in results if r["kernel"] != "direct"), key=lambda r: r["ms_per_step"])
     return {"nv": 10 * nn * nn + 2, "precision": precision, "size": size, "best": best, "all": results}
 
 
 def write_table(entries):
+    """entries: (nv, precision, tz, lx, kernel kind); kind 2 = cp.async, 3 = TMA x-march."""
     table = {}
     if os.path.exists(TILES):
         for line in open(TILES):
             p = line.split()
-            if len(p) == 4 and not line.startswith("#"):
-                table[(int(p[0]), int(p[1]))] = (int(p[2]), int(p[3]))
-    for nv, prec, tz, lx in entries:
-        table[(nv, prec)] = (tz, lx)
+            if len(p) >= 4 and not line.startswith("#"):
+                table[(int(p[0]), int(p[1]))] = (int(p[2]), int(p[3]), int(p[4]) if len(p) > 4 else 2)
+    for nv, prec, tz, lx, kind in entries:
+        table[(nv, prec)] = (tz, lx, kind)
     with open(TILES, "w") as f:
-        f.write("# nv precision tz lx -- x-march tiles chosen by nuosc_b200/autotune.py\n")
-        for (nv, prec), (tz, lx) in sorted(table.items()):
-            f.write("%d %d %d %d\n" % (nv, prec, tz, lx))
+        f.write("# nv precision tz lx kernel -- x-march tiles chosen by nuosc_b200/autotune.py "
+                "(kernel 2 cp.async, 3 TMA)\n")
+        for (nv, prec), (tz, lx, kind) in sorted(table.items()):
+            f.write("%d %d %d %d %d\n" % (nv, prec, tz, lx, kind))
 
 
 def main():
@@ -92,7 +97,7 @@ def main():
         for prec in args.precision:
             res = tune(nn, prec, args.size, args.steps, args.warmup, args.lx)
             print(json.dumps(res))
-            entries.append((res["nv"], prec, res["best"]["tz"], res["best"]["lx"]))
+            entries.append((res["nv"], prec, res["best"]["tz"], res["best"]["lx"], res["best"]["kind"]))
     if args.write:
         write_table(entries)
 

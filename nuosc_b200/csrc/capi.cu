@@ -232,8 +232,8 @@ int run_stage_direct(nuosc_handle *h, int mode, int in, int u, int acc_src, int 
 
 // one RK4 stage in the x-march path (moments of the stage output fused)
 template <typename T>
-int run_stage_xmarch(nuosc_handle *h, int mode, int in, int u, int acc_src, int acc_dst, int y_dst, double cA,
-                     double cY) {
+int run_stage_xmarch(nuosc_handle *h, bool tma, int mode, int in, int u, int acc_src, int acc_dst, int y_dst,
+                     double cA, double cY) {
     StageArgs<T> a{};
     a.in = (const T *)h->reg[in];
     a.u = u >= 0 ? (const T *)h->reg[u] : nullptr;
@@ -255,7 +255,8 @@ int run_stage_xmarch(nuosc_handle *h, int mode, int in, int u, int acc_src, int 
         h->launches++;
     }
     int ps = h->prof_begin(prof_kind(mode));
-    CUDA_TRY(launch_stage_xmarch<T>(a, mode, h->ko6, h->tile, h->stream));
+    if (tma) CUDA_TRY(launch_stage_xtma<T>(a, mode, h->ko6, h->tile, h->stream));
+    else CUDA_TRY(launch_stage_xmarch<T>(a, mode, h->ko6, h->tile, h->stream));
     h->prof_end(ps);
     ps = h->prof_begin(5);
     CUDA_TRY(launch_moment_finalize(h->d_part, h->d_mom, h->g, xmarch_num_vblocks(h->g, h->tile), h->stream));
@@ -265,18 +266,26 @@ int run_stage_xmarch(nuosc_handle *h, int mode, int in, int u, int acc_src, int 
     return 0;
 }
 
+// stage-kernel path for this handle: 0 direct, 1 cp.async x-march, 2 TMA x-march (-1: unsupported request)
 template <typename T>
-bool use_xmarch(nuosc_handle *h) {
-    if (h->kernel == NUOSC_KERNEL_DIRECT) return false;
-    return xmarch_supported<T>(h->g, h->ko6, h->tile);
+int stage_path(nuosc_handle *h) {
+    const bool tma = xtma_supported<T>(h->g, h->tile), cpa = xmarch_supported<T>(h->g, h->ko6, h->tile);
+    switch (h->kernel) {
+    case NUOSC_KERNEL_DIRECT: return 0;
+    case NUOSC_KERNEL_XMARCH: return cpa ? 1 : -1;
+    case NUOSC_KERNEL_XTMA: return tma ? 2 : -1;
+    default:
+        if (h->tile.kind == NUOSC_KERNEL_XMARCH && cpa) return 1;
+        return tma ? 2 : cpa ? 1 : 0;
+    }
 }
 
 template <typename T>
 int step_impl(nuosc_handle *h, int nsteps) {
     const double dt = h->dt;
-    const bool xm = use_xmarch<T>(h);
-    if (h->kernel == NUOSC_KERNEL_XMARCH && !xm)
-        return fail(NUOSC_ERR_UNSUPPORTED, "x-march kernel does not support this geometry");
+    const int path = stage_path<T>(h);
+    if (path < 0) return fail(NUOSC_ERR_UNSUPPORTED, "the requested stage kernel does not support this geometry/tile");
+    const bool xm = path > 0, tma = path == 2;
     if (xm) {
         const size_t need = (size_t)h->g.ncell * xmarch_num_vblocks(h->g, h->tile) * 2 * NMOM * sizeof(double);
         if (int rc = ensure((void **)&h->d_part, &h->part_bytes, need, h)) return rc;
@@ -284,10 +293,10 @@ int step_impl(nuosc_handle *h, int nsteps) {
     for (int n = 0; n < nsteps; ++n) {
         int rc;
         if (xm) {
-            if ((rc = run_stage_xmarch<T>(h, MODE_S1, 0, -1, -1, 1, 2, dt / 6.0, 0.5 * dt))) return rc;
-            if ((rc = run_stage_xmarch<T>(h, MODE_S23, 2, 0, 1, 1, 3, dt / 3.0, 0.5 * dt))) return rc;
-            if ((rc = run_stage_xmarch<T>(h, MODE_S23, 3, 0, 1, 1, 2, dt / 3.0, dt))) return rc;
-            if ((rc = run_stage_xmarch<T>(h, MODE_S4, 2, -1, 1, 0, -1, dt / 6.0, 0.0))) return rc;
+            if ((rc = run_stage_xmarch<T>(h, tma, MODE_S1, 0, -1, -1, 1, 2, dt / 6.0, 0.5 * dt))) return rc;
+            if ((rc = run_stage_xmarch<T>(h, tma, MODE_S23, 2, 0, 1, 1, 3, dt / 3.0, 0.5 * dt))) return rc;
+            if ((rc = run_stage_xmarch<T>(h, tma, MODE_S23, 3, 0, 1, 1, 2, dt / 3.0, dt))) return rc;
+            if ((rc = run_stage_xmarch<T>(h, tma, MODE_S4, 2, -1, 1, 0, -1, dt / 6.0, 0.0))) return rc;
         } else {
             if ((rc = run_stage_direct<T>(h, MODE_S1, 0, -1, -1, 1, 2, dt / 6.0, 0.5 * dt))) return rc;
             h->mom_valid = false;
@@ -630,7 +639,7 @@ int nuosc_set_renorm(nuosc_handle *h, int renorm) {
 }
 int nuosc_set_kernel(nuosc_handle *h, int kind) {
     if (!h) return fail(NUOSC_ERR_INVALID, "null handle");
-    if (kind < NUOSC_KERNEL_AUTO || kind > NUOSC_KERNEL_XMARCH) return fail(NUOSC_ERR_INVALID, "kernel kind %d", kind);
+    if (kind < NUOSC_KERNEL_AUTO || kind > NUOSC_KERNEL_XTMA) return fail(NUOSC_ERR_INVALID, "kernel kind %d", kind);
     h->kernel = kind;
     h->mom_valid = false;
     return NUOSC_OK;

@@ -70,14 +70,22 @@ cudaError_t launch_stage_direct(const StageArgs<T> &a, int mode, bool ko6, cudaS
 
 // x-march kernel: tile shape chosen by the autotuner (tile.cu)
 struct XTile {
-    int tz;      // z rows per CTA
-    int lx;      // x planes marched per CTA
-    int vb;      // velocities per CTA (32)
+    int tz;        // z rows per CTA
+    int lx;        // x planes marched per CTA
+    int vb;        // velocities per CTA (32)
+    int kind = 0;  // preferred x-march kernel from the tile table: 2 cp.async, 3 TMA, 0 either
 };
 template <typename T>
 bool xmarch_supported(const Geom &g, bool ko6, XTile t);
 template <typename T>
 cudaError_t launch_stage_xmarch(const StageArgs<T> &a, int mode, bool ko6, XTile t, cudaStream_t s);
+// TMA-fed variant of the x-march kernel (xtma.cu); needs nz % tz == 0
+template <typename T>
+bool xtma_supported(const Geom &g, XTile t);
+template <typename T>
+cudaError_t launch_stage_xtma(const StageArgs<T> &a, int mode, bool ko6, XTile t, cudaStream_t s);
+// value a kernel writes into StageArgs::status when a bounded wait expires
+constexpr int NUOSC_TIMEOUT_CODE = 1;
 int xmarch_num_vblocks(const Geom &g, XTile t);
 cudaError_t launch_moment_finalize(const double *part, double *mom, Geom g, int nvb, cudaStream_t s);
 

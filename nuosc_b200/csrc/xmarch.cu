@@ -401,11 +401,12 @@ template bool xmarch_supported<float>(const Geom &, bool, XTile);
 template cudaError_t launch_stage_xmarch<double>(const StageArgs<double> &, int, bool, XTile, cudaStream_t);
 template cudaError_t launch_stage_xmarch<float>(const StageArgs<float> &, int, bool, XTile, cudaStream_t);
 
-// Tile table keyed on (velocity count, precision): lines "nv precision tz lx"
-// in tiles.txt beside the library (or the file named by NUOSC_TILES), written
-// by the autotuner nuosc_b200/autotune.py.  Shapes not listed use 16 x 128.
+// Tile table keyed on (velocity count, precision): lines "nv precision tz lx
+// [kernel]" in tiles.txt beside the library (or the file named by
+// NUOSC_TILES), written by the autotuner nuosc_b200/autotune.py; kernel 2 is
+// the cp.async x-march, 3 the TMA one.  Shapes not listed use 16 x 128.
 XTile autotune_lookup(int nv, int precision) {
-    static std::vector<std::array<int, 4>> table;
+    static std::vector<std::array<int, 5>> table;
     static std::once_flag once;
     std::call_once(once, [] {
         std::string path;
@@ -423,14 +424,16 @@ XTile autotune_lookup(int nv, int precision) {
         if (!f) return;
         char line[256];
         while (fgets(line, sizeof line, f)) {
-            std::array<int, 4> e;
-            if (line[0] != '#' && sscanf(line, "%d %d %d %d", &e[0], &e[1], &e[2], &e[3]) == 4) table.push_back(e);
+            std::array<int, 5> e{0, 0, 0, 0, 0};
+            if (line[0] != '#' && sscanf(line, "%d %d %d %d %d", &e[0], &e[1], &e[2], &e[3], &e[4]) >= 4)
+                table.push_back(e);
         }
         fclose(f);
     });
     for (const auto &e : table)
-        if (e[0] == nv && e[1] == precision && (e[2] == 4 || e[2] == 8 || e[2] == 16) && e[3] >= 1) return XTile{e[2], e[3], VB};
-    return XTile{16, 128, VB};
+        if (e[0] == nv && e[1] == precision && (e[2] == 4 || e[2] == 8 || e[2] == 16) && e[3] >= 1)
+            return XTile{e[2], e[3], VB, e[4]};
+    return XTile{16, 128, VB, 0};
 }
 
 }  // namespace nuosc

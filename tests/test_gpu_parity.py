@@ -60,13 +60,13 @@ def assert_diag_close(a, ref):
     np.testing.assert_allclose(a[8], ref[8], atol=1e-11)
 
 
-KERNELS = [1, 2]  # direct, x-march
+KERNELS = [1, 2, 3]  # direct, cp.async x-march, TMA x-march
 
 
 def _kernel_ok(nb, s, kernel):
     if kernel == nb.KERNEL_DIRECT:
         s.set_kernel(kernel)
-    if kernel == nb.KERNEL_XMARCH:
+    if kernel in (nb.KERNEL_XMARCH, nb.KERNEL_XTMA):
         try:
             s.step_rk4(0)
             s.set_kernel(kernel)
