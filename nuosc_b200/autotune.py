@@ -30,7 +30,8 @@ def time_steps(s, stream, steps, warmup):
     return e0.elapsed_time(e1) / steps
 
 
-def tune(nn, precision, size, steps=3, warmup=2, lx_list=DEFAULT_LX, device=0, ko_order=6):
+def tune(nn, precision, size, steps=3, warmup=2, lx_list=DEFAULT_LX, device=0, ko_order=6, kinds=(2, 3),
+         tz_list=(4, 8, 16)):
     import torch
     import nuosc_b200 as nb
     torch.cuda.set_device(device)
@@ -48,8 +49,12 @@ def tune(nn, precision, size, steps=3, warmup=2, lx_list=DEFAULT_LX, device=0, k
     ms = time_steps(s, stream, steps, warmup)
     results.append({"kernel": "direct", "ms_per_step": ms, "cell_steps_per_s": cells / ms * 1e3})
     for kind, name, tzs in ((nb.KERNEL_XTMA, "xtma", (8, 16)), (nb.KERNEL_XMARCH, "xmarch", (4, 8, 16))):
+        if kind not in kinds:
+            continue
         s.set_kernel(kind)
         for tz in tzs:
+            if tz not in tz_list:
+                continue
             if kind == nb.KERNEL_XTMA and s.grid.nz % tz:
                 continue
             for lx in lx_list:
@@ -90,12 +95,15 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=2)
     ap.add_argument("--lx", type=int, nargs="+", default=list(DEFAULT_LX))
+    ap.add_argument("--kinds", type=int, nargs="+", default=[2, 3], help="2 cp.async x-march, 3 TMA x-march")
+    ap.add_argument("--tz", type=int, nargs="+", default=[4, 8, 16])
     ap.add_argument("--write", action="store_true")
     args = ap.parse_args()
     entries = []
     for nn in args.nn:
         for prec in args.precision:
-            res = tune(nn, prec, args.size, args.steps, args.warmup, args.lx)
+            res = tune(nn, prec, args.size, args.steps, args.warmup, args.lx, kinds=tuple(args.kinds),
+                       tz_list=tuple(args.tz))
             print(json.dumps(res))
             entries.append((res["nv"], prec, res["best"]["tz"], res["best"]["lx"], res["best"]["kind"]))
     if args.write:

@@ -2,25 +2,26 @@
 //
 // Same arithmetic and per-thread structure as xmarch.cu (one (z, v) column per
 // thread, (2R+1)-deep register queue in x, fused RK epilogue and moment
-// partials), but the data movement is Blackwell-native:
-//   * per x plane, lane 0 of warp 0 issues TMA tensor loads
-//     (cp.async.bulk.tensor.4d) of the whole centre-plane box with its z halo
-//     ([TZ+2R rows][4 fields][32 velocities], split into 2-3 boxes where the
-//     periodic z wrap cuts it), of the queue front plane, and a bulk copy of
-//     the TZ cells' moments, into an NS-deep shared ring; completion is
-//     tracked by one "full" mbarrier per ring slot (expect_tx bytes);
-//   * every consumer warp reads its z stencil straight from the box, so warps
-//     never exchange data and there is no CTA-wide barrier in the march: a
-//     warp waits only on the slot's full barrier and releases the slot by
-//     arriving on its "empty" mbarrier; the issuing lane waits on "empty"
-//     before refilling a slot;
+// partials), with Blackwell-native data movement:
+//   * box ring: for every x plane the CTA touches, lane 0 of warp 0 issues one
+//     TMA tensor load (cp.async.bulk.tensor.4d; 2-3 boxes where the periodic z
+//     wrap cuts it) of the plane's [TZ+2R rows][4 fields][32 velocities] box
+//     and a bulk copy of the TZ cells' moments into a ring slot whose
+//     completion is tracked by a "full" mbarrier (expect_tx bytes).  A box is
+//     used twice: first as the queue front (x+R), R planes later as the
+//     centre plane of the z stencil, so each state value crosses HBM once;
+//   * warps never exchange data and there is no CTA-wide barrier in the
+//     march: a warp waits only on full barriers and releases a slot after its
+//     last use by arriving on the slot's "empty" mbarrier; the issuing lane
+//     waits on "empty" before refilling a slot;
 //   * the pointwise U and A inputs of the epilogue are plain coalesced loads
-//     issued before the stencil arithmetic, so the ring holds only what the
-//     stencil needs and can be deep.
-// All mbarrier waits are bounded: on expiry the kernel records
-// NUOSC_ERR_TIMEOUT in the status word, stops marching and, before
-// returning, waits (again bounded) for the copies it issued.
-// Requires nz % TZ == 0; other geometries use the cp.async kernel.
+//     issued at the top of each plane, before the waits and the stencil;
+//   * moment partials: each lane holds its 16 (12 + 4 zero) partial moments in
+//     a lane-dependent permuted order so that the reduce-scatter over the 32
+//     velocities of the warp needs no selects (15 shuffle-adds + 1).
+// All mbarrier waits are bounded: on expiry the kernel records the timeout in
+// the status word, stops marching and, before returning, waits (again
+// bounded) for the copies it issued.  Requires nz % TZ == 0.
 #include "internal.cuh"
 #include "physics.cuh"
 
@@ -31,12 +32,12 @@ namespace nuosc {
 namespace {
 
 constexpr int VB = 32;
-constexpr unsigned kWaitSpins = 1u << 22;  // bounded mbarrier waits (seconds at most)
+constexpr unsigned kWaitSpins = 1u << 22;  // bounded mbarrier waits
 
 struct __align__(64) TmaMaps {
-    CUtensorMap zr;   // box of TZ+2R rows (centre plane + both halos)
-    CUtensorMap tzr;  // TZ+R rows (a halo cut by the wrap)
-    CUtensorMap tz;   // TZ rows (front plane; middle piece of a fully wrapped box)
+    CUtensorMap zr;   // box of TZ+2R rows (plane box with both halos)
+    CUtensorMap tzr;  // TZ+R rows (a box cut by the wrap)
+    CUtensorMap tz;   // TZ rows (middle piece of a box wrapped at both ends)
     CUtensorMap r;    // R rows (wrapped halo)
 };
 
@@ -79,15 +80,14 @@ __device__ __forceinline__ void bulk_load(unsigned dst, const void *src, unsigne
 
 constexpr int up128(int x) { return (x + 127) / 128 * 128; }
 
-// shared layout of one ring slot: zb [ZR][4][VB] T | fr [TZ][4][VB] T | mb [TZ][12] double
+// one ring slot: box [ZR][4][VB] T | moments [TZ][12] double
 template <typename T, int TZ, int R>
 struct Slot {
     static constexpr int ZR = TZ + 2 * R;
-    static constexpr int zb = 0;
-    static constexpr int fr = up128(zb + (int)sizeof(T) * ZR * 4 * VB);
-    static constexpr int mb = up128(fr + (int)sizeof(T) * TZ * 4 * VB);
+    static constexpr int box = 0;
+    static constexpr int mb = up128(box + (int)sizeof(T) * ZR * 4 * VB);
     static constexpr int bytes = up128(mb + 8 * TZ * NMOM);
-    static constexpr unsigned tx = sizeof(T) * (ZR + TZ) * 4 * VB + 8 * TZ * NMOM;  // bytes landing per plane
+    static constexpr unsigned tx = sizeof(T) * ZR * 4 * VB + 8 * TZ * NMOM;  // bytes landing per plane
 };
 
 template <typename T, int R>
@@ -101,44 +101,48 @@ __device__ __forceinline__ T axis_terms(const T (&s)[2 * R + 1], T f, T k3, T k2
     return fma(f, fma(T(-8), d1, d2), acc);
 }
 
-template <typename T>
-__device__ __forceinline__ void rhs_half(const T (&c)[4], T a, T b, T e, T mu, T pmo, T ct, T st, const T (&sten)[4],
+template <typename T, bool VAC>
+__device__ __forceinline__ void rhs_half(const T (&c)[4], T a, T b, T e, T mu, T p2s, T p2c, T ps, const T (&sten)[4],
                                          T (&out)[4]) {
     const T ee = c[0], mm = c[1], emr = c[2], emi = c[3];
     const T Iee = T(2) * mu * (emi * a + emr * b);
     const T Iemr = -mu * ((ee - mm) * b + e * emi);
     const T Iemi = mu * ((mm - ee) * a + e * emr);
-    out[0] = Iee + sten[0] - pmo * T(2) * st * emi;
-    out[1] = -Iee + sten[1] + pmo * T(2) * st * emi;
-    out[2] = Iemr + sten[2] - pmo * T(2) * ct * emi;
-    out[3] = Iemi + sten[3] + pmo * (T(2) * ct * emr + st * (ee - mm));
-}
-
-template <int N, int O>
-__device__ __forceinline__ void rs_step(double (&m)[16], int lane) {
-    const bool up = (lane & O) != 0;
-#pragma unroll
-    for (int i = 0; i < N / 2; ++i) {
-        const double send = up ? m[i] : m[i + N / 2];
-        const double keep = up ? m[i + N / 2] : m[i];
-        m[i] = keep + __shfl_xor_sync(0xffffffffu, send, O);
+    out[0] = Iee + sten[0];
+    out[1] = -Iee + sten[1];
+    out[2] = Iemr + sten[2];
+    out[3] = Iemi + sten[3];
+    if (VAC) {  // pmo * [H_vac, rho] (nuosc_class.cpp:280-287); p2s = 2 pmo st, p2c = 2 pmo ct, ps = pmo st
+        out[0] -= p2s * emi;
+        out[1] += p2s * emi;
+        out[2] -= p2c * emi;
+        out[3] += p2c * emr + ps * (ee - mm);
     }
 }
 
-template <int TZ>
+// one reduce-scatter step over lane pairs (lane, lane^O): N values -> N/2;
+// the lane-permuted slot order makes the kept half always the lower one
+template <int N, int O>
+__device__ __forceinline__ void rs_step(double (&m)[16]) {
+#pragma unroll
+    for (int i = 0; i < N / 2; ++i) m[i] += __shfl_xor_sync(0xffffffffu, m[i + N / 2], O);
+}
+
+template <typename T, int TZ>
 constexpr int tma_ctas_per_sm() {
     return TZ == 16 ? 1 : 2;
 }
 
 }  // namespace
 
-template <typename T, int R, int MODE, int TZ, int NS>
-__global__ void __launch_bounds__(VB *TZ, tma_ctas_per_sm<TZ>())
+template <typename T, int R, int MODE, int TZ, bool VAC>
+__global__ void __launch_bounds__(VB *TZ, tma_ctas_per_sm<T, TZ>())
     k_xtma(const __grid_constant__ TmaMaps maps, const StageArgs<T> a, int LX) {
     using S = Slot<T, TZ, R>;
     constexpr int W = 2 * R + 1;
     constexpr int ZR = S::ZR;
-    constexpr int D = NS - 2 > 0 ? NS - 2 : 1;  // planes issued ahead (slack of NS-D slots)
+    constexpr int D = 2;              // boxes issued ahead of their first use
+    constexpr int NS = R + D + 2;     // a box lives from its front use to its centre use, plus slack
     extern __shared__ __align__(1024) unsigned char smem[];
     unsigned long long *bars = (unsigned long long *)(smem + NS * S::bytes);  // full[NS], empty[NS]
     __shared__ int s_abort;
@@ -154,7 +158,8 @@ __global__ void __launch_bounds__(VB *TZ, tma_ctas_per_sm<TZ>())
     if (xs >= g.nx) return;
     const int xe = min(xs + LX, g.nx);
     const int nplanes = xe - xs;
-    const int zr = z0 + r;  // always < nz (nz % TZ == 0)
+    const int nboxes = nplanes + R;   // centres xs..xe-1 and fronts up to xe-1+R
+    const int zr = z0 + r;            // < nz since nz % TZ == 0
     const long long fs = g.fs;
     const long long P = (long long)g.nz * g.nvs;
     const long long hoff = (long long)half * 4 * fs;
@@ -170,28 +175,25 @@ __global__ void __launch_bounds__(VB *TZ, tma_ctas_per_sm<TZ>())
     }
     __syncthreads();
 
-    // lane 0 of warp 0 issues the loads of plane index i (x = xs + i) into slot i % NS
-    auto issue = [&](int i) -> bool {
-        const int s = i % NS;
-        if (i >= NS && !mbar_wait(smem_u32(&bars[NS + s]), (unsigned)((i / NS - 1) & 1))) return false;
+    // lane 0 of warp 0: load box j (plane xs + j, periodic) into slot j % NS
+    auto issue = [&](int j) -> bool {
+        const int s = j % NS;
+        if (j >= NS && !mbar_wait(smem_u32(&bars[NS + s]), (unsigned)((j / NS - 1) & 1))) return false;
         const unsigned full = smem_u32(&bars[s]);
         unsigned char *sp = smem + s * S::bytes;
         mbar_expect_tx(full, S::tx);
-        const int x = xs + i;
+        const int x = (xs + j) % g.nx;
         const int c1 = 4 * half, c0 = vb * VB;
-        // centre box rows z0-R .. z0+TZ+R-1 (periodic), as 1-3 contiguous pieces
         int zstart = z0 - R, dst = 0;
         while (dst < ZR) {
             const int zw = zstart < 0 ? zstart + g.nz : (zstart >= g.nz ? zstart - g.nz : zstart);
             int len = g.nz - zw;
             if (len > ZR - dst) len = ZR - dst;
             const CUtensorMap *m = len == ZR ? &maps.zr : len == TZ + R ? &maps.tzr : len == TZ ? &maps.tz : &maps.r;
-            tma_load_4d(smem_u32(sp + S::zb + dst * 4 * VB * sizeof(T)), m, c0, c1, zw, x, full);
+            tma_load_4d(smem_u32(sp + S::box + dst * 4 * VB * sizeof(T)), m, c0, c1, zw, x, full);
             zstart += len;
             dst += len;
         }
-        const int xf = x + R < g.nx ? x + R : x + R - g.nx;
-        tma_load_4d(smem_u32(sp + S::fr), &maps.tz, c0, c1, z0, xf, full);
         bulk_load(smem_u32(sp + S::mb), a.mom_in + ((long long)x * g.nz + z0) * NMOM, 8u * TZ * NMOM, full);
         return true;
     };
@@ -201,8 +203,21 @@ __global__ void __launch_bounds__(VB *TZ, tma_ctas_per_sm<TZ>())
     const T fx = T(vxd * a.c.fxs), fz = T(vzd * a.c.fzs);
     const T kz3 = T(a.c.kz3), kz2 = T(a.c.kz2), kz1 = T(a.c.kz1);
     const T kx3 = T(a.c.kx3), kx2 = T(a.c.kx2), kx1 = T(a.c.kx1), kc = T(a.c.kc);
-    const T mu = T(a.c.mu), pmo = T(a.c.pmo), ct = T(a.c.ct), st = T(a.c.st);
+    const T mu = T(a.c.mu), p2s = T(2 * a.c.pmo * a.c.st), p2c = T(2 * a.c.pmo * a.c.ct), ps = T(a.c.pmo * a.c.st);
     const T cA = T(a.cA), cY = T(a.cY);
+    // lane-permuted moment weights: slot i of this lane holds moment (i ^ perm),
+    // moment k = (combo k>>2, weight k&3); perm = bits 1..4 of the lane
+    const int perm = (lane >> 1) & 15;
+    double wperm[4];
+    {
+        const double v4w[4] = {wd, vxd * wd, vyd * wd, vzd * wd};
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int k = j ^ (perm & 3);
+            wperm[j] = k == 0 ? v4w[0] : k == 1 ? v4w[1] : k == 2 ? v4w[2] : v4w[3];
+        }
+    }
+    const bool sw1 = (perm >> 2) & 1, sw2 = (perm >> 3) & 1;
 
     // prime the register queue with planes xs-R .. xs+R-1
     T q[4][W];
@@ -213,33 +228,38 @@ __global__ void __launch_bounds__(VB *TZ, tma_ctas_per_sm<TZ>())
         for (int f = 0; f < 4; ++f) q[f][p] = vact ? in[f * fs + o] : T(0);
     }
     bool ok = true;
-    if (tid == 0)
-        for (int d = 0; d < D && d < nplanes; ++d) ok = ok && issue(d);
+    if (tid == 0)  // boxes j < R are only centres: skip those past a short segment's end
+        for (int j = 0; j < R + D && j < nboxes; ++j)
+            if (j >= R || j < nplanes) ok = ok && issue(j);
 
-    int done = 0;
     for (int i = 0; i < nplanes; ++i) {
-        if (tid == 0 && ok && i + D < nplanes) ok = issue(i + D);
+        if (tid == 0 && ok && i + R + D < nboxes) ok = issue(i + R + D);
         if (tid == 0 && !ok) s_abort = 1;
-        const int s = i % NS;
         const int x = xs + i;
-        // pointwise epilogue inputs first (they are not in the ring)
         const long long oc = hoff + (long long)x * P + own;
+        // pointwise epilogue inputs first (they are not in the ring)
         T uin[4], ain[4];
 #pragma unroll
         for (int f = 0; f < 4; ++f) {
             uin[f] = (MODE == MODE_S23 && vact) ? a.u[oc + f * fs] : T(0);
             ain[f] = (MODE != MODE_S1 && vact) ? a.acc_src[oc + f * fs] : T(0);
         }
-        if (!mbar_wait(smem_u32(&bars[s]), (unsigned)((i / NS) & 1)) || *(volatile int *)&s_abort) {
+        const int jf = i + R, sf = jf % NS, sc = i % NS;
+        if (!mbar_wait(smem_u32(&bars[sf]), (unsigned)((jf / NS) & 1)) ||
+            !mbar_wait(smem_u32(&bars[sc]), (unsigned)((i / NS) & 1)) || *(volatile int *)&s_abort) {
             s_abort = 1;
             break;
         }
-        const unsigned char *sp = smem + s * S::bytes;
-        const T *zb = (const T *)(sp + S::zb);
-        const T *fr = (const T *)(sp + S::fr);
-        const double *mb = (const double *)(sp + S::mb);
+        const T *fbox = (const T *)(smem + sf * S::bytes + S::box);
 #pragma unroll
-        for (int f = 0; f < 4; ++f) q[f][2 * R] = vact ? fr[(r * 4 + f) * VB + lane] : T(0);
+        for (int f = 0; f < 4; ++f) q[f][2 * R] = fbox[((R + r) * 4 + f) * VB + lane];
+        if (jf >= nplanes) {  // this box is never a centre: its front use was the last
+            __syncwarp();
+            if (lane == 0) mbar_arrive(smem_u32(&bars[NS + sf]));
+        }
+        const unsigned char *sp = smem + sc * S::bytes;
+        const T *zb = (const T *)(sp + S::box);
+        const double *mb = (const double *)(sp + S::mb);
 
         T sten[4], cen[4];
 #pragma unroll
@@ -262,13 +282,12 @@ __global__ void __launch_bounds__(VB *TZ, tma_ctas_per_sm<TZ>())
                 m[2 * k + 1] = t.y;
             }
         }
-        // the slot's shared data is consumed: release it
         __syncwarp();
-        if (lane == 0) mbar_arrive(smem_u32(&bars[NS + s]));
+        if (lane == 0) mbar_arrive(smem_u32(&bars[NS + sc]));  // centre use is the box's last use
 
         const T ia = T(inp(m, vxd, vyd, vzd)), ib = T(inp(m + 4, vxd, vyd, vzd)), ie = T(inp(m + 8, vxd, vyd, vzd));
         T kk[4];
-        rhs_half(cen, ia, ib, ie, mu, pmo, ct, st, sten, kk);
+        rhs_half<T, VAC>(cen, ia, ib, ie, mu, p2s, p2c, ps, sten, kk);
 
         T outm[4];
 #pragma unroll
@@ -300,33 +319,29 @@ __global__ void __launch_bounds__(VB *TZ, tma_ctas_per_sm<TZ>())
             if (half == 0) moment_terms<false>(outm[0], outm[1], outm[2], outm[3], d0, d1, d2);
             else moment_terms<true>(outm[0], outm[1], outm[2], outm[3], d0, d1, d2);
             if (!vact) d0 = d1 = d2 = 0.0;
-            const double v4w[4] = {wd, vxd * wd, vyd * wd, vzd * wd};
+            // combos in slot order: dperm[c] = d[c ^ (perm >> 2)], d[3] = 0
+            const double t0 = sw1 ? d1 : d0, t1 = sw1 ? d0 : d1, t2 = sw1 ? 0.0 : d2, t3 = sw1 ? d2 : 0.0;
+            const double dp[4] = {sw2 ? t2 : t0, sw2 ? t3 : t1, sw2 ? t0 : t2, sw2 ? t1 : t3};
             double mp[16];
 #pragma unroll
-            for (int s4 = 0; s4 < 4; ++s4) {
-                mp[s4] = v4w[s4] * d0;
-                mp[4 + s4] = v4w[s4] * d1;
-                mp[8 + s4] = v4w[s4] * d2;
-                mp[12 + s4] = 0.0;
-            }
-            rs_step<16, 16>(mp, lane);
-            rs_step<8, 8>(mp, lane);
-            rs_step<4, 4>(mp, lane);
-            rs_step<2, 2>(mp, lane);
+            for (int c = 0; c < 4; ++c)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) mp[4 * c + j] = wperm[j] * dp[c];
+            rs_step<16, 16>(mp);
+            rs_step<8, 8>(mp);
+            rs_step<4, 4>(mp);
+            rs_step<2, 2>(mp);
             mp[0] += __shfl_xor_sync(0xffffffffu, mp[0], 1);
-            const int idx = lane >> 1;
-            if ((lane & 1) == 0 && idx < NMOM) {
+            if ((lane & 1) == 0 && perm < NMOM) {  // lanes 2k, 2k+1 hold moment perm
                 const long long cell = (long long)x * g.nz + zr;
-                a.mom_part[((cell * nvb + vb) * 2 + half) * NMOM + idx] = mp[0];
+                a.mom_part[((cell * nvb + vb) * 2 + half) * NMOM + perm] = mp[0];
             }
         }
 #pragma unroll
         for (int f = 0; f < 4; ++f)
 #pragma unroll
             for (int k = 0; k < 2 * R; ++k) q[f][k] = q[f][k + 1];
-        done = i + 1;
     }
-    (void)done;
     __syncthreads();
     if (tid == 0 && s_abort) {
         // a wait expired: report it, then drain (bounded) every slot that may
@@ -376,39 +391,38 @@ bool make_map(CUtensorMap *m, const T *base, const Geom &g, int rows) {
               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-template <typename T, int TZ, int R>
-constexpr int tma_ring() {
-    constexpr int b = Slot<T, TZ, R>::bytes + 16;
-    constexpr int cap = 227 * 1024 / tma_ctas_per_sm<TZ>() - 1024;
-    return cap / b >= 6 ? 6 : cap / b >= 5 ? 5 : cap / b >= 4 ? 4 : 3;
-}
-
-template <typename T, int R, int MODE, int TZ>
+template <typename T, int R, int MODE, int TZ, bool VAC>
 cudaError_t launch_t(const StageArgs<T> &a, XTile t, cudaStream_t s) {
-    constexpr int NS = tma_ring<T, TZ, R>();
+    constexpr int NS = R + 2 + 2;
     using Sl = Slot<T, TZ, R>;
+    static_assert(tma_ctas_per_sm<T, TZ>() * ((R + 4) * Sl::bytes + 2048) <= 227 * 1024, "ring exceeds shared memory");
     TmaMaps maps;
     if (!make_map<T>(&maps.zr, a.in, a.g, TZ + 2 * R) || !make_map<T>(&maps.tzr, a.in, a.g, TZ + R) ||
         !make_map<T>(&maps.tz, a.in, a.g, TZ) || !make_map<T>(&maps.r, a.in, a.g, R))
         return cudaErrorInvalidValue;
     const size_t smem = (size_t)NS * Sl::bytes + 2 * NS * 8;
-    cudaError_t e =
-        cudaFuncSetAttribute(k_xtma<T, R, MODE, TZ, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = cudaFuncSetAttribute(k_xtma<T, R, MODE, TZ, VAC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
     if (e != cudaSuccess) return e;
     const int nseg = (a.g.nx + t.lx - 1) / t.lx;
     dim3 grid(a.g.nz / TZ, (a.g.nvs + VB - 1) / VB, nseg * 2);
-    k_xtma<T, R, MODE, TZ, NS><<<grid, VB * TZ, smem, s>>>(maps, a, t.lx);
+    k_xtma<T, R, MODE, TZ, VAC><<<grid, VB * TZ, smem, s>>>(maps, a, t.lx);
     return cudaGetLastError();
 }
 
-template <typename T, int R, int TZ>
+template <typename T, int R, int TZ, bool VAC>
 cudaError_t launch_tm(const StageArgs<T> &a, int mode, XTile t, cudaStream_t s) {
     switch (mode) {
-    case MODE_S1: return launch_t<T, R, MODE_S1, TZ>(a, t, s);
-    case MODE_S23: return launch_t<T, R, MODE_S23, TZ>(a, t, s);
-    case MODE_S4: return launch_t<T, R, MODE_S4, TZ>(a, t, s);
+    case MODE_S1: return launch_t<T, R, MODE_S1, TZ, VAC>(a, t, s);
+    case MODE_S23: return launch_t<T, R, MODE_S23, TZ, VAC>(a, t, s);
+    case MODE_S4: return launch_t<T, R, MODE_S4, TZ, VAC>(a, t, s);
     default: return cudaErrorInvalidValue;
     }
+}
+
+template <typename T, int R, int TZ>
+cudaError_t launch_tv(const StageArgs<T> &a, int mode, XTile t, cudaStream_t s) {
+    return a.c.pmo != 0.0 ? launch_tm<T, R, TZ, true>(a, mode, t, s) : launch_tm<T, R, TZ, false>(a, mode, t, s);
 }
 
 }  // namespace
@@ -421,8 +435,8 @@ bool xtma_supported(const Geom &g, XTile t) {
 template <typename T>
 cudaError_t launch_stage_xtma(const StageArgs<T> &a, int mode, bool ko6, XTile t, cudaStream_t s) {
     if (!a.mom_part || a.g.nz % t.tz) return cudaErrorInvalidValue;
-    if (t.tz == 16) return ko6 ? launch_tm<T, 3, 16>(a, mode, t, s) : launch_tm<T, 2, 16>(a, mode, t, s);
-    return ko6 ? launch_tm<T, 3, 8>(a, mode, t, s) : launch_tm<T, 2, 8>(a, mode, t, s);
+    if (t.tz == 16) return ko6 ? launch_tv<T, 3, 16>(a, mode, t, s) : launch_tv<T, 2, 16>(a, mode, t, s);
+    return ko6 ? launch_tv<T, 3, 8>(a, mode, t, s) : launch_tv<T, 2, 8>(a, mode, t, s);
 }
 
 template bool xtma_supported<double>(const Geom &, XTile);
