@@ -63,7 +63,26 @@ def build(verbose=False, jobs=8, extra=()):
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)
+    build_driver(verbose)
     return LIB
+
+
+def build_driver(verbose=False):
+    """The command-line driver nuosc_b200/nuosc (the reference's main, on the C ABI)."""
+    src = os.path.join(HERE, "driver", "nuosc_main.cpp")
+    exe = os.path.join(HERE, "nuosc")
+    deps = [src, LIB, os.path.join(ROOT, "include", "nuosc_b200.hpp"), os.path.join(ROOT, "include", "nuosc_b200.h")]
+    if os.path.exists(exe) and all(os.path.getmtime(exe) >= os.path.getmtime(d) for d in deps):
+        return exe
+    cxx = next((c for c in ("/usr/bin/g++", shutil.which("g++")) if c and os.path.exists(c)), None)
+    if cxx is None:
+        raise RuntimeError("g++ not found")
+    cmd = [cxx, "-O2", "-std=c++17", "-I" + os.path.join(ROOT, "include"), src, "-L" + HERE, "-lnuosc_b200",
+           "-Wl,-rpath,$ORIGIN", "-o", exe]
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.run(cmd, check=True)
+    return exe
 
 
 def _drain(procs):
