@@ -200,6 +200,39 @@ long long nuosc_kernel_launches(const nuosc_handle *h);
 int nuosc_set_profiling(nuosc_handle *h, int on);
 int nuosc_get_profile(nuosc_handle *h, double *ms, long long *launches, int nkinds);
 
+/* ---- right-hand side without device allocation -------------------------
+ * No counterpart in the reference.  For callers that may not call cudaMalloc:
+ * code issuing work while its stream is being captured into a CUDA graph
+ * (allocation is refused during capture), and host frameworks that keep all
+ * device memory in their own allocator and hand a plugin only their buffers.
+ * The caller passes everything in its own device memory: `in` and `out` are
+ * states laid out like the library's registers, [8 fields][nx][nz][nv_stride]
+ * of double (NUOSC_FP64) or float (NUOSC_FP32), padding velocities zero, and
+ * the quadrature arrays (nv_stride doubles each, zero in the padding).  The
+ * call computes out = L(in), the calRHS of the reference, on `stream` and
+ * allocates nothing: the per-cell velocity moments it needs go to a
+ * file-scope device array of NUOSC_NOALLOC_MAX_CELLS * 12 doubles (6 MiB),
+ * which every GPU that loads the library holds until the process exits.
+ *   - grids with nx*nz > NUOSC_NOALLOC_MAX_CELLS are rejected (NUOSC_ERR_INVALID);
+ *   - the first call on a device looks up the array's device address
+ *     (cudaGetSymbolAddress) with that device current; make that first call
+ *     before any stream capture begins;
+ *   - all calls share the one array and it keeps the last call's moments;
+ *     each call rewrites every entry it reads, so nothing needs clearing, but
+ *     calls that overlap on the GPU (e.g. on two streams at once) race on it.
+ * Returns NUOSC_OK once the two kernels are queued; errors are reported by
+ * nuosc_last_error(). */
+#define NUOSC_NOALLOC_MAX_CELLS 65536
+typedef struct nuosc_rhs_desc {
+    int nx, nz, nv;     /* interior cells and velocities */
+    int nv_stride;      /* velocities per (x,z) row of in/out (>= nv) */
+    int precision;      /* NUOSC_FP64 or NUOSC_FP32: element type of in/out */
+    int ko_order;       /* 6: 6th-difference KO (reference with KO_ORD_3 undefined), 4: 4th-difference KO */
+    double dx, dz, ko, mu, pmo;
+    const double *vx, *vy, *vz, *vw; /* device arrays of nv_stride entries */
+} nuosc_rhs_desc;
+int nuosc_calrhs_noalloc(const nuosc_rhs_desc *desc, const void *in, void *out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

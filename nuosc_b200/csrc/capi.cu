@@ -35,8 +35,15 @@ XTile autotune_lookup(int nv, int precision);
 using namespace nuosc;
 
 namespace {
-
 thread_local std::string g_err;
+}  // namespace
+
+int nuosc::set_last_error(int code, const char *msg) {
+    g_err = msg;
+    return code;
+}
+
+namespace {
 
 int fail(int code, const char *fmt, ...) {
     char buf[512];

@@ -86,6 +86,9 @@ template <typename T>
 cudaError_t launch_stage_xtma(const StageArgs<T> &a, int mode, bool ko6, XTile t, cudaStream_t s);
 // value a kernel writes into StageArgs::status when a bounded wait expires
 constexpr int NUOSC_TIMEOUT_CODE = 1;
+
+// records msg as the calling thread's nuosc_last_error() and returns code (capi.cu)
+int set_last_error(int code, const char *msg);
 int xmarch_num_vblocks(const Geom &g, XTile t);
 cudaError_t launch_moment_finalize(const double *part, double *mom, Geom g, int nvb, cudaStream_t s);
 

@@ -1,0 +1,115 @@
+// noalloc.cu -- calRHS for callers that cannot allocate device memory.
+//
+// Some callers of this library may not call cudaMalloc: code that runs while
+// its stream is being captured into a CUDA graph (allocation calls are
+// refused during capture), and host frameworks that reserve all device
+// memory for their own allocator and hand plugins only their own buffers.
+// nuosc_calrhs_noalloc serves them: the caller passes the input and output
+// state (and the velocity quadrature) in its own device memory, and the one
+// piece of scratch the right-hand side needs -- the 12 velocity moments per
+// (x,z) cell -- lives in the file-scope device array below, sized for grids
+// of up to NUOSC_NOALLOC_MAX_CELLS cells.  Every GPU that loads the library
+// holds that array (6 MiB) until the process exits.
+//
+// The kernels are the library's own moment pass and direct stage kernel
+// (kernels.cu), unchanged; only the scratch pointer differs.
+#include "../../include/nuosc_b200.h"
+#include "internal.cuh"
+
+#include <cmath>
+#include <cstdio>
+#include <mutex>
+#include <string>
+
+namespace nuosc {
+namespace {
+
+// 12 moments per cell for at most NUOSC_NOALLOC_MAX_CELLS cells
+static __device__ __align__(256) double g_noalloc_moments[(size_t)NUOSC_NOALLOC_MAX_CELLS * NMOM];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_mu;
+double *g_scratch[kMaxDevices] = {nullptr};
+
+int fail(int code, const char *msg) { return set_last_error(code, msg); }
+
+}  // namespace
+}  // namespace nuosc
+
+using namespace nuosc;
+
+extern "C" int nuosc_calrhs_noalloc(const nuosc_rhs_desc *d, const void *in, void *out, void *stream) {
+    if (!d || !in || !out) return fail(NUOSC_ERR_INVALID, "calrhs_noalloc: null argument");
+    if (d->nx < 4 || d->nz < 4 || d->nv < 1 || d->nv_stride < d->nv)
+        return fail(NUOSC_ERR_INVALID, "calrhs_noalloc: bad geometry");
+    if ((long long)d->nx * d->nz > NUOSC_NOALLOC_MAX_CELLS)
+        return fail(NUOSC_ERR_INVALID,
+                    "calrhs_noalloc: nx*nz exceeds NUOSC_NOALLOC_MAX_CELLS (65536) cells of device scratch");
+    if (d->precision != NUOSC_FP64 && d->precision != NUOSC_FP32)
+        return fail(NUOSC_ERR_INVALID, "calrhs_noalloc: precision must be NUOSC_FP64 or NUOSC_FP32");
+    if (d->ko_order != 6 && d->ko_order != 4) return fail(NUOSC_ERR_INVALID, "calrhs_noalloc: ko_order must be 6 or 4");
+    if (!d->vx || !d->vy || !d->vz || !d->vw) return fail(NUOSC_ERR_INVALID, "calrhs_noalloc: null quadrature");
+
+    // device address of the scratch array: looked up once per device, with that device current
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices)
+        return fail(NUOSC_ERR_CUDA, "calrhs_noalloc: no current CUDA device");
+    double *scratch = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_mu);
+        if (!g_scratch[dev]) {
+            void *p = nullptr;
+            const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_moments);
+            if (e != cudaSuccess) return fail(NUOSC_ERR_CUDA, "calrhs_noalloc: cudaGetSymbolAddress failed");
+            g_scratch[dev] = (double *)p;
+        }
+        scratch = g_scratch[dev];
+    }
+
+    Geom g;
+    g.nx = d->nx;
+    g.nz = d->nz;
+    g.nv = d->nv;
+    g.nvs = d->nv_stride;
+    g.ncell = (long long)d->nx * d->nz;
+    g.fs = g.ncell * d->nv_stride;
+    const bool ko6 = d->ko_order == 6;
+    Coeffs c{};
+    c.fxs = -1.0 / (12 * d->dx);
+    c.fzs = -1.0 / (12 * d->dz);
+    c.kx = ko6 ? -d->ko / d->dx / 64.0 : -d->ko / d->dx / 16.0;
+    c.kz = ko6 ? -d->ko / d->dz / 64.0 : -d->ko / d->dz / 16.0;
+    const double theta = 37 * M_PI / 180.;
+    c.ct = std::cos(2 * theta);
+    c.st = std::sin(2 * theta);
+    c.mu = d->mu;
+    c.pmo = d->pmo;
+    const Quad q{d->vx, d->vy, d->vz, d->vw};
+    cudaStream_t s = (cudaStream_t)stream;
+    cudaError_t e;
+    if (d->precision == NUOSC_FP64) {
+        StageArgs<double> a{};
+        a.in = (const double *)in;
+        a.acc_dst = (double *)out;
+        a.mom_in = scratch;
+        a.q = q;
+        a.g = g;
+        a.c = c;
+        a.cA = 1.0;
+        e = launch_moments<double>(a.in, scratch, q, g, s);
+        if (e == cudaSuccess) e = launch_stage_direct<double>(a, MODE_RHS, ko6, s);
+    } else {
+        StageArgs<float> a{};
+        a.in = (const float *)in;
+        a.acc_dst = (float *)out;
+        a.mom_in = scratch;
+        a.q = q;
+        a.g = g;
+        a.c = c;
+        a.cA = 1.0;
+        e = launch_moments<float>(a.in, scratch, q, g, s);
+        if (e == cudaSuccess) e = launch_stage_direct<float>(a, MODE_RHS, ko6, s);
+    }
+    if (e != cudaSuccess) return fail(NUOSC_ERR_CUDA, cudaGetErrorString(e));
+    return NUOSC_OK;
+}
