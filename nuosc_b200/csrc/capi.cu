@@ -266,7 +266,8 @@ int run_stage_xmarch(nuosc_handle *h, bool tma, int mode, int in, int u, int acc
     else CUDA_TRY(launch_stage_xmarch<T>(a, mode, h->ko6, h->tile, h->stream));
     h->prof_end(ps);
     ps = h->prof_begin(5);
-    CUDA_TRY(launch_moment_finalize(h->d_part, h->d_mom, h->g, xmarch_num_vblocks(h->g, h->tile), h->stream));
+    const int nvb = tma ? xtma_num_vblocks<T>(h->g) : xmarch_num_vblocks(h->g, h->tile);
+    CUDA_TRY(launch_moment_finalize(h->d_part, h->d_mom, h->g, nvb, h->stream));
     h->prof_end(ps);
     h->launches += 2;
     h->mom_valid = true;  // d_mom now holds the moments of the register this stage wrote

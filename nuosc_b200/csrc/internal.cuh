@@ -84,6 +84,9 @@ template <typename T>
 bool xtma_supported(const Geom &g, XTile t);
 template <typename T>
 cudaError_t launch_stage_xtma(const StageArgs<T> &a, int mode, bool ko6, XTile t, cudaStream_t s);
+// velocity blocks of the TMA kernel's moment partials (32 velocities per block in FP64, 64 in FP32)
+template <typename T>
+int xtma_num_vblocks(const Geom &g);
 // value a kernel writes into StageArgs::status when a bounded wait expires
 constexpr int NUOSC_TIMEOUT_CODE = 1;
 

@@ -1,11 +1,12 @@
 // xtma.cu -- TMA-fed x-march stage kernel (the fast path of the fused stage).
 //
 // Same arithmetic and per-thread structure as xmarch.cu (one (z, v) column per
-// thread, (2R+1)-deep register queue in x, fused RK epilogue and moment
-// partials), with Blackwell-native data movement:
+// thread -- two adjacent velocities per thread in FP32 --, a (2R+1)-deep
+// register queue in x, fused RK epilogue and moment partials), with
+// Blackwell-native data movement:
 //   * box ring: for every x plane the CTA touches, lane 0 of warp 0 issues one
 //     TMA tensor load (cp.async.bulk.tensor.4d; 2-3 boxes where the periodic z
-//     wrap cuts it) of the plane's [TZ+2R rows][4 fields][32 velocities] box
+//     wrap cuts it) of the plane's [TZ+2R rows][4 fields][VB velocities] box
 //     and a bulk copy of the TZ cells' moments into a ring slot whose
 //     completion is tracked by a "full" mbarrier (expect_tx bytes).  A box is
 //     used twice: first as the queue front (x+R), R planes later as the
@@ -18,7 +19,7 @@
 //     issued at the top of each plane, before the waits and the stencil;
 //   * moment partials: each lane holds its 16 (12 + 4 zero) partial moments in
 //     a lane-dependent permuted order so that the reduce-scatter over the 32
-//     velocities of the warp needs no selects (15 shuffle-adds + 1).
+//     lanes of the warp needs no selects (15 shuffle-adds + 1).
 // All mbarrier waits are bounded: on expiry the kernel records the timeout in
 // the status word, stops marching and, before returning, waits (again
 // bounded) for the copies it issued.  Requires nz % TZ == 0.
@@ -31,8 +32,17 @@ namespace nuosc {
 
 namespace {
 
-constexpr int VB = 32;
 constexpr unsigned kWaitSpins = 1u << 22;  // bounded mbarrier waits
+
+// velocities per thread and per CTA: FP32 threads take two adjacent velocities
+template <typename T>
+constexpr int vpt() {
+    return sizeof(T) == 4 ? 2 : 1;
+}
+template <typename T>
+constexpr int vblock() {
+    return 32 * vpt<T>();
+}
 
 struct __align__(64) TmaMaps {
     CUtensorMap zr;   // box of TZ+2R rows (plane box with both halos)
@@ -78,11 +88,29 @@ __device__ __forceinline__ void bulk_load(unsigned dst, const void *src, unsigne
                  : "memory");
 }
 
+// VPT consecutive values (8-byte vector access when VPT == 2)
+template <typename T, int N>
+__device__ __forceinline__ void ldv(const T *p, T (&o)[N]) {
+    if constexpr (N == 2) {
+        const float2 t = *reinterpret_cast<const float2 *>(p);
+        o[0] = t.x;
+        o[1] = t.y;
+    } else {
+        o[0] = *p;
+    }
+}
+template <typename T, int N>
+__device__ __forceinline__ void stv(T *p, const T (&o)[N]) {
+    if constexpr (N == 2) *reinterpret_cast<float2 *>(p) = make_float2(o[0], o[1]);
+    else *p = o[0];
+}
+
 constexpr int up128(int x) { return (x + 127) / 128 * 128; }
 
 // one ring slot: box [ZR][4][VB] T | moments [TZ][12] double
 template <typename T, int TZ, int R>
 struct Slot {
+    static constexpr int VB = vblock<T>();
     static constexpr int ZR = TZ + 2 * R;
     static constexpr int box = 0;
     static constexpr int mb = up128(box + (int)sizeof(T) * ZR * 4 * VB);
@@ -136,13 +164,15 @@ constexpr int tma_ctas_per_sm() {
 }  // namespace
 
 template <typename T, int R, int MODE, int TZ, bool VAC>
-__global__ void __launch_bounds__(VB *TZ, tma_ctas_per_sm<T, TZ>())
+__global__ void __launch_bounds__(32 * TZ, tma_ctas_per_sm<T, TZ>())
     k_xtma(const __grid_constant__ TmaMaps maps, const StageArgs<T> a, int LX) {
     using S = Slot<T, TZ, R>;
+    constexpr int NP = vpt<T>();       // velocities per thread
+    constexpr int VB = S::VB;          // velocities per CTA
     constexpr int W = 2 * R + 1;
     constexpr int ZR = S::ZR;
-    constexpr int D = 2;              // boxes issued ahead of their first use
-    constexpr int NS = R + D + 2;     // a box lives from its front use to its centre use, plus slack
+    constexpr int D = 2;               // boxes issued ahead of their first use
+    constexpr int NS = R + D + 2;      // a box lives from its front use to its centre use, plus slack
     extern __shared__ __align__(1024) unsigned char smem[];
     unsigned long long *bars = (unsigned long long *)(smem + NS * S::bytes);  // full[NS], empty[NS]
     __shared__ int s_abort;
@@ -151,15 +181,15 @@ __global__ void __launch_bounds__(VB *TZ, tma_ctas_per_sm<T, TZ>())
     const int tid = threadIdx.x, lane = tid & 31, r = tid >> 5;
     const int z0 = blockIdx.x * TZ;
     const int vb = blockIdx.y;
-    const int v = vb * VB + lane;
-    const bool vact = v < g.nvs;
+    const int v = vb * VB + NP * lane;  // first of this thread's NP velocities
+    const bool vact = v < g.nvs;        // nvs is a multiple of NP, so all NP are active together
     const int seg = blockIdx.z >> 1, half = blockIdx.z & 1;
     const int xs = seg * LX;
     if (xs >= g.nx) return;
     const int xe = min(xs + LX, g.nx);
     const int nplanes = xe - xs;
-    const int nboxes = nplanes + R;   // centres xs..xe-1 and fronts up to xe-1+R
-    const int zr = z0 + r;            // < nz since nz % TZ == 0
+    const int nboxes = nplanes + R;    // centres xs..xe-1 and fronts up to xe-1+R
+    const int zr = z0 + r;             // < nz since nz % TZ == 0
     const long long fs = g.fs;
     const long long P = (long long)g.nz * g.nvs;
     const long long hoff = (long long)half * 4 * fs;
@@ -198,34 +228,63 @@ __global__ void __launch_bounds__(VB *TZ, tma_ctas_per_sm<T, TZ>())
         return true;
     };
 
-    // per-velocity and uniform constants
-    const double vxd = a.q.vx[vc], vyd = a.q.vy[vc], vzd = a.q.vz[vc], wd = vact ? a.q.vw[vc] : 0.0;
-    const T fx = T(vxd * a.c.fxs), fz = T(vzd * a.c.fzs);
+    // per-velocity and uniform constants.  Lane-permuted moment weights: slot i
+    // of this lane holds moment (i ^ perm), moment k = (combo k>>2, weight
+    // k&3); perm = bits 1..4 of the lane.  With two velocities per thread
+    // (FP32) the FP64 per-velocity constants live in shared memory and are
+    // read per plane, which keeps the register queue clear of spills.
+    const int perm = (lane >> 1) & 15;
+    constexpr bool kShared = NP == 2;
+    __shared__ __align__(16) double s_vq[kShared ? 3 : 1][kShared ? VB : 2];          // vx, vy, vz
+    __shared__ __align__(16) double s_wp[kShared ? 32 : 1][kShared ? NP * 4 : 2];     // permuted weights
+    double vxd[NP], vyd[NP], vzd[NP], wperm[NP][4];
+    T fx[NP], fz[NP];
+#pragma unroll
+    for (int p = 0; p < NP; ++p) {
+        vxd[p] = a.q.vx[vc + p];
+        vyd[p] = a.q.vy[vc + p];
+        vzd[p] = a.q.vz[vc + p];
+        fx[p] = T(vxd[p] * a.c.fxs);
+        fz[p] = T(vzd[p] * a.c.fzs);
+        const double wd = vact ? a.q.vw[vc + p] : 0.0;
+        const double v4w[4] = {wd, vxd[p] * wd, vyd[p] * wd, vzd[p] * wd};
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int k = j ^ (perm & 3);
+            wperm[p][j] = k == 0 ? v4w[0] : k == 1 ? v4w[1] : k == 2 ? v4w[2] : v4w[3];
+        }
+    }
+    if constexpr (kShared) {
+        if (r == 0) {
+#pragma unroll
+            for (int p = 0; p < NP; ++p) {
+                s_vq[0][NP * lane + p] = vxd[p];
+                s_vq[1][NP * lane + p] = vyd[p];
+                s_vq[2][NP * lane + p] = vzd[p];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) s_wp[lane][4 * p + j] = wperm[p][j];
+            }
+        }
+        __syncthreads();
+    }
     const T kz3 = T(a.c.kz3), kz2 = T(a.c.kz2), kz1 = T(a.c.kz1);
     const T kx3 = T(a.c.kx3), kx2 = T(a.c.kx2), kx1 = T(a.c.kx1), kc = T(a.c.kc);
     const T mu = T(a.c.mu), p2s = T(2 * a.c.pmo * a.c.st), p2c = T(2 * a.c.pmo * a.c.ct), ps = T(a.c.pmo * a.c.st);
     const T cA = T(a.cA), cY = T(a.cY);
-    // lane-permuted moment weights: slot i of this lane holds moment (i ^ perm),
-    // moment k = (combo k>>2, weight k&3); perm = bits 1..4 of the lane
-    const int perm = (lane >> 1) & 15;
-    double wperm[4];
-    {
-        const double v4w[4] = {wd, vxd * wd, vyd * wd, vzd * wd};
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const int k = j ^ (perm & 3);
-            wperm[j] = k == 0 ? v4w[0] : k == 1 ? v4w[1] : k == 2 ? v4w[2] : v4w[3];
-        }
-    }
     const bool sw1 = (perm >> 2) & 1, sw2 = (perm >> 3) & 1;
 
     // prime the register queue with planes xs-R .. xs+R-1
-    T q[4][W];
+    T q[4][W][NP];
 #pragma unroll
-    for (int p = 0; p < 2 * R; ++p) {
-        const long long o = (long long)wrap_index(xs - R + p, g.nx) * P + own;
+    for (int k = 0; k < 2 * R; ++k) {
+        const long long o = (long long)wrap_index(xs - R + k, g.nx) * P + own;
 #pragma unroll
-        for (int f = 0; f < 4; ++f) q[f][p] = vact ? in[f * fs + o] : T(0);
+        for (int f = 0; f < 4; ++f) {
+            T t[NP];
+            if (vact) ldv<T, NP>(in + f * fs + o, t);
+#pragma unroll
+            for (int p = 0; p < NP; ++p) q[f][k][p] = vact ? t[p] : T(0);
+        }
     }
     bool ok = true;
     if (tid == 0)  // boxes j < R are only centres: skip those past a short segment's end
@@ -238,11 +297,15 @@ __global__ void __launch_bounds__(VB *TZ, tma_ctas_per_sm<T, TZ>())
         const int x = xs + i;
         const long long oc = hoff + (long long)x * P + own;
         // pointwise epilogue inputs first (they are not in the ring)
-        T uin[4], ain[4];
+        T uin[4][NP], ain[4][NP];
 #pragma unroll
         for (int f = 0; f < 4; ++f) {
-            uin[f] = (MODE == MODE_S23 && vact) ? a.u[oc + f * fs] : T(0);
-            ain[f] = (MODE != MODE_S1 && vact) ? a.acc_src[oc + f * fs] : T(0);
+#pragma unroll
+            for (int p = 0; p < NP; ++p) uin[f][p] = ain[f][p] = T(0);
+            if (vact) {
+                if (MODE == MODE_S23) ldv<T, NP>(a.u + oc + f * fs, uin[f]);
+                if (MODE != MODE_S1) ldv<T, NP>(a.acc_src + oc + f * fs, ain[f]);
+            }
         }
         const int jf = i + R, sf = jf % NS, sc = i % NS;
         if (!mbar_wait(smem_u32(&bars[sf]), (unsigned)((jf / NS) & 1)) ||
@@ -252,7 +315,7 @@ __global__ void __launch_bounds__(VB *TZ, tma_ctas_per_sm<T, TZ>())
         }
         const T *fbox = (const T *)(smem + sf * S::bytes + S::box);
 #pragma unroll
-        for (int f = 0; f < 4; ++f) q[f][2 * R] = fbox[((R + r) * 4 + f) * VB + lane];
+        for (int f = 0; f < 4; ++f) ldv<T, NP>(&fbox[((R + r) * 4 + f) * VB + NP * lane], q[f][2 * R]);
         if (jf >= nplanes) {  // this box is never a centre: its front use was the last
             __syncwarp();
             if (lane == 0) mbar_arrive(smem_u32(&bars[NS + sf]));
@@ -261,16 +324,24 @@ __global__ void __launch_bounds__(VB *TZ, tma_ctas_per_sm<T, TZ>())
         const T *zb = (const T *)(sp + S::box);
         const double *mb = (const double *)(sp + S::mb);
 
-        T sten[4], cen[4];
+        T sten[4][NP];
 #pragma unroll
         for (int f = 0; f < 4; ++f) {
-            T zs[W];
+            T zs[W][NP];
 #pragma unroll
-            for (int k = 0; k < W; ++k) zs[k] = zb[((r + k) * 4 + f) * VB + lane];
-            cen[f] = q[f][R];
-            T acc = kc * cen[f];
-            acc = axis_terms<T, R>(zs, fz, kz3, kz2, kz1, acc);
-            sten[f] = axis_terms<T, R>(q[f], fx, kx3, kx2, kx1, acc);
+            for (int k = 0; k < W; ++k) ldv<T, NP>(&zb[((r + k) * 4 + f) * VB + NP * lane], zs[k]);
+#pragma unroll
+            for (int p = 0; p < NP; ++p) {
+                T zsp[W], xsp[W];
+#pragma unroll
+                for (int k = 0; k < W; ++k) {
+                    zsp[k] = zs[k][p];
+                    xsp[k] = q[f][k][p];
+                }
+                T acc = kc * xsp[R];
+                acc = axis_terms<T, R>(zsp, fz[p], kz3, kz2, kz1, acc);
+                sten[f][p] = axis_terms<T, R>(xsp, fx[p], kx3, kx2, kx1, acc);
+            }
         }
         double m[NMOM];
         {
@@ -285,48 +356,65 @@ __global__ void __launch_bounds__(VB *TZ, tma_ctas_per_sm<T, TZ>())
         __syncwarp();
         if (lane == 0) mbar_arrive(smem_u32(&bars[NS + sc]));  // centre use is the box's last use
 
-        const T ia = T(inp(m, vxd, vyd, vzd)), ib = T(inp(m + 4, vxd, vyd, vzd)), ie = T(inp(m + 8, vxd, vyd, vzd));
-        T kk[4];
-        rhs_half<T, VAC>(cen, ia, ib, ie, mu, p2s, p2c, ps, sten, kk);
-
-        T outm[4];
+        T outm[4][NP];
 #pragma unroll
-        for (int f = 0; f < 4; ++f) {
-            if (MODE == MODE_S1) {
-                const T A = cen[f] + cA * kk[f];
-                const T Y = cen[f] + cY * kk[f];
-                if (vact) {
-                    a.acc_dst[oc + f * fs] = A;
-                    a.y_dst[oc + f * fs] = Y;
+        for (int p = 0; p < NP; ++p) {
+            const double ux = kShared ? s_vq[0][NP * lane + p] : vxd[p];
+            const double uy = kShared ? s_vq[1][NP * lane + p] : vyd[p];
+            const double uz = kShared ? s_vq[2][NP * lane + p] : vzd[p];
+            const T ia = T(inp(m, ux, uy, uz)), ib = T(inp(m + 4, ux, uy, uz)), ie = T(inp(m + 8, ux, uy, uz));
+            const T cen[4] = {q[0][R][p], q[1][R][p], q[2][R][p], q[3][R][p]};
+            const T st4[4] = {sten[0][p], sten[1][p], sten[2][p], sten[3][p]};
+            T kk[4];
+            rhs_half<T, VAC>(cen, ia, ib, ie, mu, p2s, p2c, ps, st4, kk);
+#pragma unroll
+            for (int f = 0; f < 4; ++f) {
+                if (MODE == MODE_S1) {
+                    uin[f][p] = cen[f] + cA * kk[f];  // A
+                    outm[f][p] = cen[f] + cY * kk[f];  // Y
+                } else if (MODE == MODE_S23) {
+                    ain[f][p] = ain[f][p] + cA * kk[f];
+                    outm[f][p] = uin[f][p] + cY * kk[f];
+                } else {
+                    outm[f][p] = ain[f][p] + cA * kk[f];
                 }
-                outm[f] = Y;
-            } else if (MODE == MODE_S23) {
-                const T A = ain[f] + cA * kk[f];
-                const T Y = uin[f] + cY * kk[f];
-                if (vact) {
-                    a.acc_dst[oc + f * fs] = A;
-                    a.y_dst[oc + f * fs] = Y;
-                }
-                outm[f] = Y;
-            } else {
-                const T A = ain[f] + cA * kk[f];
-                if (vact) a.acc_dst[oc + f * fs] = A;
-                outm[f] = A;
             }
         }
+        if (vact) {
+#pragma unroll
+            for (int f = 0; f < 4; ++f) {
+                if (MODE == MODE_S1) {
+                    stv<T, NP>(a.acc_dst + oc + f * fs, uin[f]);
+                    stv<T, NP>(a.y_dst + oc + f * fs, outm[f]);
+                } else if (MODE == MODE_S23) {
+                    stv<T, NP>(a.acc_dst + oc + f * fs, ain[f]);
+                    stv<T, NP>(a.y_dst + oc + f * fs, outm[f]);
+                } else {
+                    stv<T, NP>(a.acc_dst + oc + f * fs, outm[f]);
+                }
+            }
+        }
+        // velocity-moment partials of the written state (nuosc_class.cpp:69-71)
         {
-            double d0, d1, d2;
-            if (half == 0) moment_terms<false>(outm[0], outm[1], outm[2], outm[3], d0, d1, d2);
-            else moment_terms<true>(outm[0], outm[1], outm[2], outm[3], d0, d1, d2);
-            if (!vact) d0 = d1 = d2 = 0.0;
-            // combos in slot order: dperm[c] = d[c ^ (perm >> 2)], d[3] = 0
-            const double t0 = sw1 ? d1 : d0, t1 = sw1 ? d0 : d1, t2 = sw1 ? 0.0 : d2, t3 = sw1 ? d2 : 0.0;
-            const double dp[4] = {sw2 ? t2 : t0, sw2 ? t3 : t1, sw2 ? t0 : t2, sw2 ? t1 : t3};
             double mp[16];
 #pragma unroll
-            for (int c = 0; c < 4; ++c)
+            for (int k = 0; k < 16; ++k) mp[k] = 0.0;
 #pragma unroll
-                for (int j = 0; j < 4; ++j) mp[4 * c + j] = wperm[j] * dp[c];
+            for (int p = 0; p < NP; ++p) {
+                double d0, d1, d2;
+                if (half == 0) moment_terms<false>(outm[0][p], outm[1][p], outm[2][p], outm[3][p], d0, d1, d2);
+                else moment_terms<true>(outm[0][p], outm[1][p], outm[2][p], outm[3][p], d0, d1, d2);
+                if (!vact) d0 = d1 = d2 = 0.0;
+                // combos in slot order: dp[c] = d[c ^ (perm >> 2)], d[3] = 0
+                const double t0 = sw1 ? d1 : d0, t1 = sw1 ? d0 : d1, t2 = sw1 ? 0.0 : d2, t3 = sw1 ? d2 : 0.0;
+                const double dp[4] = {sw2 ? t2 : t0, sw2 ? t3 : t1, sw2 ? t0 : t2, sw2 ? t1 : t3};
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const double wj = kShared ? s_wp[lane][4 * p + j] : wperm[p][j];
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) mp[4 * c + j] = fma(wj, dp[c], mp[4 * c + j]);
+                }
+            }
             rs_step<16, 16>(mp);
             rs_step<8, 8>(mp);
             rs_step<4, 4>(mp);
@@ -340,7 +428,9 @@ __global__ void __launch_bounds__(VB *TZ, tma_ctas_per_sm<T, TZ>())
 #pragma unroll
         for (int f = 0; f < 4; ++f)
 #pragma unroll
-            for (int k = 0; k < 2 * R; ++k) q[f][k] = q[f][k + 1];
+            for (int k = 0; k < 2 * R; ++k)
+#pragma unroll
+                for (int p = 0; p < NP; ++p) q[f][k][p] = q[f][k + 1][p];
     }
     __syncthreads();
     if (tid == 0 && s_abort) {
@@ -375,7 +465,7 @@ EncodeFn encode_fn() {
     return fn;
 }
 
-// 4D view of one register: (v, field, z, x) with box {32, 4, rows, 1}
+// 4D view of one register: (v, field, z, x) with box {VB, 4, rows, 1}
 template <typename T>
 bool make_map(CUtensorMap *m, const T *base, const Geom &g, int rows) {
     EncodeFn fn = encode_fn();
@@ -383,7 +473,7 @@ bool make_map(CUtensorMap *m, const T *base, const Geom &g, int rows) {
     const cuuint64_t dims[4] = {(cuuint64_t)g.nvs, 8, (cuuint64_t)g.nz, (cuuint64_t)g.nx};
     const cuuint64_t strides[3] = {(cuuint64_t)g.fs * sizeof(T), (cuuint64_t)g.nvs * sizeof(T),
                                    (cuuint64_t)g.nz * g.nvs * sizeof(T)};
-    const cuuint32_t box[4] = {(cuuint32_t)VB, 4, (cuuint32_t)rows, 1};
+    const cuuint32_t box[4] = {(cuuint32_t)vblock<T>(), 4, (cuuint32_t)rows, 1};
     const cuuint32_t estr[4] = {1, 1, 1, 1};
     const CUtensorMapDataType dt = sizeof(T) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
     return fn(m, dt, 4, (void *)base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
@@ -405,8 +495,8 @@ cudaError_t launch_t(const StageArgs<T> &a, XTile t, cudaStream_t s) {
                                          (int)smem);
     if (e != cudaSuccess) return e;
     const int nseg = (a.g.nx + t.lx - 1) / t.lx;
-    dim3 grid(a.g.nz / TZ, (a.g.nvs + VB - 1) / VB, nseg * 2);
-    k_xtma<T, R, MODE, TZ, VAC><<<grid, VB * TZ, smem, s>>>(maps, a, t.lx);
+    dim3 grid(a.g.nz / TZ, (a.g.nvs + Sl::VB - 1) / Sl::VB, nseg * 2);
+    k_xtma<T, R, MODE, TZ, VAC><<<grid, 32 * TZ, smem, s>>>(maps, a, t.lx);
     return cudaGetLastError();
 }
 
@@ -429,7 +519,13 @@ cudaError_t launch_tv(const StageArgs<T> &a, int mode, XTile t, cudaStream_t s) 
 
 template <typename T>
 bool xtma_supported(const Geom &g, XTile t) {
-    return (t.tz == 8 || t.tz == 16) && g.nz % t.tz == 0 && g.nx >= 4 && encode_fn() != nullptr;
+    return (t.tz == 8 || t.tz == 16) && g.nz % t.tz == 0 && g.nx >= 4 && g.nvs % vpt<T>() == 0 &&
+           encode_fn() != nullptr;
+}
+
+template <typename T>
+int xtma_num_vblocks(const Geom &g) {
+    return (g.nvs + vblock<T>() - 1) / vblock<T>();
 }
 
 template <typename T>
@@ -441,6 +537,8 @@ cudaError_t launch_stage_xtma(const StageArgs<T> &a, int mode, bool ko6, XTile t
 
 template bool xtma_supported<double>(const Geom &, XTile);
 template bool xtma_supported<float>(const Geom &, XTile);
+template int xtma_num_vblocks<double>(const Geom &);
+template int xtma_num_vblocks<float>(const Geom &);
 template cudaError_t launch_stage_xtma<double>(const StageArgs<double> &, int, bool, XTile, cudaStream_t);
 template cudaError_t launch_stage_xtma<float>(const StageArgs<float> &, int, bool, XTile, cudaStream_t);
 

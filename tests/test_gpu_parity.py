@@ -333,6 +333,30 @@ def test_fp32_tracks_fp64(nb):
     assert d[:, 6].max() < 1e-6      # |M0|
 
 
+FP32_TOL = 2e-5  # norm-wise, FP32 state after 10 steps against the FP64 oracle
+
+
+@pytest.mark.parametrize("pmo", [0.0, 0.3])
+def test_fp32_kernels_against_oracle(nb, pmo):
+    """FP32 state (two velocities per thread in the TMA kernel, one in the
+    others), FP64 moments: every stage kernel stays within FP32 rounding of the
+    FP64 oracle on a 32x32 x 162 case."""
+    p = box_params(32, 4, pmo=pmo)
+    o = po.Oracle(nn=4, x0=p[0], x1=p[1], z0=p[0], z1=p[1], dx=0.1, dz=0.1, cfl=0.4, ko=0.1, ko_order=6, pmo=pmo)
+    o.fill_init(ipt=1, seed=8, alpha=1.2, eps0=1e-3, sigma=1.0, lnue=0.6, lnueb=0.4)
+    o.step(10)
+    ref = o.get_state(0)
+    for kernel in KERNELS:
+        s = make(nb, p, 6, precision=nb.FP32)
+        s.fillInitValue(1, seed=8, alpha=1.2, eps0=1e-3, sigma=1.0, lnue=0.6, lnueb=0.4)
+        s.set_kernel(kernel)
+        s.step_rk4(10)
+        st = s.get_state()
+        for f in range(8):
+            assert po.relerr(st[f], ref[f]) < FP32_TOL, (kernel, f)
+        s.close()
+
+
 def test_launch_count(nb):
     s = make(nb, box_params(16, 2), 6)
     s.fillInitValue(1, seed=1, **PHYS)
