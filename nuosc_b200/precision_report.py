@@ -33,7 +33,7 @@ def run(precision, size, nn, steps, every, hard, device=0, seed=20240601, dx=0.0
         s.fillInitValue(1, 0.9, 1e-6, 1.0, 0.6, 0.5, seed=seed)
     stream = torch.cuda.ExternalStream(nb.lib().nuosc_stream(s.handle))
     series = [s.analysis()]
-    total_ms = 0.0
+    total_ms, done = 0.0, 0
     for _ in range(steps // every):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
@@ -41,9 +41,15 @@ def run(precision, size, nn, steps, every, hard, device=0, seed=20240601, dx=0.0
         e1.record(stream)
         e1.synchronize()
         total_ms += e0.elapsed_time(e1)
-        series.append(s.analysis())
+        done += every
+        try:
+            series.append(s.analysis())
+        except nb.NuoscError as e:  # the scheme left max||P|-1| < 10 (the reference asserts there)
+            if e.code != 4:
+                raise
+            break
     s.close()
-    return series, total_ms / max(1, (steps // every) * every)
+    return series, total_ms / max(1, done)
 
 
 def report(size, nn, steps, every, hard):
@@ -55,6 +61,7 @@ def report(size, nn, steps, every, hard):
                      "fp64": {k: a[k] for k in KEYS}})
     worst = {("max_d_" + k): max(r["d_" + k] for r in rows) for k in KEYS}
     return {"size": size, "nv": 10 * nn * nn + 2, "steps": steps, "every": every, "hard": hard,
+            "compared_to_step": every * (len(rows) - 1), "fp64_outputs": len(s64), "fp32_outputs": len(s32),
             "ms_per_step_fp64": ms64, "ms_per_step_fp32": ms32, "fp32_speedup": ms64 / ms32,
             "worst": worst, "final": rows[-1], "series": rows}
 
