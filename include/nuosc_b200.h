@@ -233,6 +233,44 @@ typedef struct nuosc_rhs_desc {
 } nuosc_rhs_desc;
 int nuosc_calrhs_noalloc(const nuosc_rhs_desc *desc, const void *in, void *out, void *stream);
 
+/* ---- batched stepping of many independent solves -----------------------
+ * No counterpart in the reference, which runs one NuOsc per process
+ * (nuosc.cpp:171-240).  A batch steps several handles (instances of possibly
+ * different nx, nz, nv, mu, pmo, initial data) together: each RK stage is ONE
+ * persistent kernel whose CTAs take tiles of all instances from a work-list
+ * (largest instances first), then one moment-finalize kernel for all; the
+ * whole step is captured once in a CUDA graph and replayed.  Every instance's
+ * result is bit-for-bit the result of nuosc_step_rk4 on that handle alone.
+ *   - members share device, precision and ghost width (KO order); every
+ *     member needs nz % 8 == 0 and nz >= 14 (the TMA march kernel; nz % 16
+ *     == 0 and nz >= 22 for all members selects 16-row tiles);
+ *   - a handle belongs to at most one live batch and must outlive it;
+ *     members stay usable alone (analysis, snapshots, set_state ...) between
+ *     batch steps; nuosc_batch_step orders itself after work queued on the
+ *     members' streams and the members' streams after it;
+ *   - mu, pmo, renorm and tile changes on a member are picked up at the next
+ *     nuosc_batch_step (the work-list is rebuilt). */
+typedef struct nuosc_batch nuosc_batch;
+typedef struct nuosc_batch_info {
+    int n;                     /* instances */
+    int tz;                    /* z rows per tile */
+    int ctas;                  /* CTAs of each persistent stage launch */
+    long long tiles;           /* tiles per stage launch, all instances */
+    long long cells;           /* x-z cells, all instances */
+    long long cell_velocities; /* sum of nx*nz*nv: the work unit of one step */
+    size_t device_bytes;       /* sum of the members' device memory */
+    long long graph_launches;  /* step graphs replayed so far */
+    long long kernel_launches; /* kernels those replays ran (plus moment passes) */
+} nuosc_batch_info;
+int nuosc_batch_create(nuosc_handle *const *members, int n, nuosc_batch **out);
+/* nsteps RK4 steps of every member (nuosc_step_rk4 on each); asynchronous */
+int nuosc_batch_step(nuosc_batch *b, int nsteps);
+/* wait for the batch and check every member's in-kernel status word */
+int nuosc_batch_synchronize(nuosc_batch *b);
+int nuosc_batch_get_info(const nuosc_batch *b, nuosc_batch_info *info);
+void *nuosc_batch_stream(nuosc_batch *b);
+int nuosc_batch_destroy(nuosc_batch *b);
+
 #ifdef __cplusplus
 }
 #endif

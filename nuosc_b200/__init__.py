@@ -24,7 +24,7 @@ from . import _lib
 from ._lib import (FP32, FP64, KERNEL_AUTO, KERNEL_DIRECT, KERNEL_XMARCH, KERNEL_XTMA, LAYOUT_COMPACT,
                    LAYOUT_GHOSTED, REG_COR, REG_PRE, REG_RHS, REG_STAT, FIELDS, NuoscError, check, lib)
 
-__all__ = ["NuOsc", "NuoscError", "FP32", "FP64", "REG_STAT", "REG_RHS", "REG_PRE", "REG_COR",
+__all__ = ["NuOsc", "Batch", "NuoscError", "FP32", "FP64", "REG_STAT", "REG_RHS", "REG_PRE", "REG_COR",
            "KERNEL_AUTO", "KERNEL_DIRECT", "KERNEL_XMARCH", "KERNEL_XTMA", "FIELDS", "lib"]
 
 lib()  # fail at import time if the CUDA library is missing
@@ -89,7 +89,7 @@ class NuOsc:
     # ------------------------------------------------------------ lifetime
     def close(self):
         if getattr(self, "_h", None):
-            lib().nuosc_destroy(self._h)
+            check(lib().nuosc_destroy(self._h))  # refused while the handle is in a live Batch
             self._h = None
 
     def __del__(self):
@@ -267,3 +267,57 @@ class NuOsc:
         out = np.zeros((len(xidx), self.grid.nz, len(vidx)))
         check(lib().nuosc_gather(self._h, f, _ip(xidx), len(xidx), _ip(vidx), len(vidx), _dp(out)))
         return out
+
+
+class Batch:
+    """Several NuOsc instances stepped together (nuosc_batch_* of the C ABI).
+
+    Each RK stage of a batch step is one persistent kernel over the tiles of
+    all members, and the step is one CUDA graph replay; every member's state
+    after `step_rk4(n)` is bit-for-bit what `member.step_rk4(n)` gives alone.
+    Members must share device, precision and ghost width and have nz % 8 == 0,
+    nz >= 14.  The batch keeps its members alive; close() (or the context
+    manager) releases the batch, after which members can be closed.
+    """
+
+    def __init__(self, members):
+        self.members = list(members)
+        hs = (C.c_void_p * len(self.members))(*[m.handle for m in self.members])
+        b = C.c_void_p()
+        check(lib().nuosc_batch_create(hs, len(self.members), C.byref(b)))
+        self._b = b
+
+    def close(self):
+        if getattr(self, "_b", None):
+            lib().nuosc_batch_destroy(self._b)
+            self._b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._b
+
+    def step_rk4(self, nsteps=1):
+        check(lib().nuosc_batch_step(self._b, int(nsteps)))
+
+    def synchronize(self):
+        check(lib().nuosc_batch_synchronize(self._b))
+
+    def stream(self):
+        return lib().nuosc_batch_stream(self._b)
+
+    def info(self):
+        i = _lib.BatchInfo()
+        check(lib().nuosc_batch_get_info(self._b, C.byref(i)))
+        return i.as_dict()

@@ -50,6 +50,15 @@ class Diag(C.Structure):
         return {n: getattr(self, n) for n, _ in self._fields_}
 
 
+class BatchInfo(C.Structure):
+    _fields_ = [("n", C.c_int), ("tz", C.c_int), ("ctas", C.c_int), ("tiles", C.c_longlong),
+                ("cells", C.c_longlong), ("cell_velocities", C.c_longlong), ("device_bytes", C.c_size_t),
+                ("graph_launches", C.c_longlong), ("kernel_launches", C.c_longlong)]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
 _P = C.c_void_p
 _I = C.c_int
 _D = C.c_double
@@ -88,6 +97,11 @@ _SIGS = {
     "nuosc_synchronize": [_P],
     "nuosc_set_profiling": [_P, _I],
     "nuosc_get_profile": [_P, _DP, C.POINTER(C.c_longlong), _I],
+    "nuosc_batch_create": [C.POINTER(_P), _I, C.POINTER(_P)],
+    "nuosc_batch_step": [_P, _I],
+    "nuosc_batch_synchronize": [_P],
+    "nuosc_batch_get_info": [_P, C.POINTER(BatchInfo)],
+    "nuosc_batch_destroy": [_P],
 }
 PROF_KINDS = ["stage_s1", "stage_s23", "stage_s4", "calrhs", "moments", "moment_finalize"]
 
@@ -111,6 +125,8 @@ def lib():
         L.nuosc_stream.argtypes = [_P]
         L.nuosc_kernel_launches.restype = C.c_longlong
         L.nuosc_kernel_launches.argtypes = [_P]
+        L.nuosc_batch_stream.restype = _P
+        L.nuosc_batch_stream.argtypes = [_P]
         _lib = L
     return _lib
 

@@ -88,6 +88,7 @@ struct nuosc_handle {
     XTile tile{16, 64, 32};
     long long launches = 0;
     bool mom_valid = false;  // d_mom holds the moments of v_stat
+    nuosc_batch *batch = nullptr;  // the live batch this handle belongs to
 
     std::vector<double> vx, vy, vz, vw, G0, G0b;  // host copies (length nv)
     void *reg[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -239,8 +240,8 @@ int run_stage_direct(nuosc_handle *h, int mode, int in, int u, int acc_src, int 
 
 // one RK4 stage in the x-march path (moments of the stage output fused)
 template <typename T>
-int run_stage_xmarch(nuosc_handle *h, bool tma, int mode, int in, int u, int acc_src, int acc_dst, int y_dst,
-                     double cA, double cY) {
+int run_stage_xmarch(nuosc_handle *h, bool tma, const XTile &tile, int mode, int in, int u, int acc_src, int acc_dst,
+                     int y_dst, double cA, double cY) {
     StageArgs<T> a{};
     a.in = (const T *)h->reg[in];
     a.u = u >= 0 ? (const T *)h->reg[u] : nullptr;
@@ -262,11 +263,11 @@ int run_stage_xmarch(nuosc_handle *h, bool tma, int mode, int in, int u, int acc
         h->launches++;
     }
     int ps = h->prof_begin(prof_kind(mode));
-    if (tma) CUDA_TRY(launch_stage_xtma<T>(a, mode, h->ko6, h->tile, h->stream));
-    else CUDA_TRY(launch_stage_xmarch<T>(a, mode, h->ko6, h->tile, h->stream));
+    if (tma) CUDA_TRY(launch_stage_xtma<T>(a, mode, h->ko6, tile, h->stream));
+    else CUDA_TRY(launch_stage_xmarch<T>(a, mode, h->ko6, tile, h->stream));
     h->prof_end(ps);
     ps = h->prof_begin(5);
-    const int nvb = tma ? xtma_num_vblocks<T>(h->g) : xmarch_num_vblocks(h->g, h->tile);
+    const int nvb = tma ? xtma_num_vblocks<T>(h->g) : xmarch_num_vblocks(h->g, tile);
     CUDA_TRY(launch_moment_finalize(h->d_part, h->d_mom, h->g, nvb, h->stream));
     h->prof_end(ps);
     h->launches += 2;
@@ -274,10 +275,18 @@ int run_stage_xmarch(nuosc_handle *h, bool tma, int mode, int in, int u, int acc
     return 0;
 }
 
-// stage-kernel path for this handle: 0 direct, 1 cp.async x-march, 2 TMA x-march (-1: unsupported request)
+// stage-kernel path for this handle: 0 direct, 1 cp.async x-march, 2 TMA x-march (-1: unsupported request).
+// `tile` is the handle's tile, with 8-row tiles in place of 16-row ones when
+// nz only fits those (the TMA kernel is preferred at either height).
 template <typename T>
-int stage_path(nuosc_handle *h) {
-    const bool tma = xtma_supported<T>(h->g, h->tile), cpa = xmarch_supported<T>(h->g, h->ko6, h->tile);
+int stage_path(nuosc_handle *h, XTile &tile) {
+    tile = h->tile;
+    if (!xtma_supported<T>(h->g, tile) && tile.tz == 16) {
+        XTile t8 = tile;
+        t8.tz = 8;
+        if (xtma_supported<T>(h->g, t8)) tile = t8;
+    }
+    const bool tma = xtma_supported<T>(h->g, tile), cpa = xmarch_supported<T>(h->g, h->ko6, h->tile);
     switch (h->kernel) {
     case NUOSC_KERNEL_DIRECT: return 0;
     case NUOSC_KERNEL_XMARCH: return cpa ? 1 : -1;
@@ -291,9 +300,11 @@ int stage_path(nuosc_handle *h) {
 template <typename T>
 int step_impl(nuosc_handle *h, int nsteps) {
     const double dt = h->dt;
-    const int path = stage_path<T>(h);
+    XTile tile;
+    const int path = stage_path<T>(h, tile);
     if (path < 0) return fail(NUOSC_ERR_UNSUPPORTED, "the requested stage kernel does not support this geometry/tile");
     const bool xm = path > 0, tma = path == 2;
+    if (!tma) tile = h->tile;
     if (xm) {
         const size_t need = (size_t)h->g.ncell * xmarch_num_vblocks(h->g, h->tile) * 2 * NMOM * sizeof(double);
         if (int rc = ensure((void **)&h->d_part, &h->part_bytes, need, h)) return rc;
@@ -301,10 +312,10 @@ int step_impl(nuosc_handle *h, int nsteps) {
     for (int n = 0; n < nsteps; ++n) {
         int rc;
         if (xm) {
-            if ((rc = run_stage_xmarch<T>(h, tma, MODE_S1, 0, -1, -1, 1, 2, dt / 6.0, 0.5 * dt))) return rc;
-            if ((rc = run_stage_xmarch<T>(h, tma, MODE_S23, 2, 0, 1, 1, 3, dt / 3.0, 0.5 * dt))) return rc;
-            if ((rc = run_stage_xmarch<T>(h, tma, MODE_S23, 3, 0, 1, 1, 2, dt / 3.0, dt))) return rc;
-            if ((rc = run_stage_xmarch<T>(h, tma, MODE_S4, 2, -1, 1, 0, -1, dt / 6.0, 0.0))) return rc;
+            if ((rc = run_stage_xmarch<T>(h, tma, tile, MODE_S1, 0, -1, -1, 1, 2, dt / 6.0, 0.5 * dt))) return rc;
+            if ((rc = run_stage_xmarch<T>(h, tma, tile, MODE_S23, 2, 0, 1, 1, 3, dt / 3.0, 0.5 * dt))) return rc;
+            if ((rc = run_stage_xmarch<T>(h, tma, tile, MODE_S23, 3, 0, 1, 1, 2, dt / 3.0, dt))) return rc;
+            if ((rc = run_stage_xmarch<T>(h, tma, tile, MODE_S4, 2, -1, 1, 0, -1, dt / 6.0, 0.0))) return rc;
         } else {
             if ((rc = run_stage_direct<T>(h, MODE_S1, 0, -1, -1, 1, 2, dt / 6.0, 0.5 * dt))) return rc;
             h->mom_valid = false;
@@ -612,6 +623,7 @@ int nuosc_create(const nuosc_params *p, nuosc_handle **out) {
 
 int nuosc_destroy(nuosc_handle *h) {
     if (!h) return NUOSC_OK;
+    if (h->batch) return fail(NUOSC_ERR_INVALID, "destroy: the handle is a member of a live batch");
     cudaSetDevice(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
     h->prof_collect();
@@ -936,6 +948,313 @@ int nuosc_get_profile(nuosc_handle *h, double *ms, long long *launches, int nkin
         h->prof_ms[k] = 0;
         h->prof_n[k] = 0;
     }
+    return NUOSC_OK;
+}
+
+}  // extern "C"
+
+// ====================================================================== batch
+// Many independent solves stepped together (no counterpart in the reference).
+// Per RK stage: one persistent TMA march kernel over the tiles of all members
+// (work-list ordered largest member first), then one moment-finalize kernel
+// for all members.  One step is captured in a CUDA graph and replayed.
+
+struct nuosc_batch {
+    int device = 0;
+    int precision = NUOSC_FP64;
+    bool ko6 = true;
+    int tz = 16;
+    std::vector<nuosc_handle *> m;  // service order: largest first
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev = nullptr;
+    char *d_buf = nullptr;          // stage tables | tile starts | finalize table | cell starts | counters
+    size_t item_bytes = 0;
+    long long *d_starts = nullptr;
+    FinalizeItem *d_fin = nullptr;
+    long long *d_fstarts = nullptr;
+    unsigned long long *d_counter = nullptr;
+    long long ntiles = 0, nmom = 0, cells = 0, cellv = 0;
+    int grid[4] = {0, 0, 0, 0};
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<double> sig;        // member settings the tables were built from
+    long long graph_launches = 0, kernel_launches = 0, per_step = 0;
+};
+
+namespace {
+
+// RK4 stage k of step_impl's x-march sequence: (mode, in, u, acc_src, acc_dst,
+// y_dst) with cA = dt / da and cY = fy * dt, the same expressions as step_impl
+struct StageSpec {
+    int mode, in, u, acc_src, acc_dst, y_dst;
+    double da, fy;
+};
+constexpr StageSpec kStages[4] = {{MODE_S1, 0, -1, -1, 1, 2, 6.0, 0.5},
+                                  {MODE_S23, 2, 0, 1, 1, 3, 3.0, 0.5},
+                                  {MODE_S23, 3, 0, 1, 1, 2, 3.0, 1.0},
+                                  {MODE_S4, 2, -1, 1, 0, -1, 6.0, 0.0}};
+
+std::vector<double> batch_signature(const nuosc_batch *b) {
+    std::vector<double> s;
+    for (const nuosc_handle *h : b->m) {
+        s.push_back(h->mu);
+        s.push_back(h->pmo);
+        s.push_back(h->dt);
+        s.push_back(h->tile.lx);
+        s.push_back(h->renorm ? 1.0 : 0.0);
+        s.push_back((double)(uintptr_t)h->d_part);
+    }
+    return s;
+}
+
+void batch_release_graph(nuosc_batch *b) {
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    b->exec = nullptr;
+    b->graph = nullptr;
+}
+
+// (re)build the device tables and the step graph from the members' current settings
+template <typename T>
+int batch_build(nuosc_batch *b) {
+    const int n = (int)b->m.size();
+    CUDA_TRY(cudaStreamSynchronize(b->stream));  // no replay still reads the tables
+    batch_release_graph(b);
+    for (nuosc_handle *h : b->m) {
+        const size_t need = (size_t)h->g.ncell * xmarch_num_vblocks(h->g, h->tile) * 2 * NMOM * sizeof(double);
+        if (int rc = ensure((void **)&h->d_part, &h->part_bytes, need, h)) return rc;
+    }
+    b->item_bytes = xtma_batch_item_bytes<T>();
+    const size_t tab = 4 * (size_t)n * b->item_bytes;
+    std::vector<char> host(tab);
+    std::vector<long long> starts(n), fstarts(n);
+    std::vector<FinalizeItem> fin(n);
+    long long tiles = 0, nmom = 0;
+    for (int i = 0; i < n; ++i) {
+        nuosc_handle *h = b->m[i];
+        long long ti = -1;
+        for (int k = 0; k < 4; ++k) {
+            const StageSpec &sp = kStages[k];
+            StageArgs<T> a{};
+            a.in = (const T *)h->reg[sp.in];
+            a.u = sp.u >= 0 ? (const T *)h->reg[sp.u] : nullptr;
+            a.acc_src = sp.acc_src >= 0 ? (const T *)h->reg[sp.acc_src] : nullptr;
+            a.acc_dst = (T *)h->reg[sp.acc_dst];
+            a.y_dst = sp.y_dst >= 0 ? (T *)h->reg[sp.y_dst] : nullptr;
+            a.mom_in = h->d_mom;
+            a.mom_part = h->d_part;
+            a.q = h->quad();
+            a.g = h->g;
+            a.c = h->coeffs();
+            a.cA = h->dt / sp.da;
+            a.cY = sp.fy == 1.0 ? h->dt : sp.fy * h->dt;
+            a.status = h->d_status;
+            ti = xtma_batch_fill<T>(&host[((size_t)k * n + i) * b->item_bytes], a, b->ko6, b->tz, h->tile.lx);
+            if (ti < 0) return fail(NUOSC_ERR_UNSUPPORTED, "batch member %d (%dx%d) cannot run %d-row TMA tiles", i,
+                                    h->g.nx, h->g.nz, b->tz);
+        }
+        starts[i] = tiles;
+        tiles += ti;
+        fin[i] = FinalizeItem{h->d_part, h->d_mom, h->g.ncell, xtma_num_vblocks<T>(h->g)};
+        fstarts[i] = nmom;
+        nmom += h->g.ncell * NMOM;
+    }
+    if (!b->d_buf) {
+        const size_t bytes = tab + 2 * (size_t)n * sizeof(long long) + (size_t)n * sizeof(FinalizeItem) + 256;
+        CUDA_TRY(cudaMalloc((void **)&b->d_buf, bytes));
+        size_t off = tab;
+        b->d_starts = (long long *)(b->d_buf + off);
+        off += (size_t)n * sizeof(long long);
+        b->d_fstarts = (long long *)(b->d_buf + off);
+        off += (size_t)n * sizeof(long long);
+        b->d_fin = (FinalizeItem *)(b->d_buf + off);
+        off += (size_t)n * sizeof(FinalizeItem);
+        b->d_counter = (unsigned long long *)(b->d_buf + (off + 63) / 64 * 64);
+    }
+    CUDA_TRY(cudaMemcpyAsync(b->d_buf, host.data(), tab, cudaMemcpyHostToDevice, b->stream));
+    CUDA_TRY(cudaMemcpyAsync(b->d_starts, starts.data(), n * sizeof(long long), cudaMemcpyHostToDevice, b->stream));
+    CUDA_TRY(cudaMemcpyAsync(b->d_fstarts, fstarts.data(), n * sizeof(long long), cudaMemcpyHostToDevice, b->stream));
+    CUDA_TRY(cudaMemcpyAsync(b->d_fin, fin.data(), n * sizeof(FinalizeItem), cudaMemcpyHostToDevice, b->stream));
+    CUDA_TRY(cudaStreamSynchronize(b->stream));  // host staging is freed on return
+    b->ntiles = tiles;
+    b->nmom = nmom;
+    for (int k = 0; k < 4; ++k) {
+        b->grid[k] = xtma_batch_grid<T>(kStages[k].mode, b->ko6, b->tz, b->device);
+        if (b->grid[k] < 1) return fail(NUOSC_ERR_CUDA, "batch: cannot size the persistent stage grid");
+    }
+
+    // one step: reset the work counters, 4 x (stage kernel, finalize), renormalisation
+    CUDA_TRY(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    long long per_step = 0;
+    cudaError_t e = cudaMemsetAsync(b->d_counter, 0, 4 * sizeof(unsigned long long), b->stream);
+    for (int k = 0; k < 4 && e == cudaSuccess; ++k) {
+        e = launch_stage_xtma_batch<T>(b->d_buf + (size_t)k * n * b->item_bytes, b->d_starts, n, tiles,
+                                       b->d_counter + k, kStages[k].mode, b->ko6, b->tz, b->grid[k], b->stream);
+        if (e == cudaSuccess) e = launch_moment_finalize_batch(b->d_fin, b->d_fstarts, n, nmom, b->stream);
+        per_step += 2;
+    }
+    for (nuosc_handle *h : b->m) {
+        if (!h->renorm || e != cudaSuccess) continue;
+        e = launch_renormalize<T>((T *)h->reg[0], h->dG0(), h->dG0b(), h->g, b->stream);
+        if (e == cudaSuccess) e = launch_moments<T>((const T *)h->reg[0], h->d_mom, h->quad(), h->g, b->stream);
+        per_step += 2;
+    }
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e2 = cudaStreamEndCapture(b->stream, &graph);
+    if (e != cudaSuccess || e2 != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        return fail(NUOSC_ERR_CUDA, "batch graph capture: %s", cudaGetErrorString(e != cudaSuccess ? e : e2));
+    }
+    b->graph = graph;
+    CUDA_TRY(cudaGraphInstantiate(&b->exec, graph, 0));
+    b->per_step = per_step;
+    b->sig = batch_signature(b);
+    return 0;
+}
+
+template <typename T>
+int batch_step_impl(nuosc_batch *b, int nsteps) {
+    if (batch_signature(b) != b->sig)
+        if (int rc = batch_build<T>(b)) return rc;
+    // after everything queued on the members' streams
+    for (nuosc_handle *h : b->m) {
+        CUDA_TRY(cudaEventRecord(b->ev, h->stream));
+        CUDA_TRY(cudaStreamWaitEvent(b->stream, b->ev, 0));
+    }
+    for (nuosc_handle *h : b->m) {
+        if (h->mom_valid) continue;
+        CUDA_TRY(launch_moments<T>((const T *)h->reg[0], h->d_mom, h->quad(), h->g, b->stream));
+        b->kernel_launches++;
+        h->mom_valid = true;
+    }
+    for (int s = 0; s < nsteps; ++s) {
+        CUDA_TRY(cudaGraphLaunch(b->exec, b->stream));
+        b->graph_launches++;
+        b->kernel_launches += b->per_step;
+    }
+    CUDA_TRY(cudaEventRecord(b->ev, b->stream));
+    for (nuosc_handle *h : b->m) {
+        CUDA_TRY(cudaStreamWaitEvent(h->stream, b->ev, 0));
+        for (int k = 0; k < nsteps; ++k) h->phy_time += h->dt;  // as step_impl: dt added once per step
+    }
+    return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int nuosc_batch_create(nuosc_handle *const *members, int n, nuosc_batch **out) {
+    g_err.clear();
+    if (!members || !out || n < 1) return fail(NUOSC_ERR_INVALID, "batch_create: null argument or empty batch");
+    *out = nullptr;
+    for (int i = 0; i < n; ++i) {
+        const nuosc_handle *h = members[i];
+        if (!h) return fail(NUOSC_ERR_INVALID, "batch member %d is null", i);
+        if (h->batch) return fail(NUOSC_ERR_INVALID, "batch member %d already belongs to a batch", i);
+        for (int j = 0; j < i; ++j)
+            if (members[j] == h) return fail(NUOSC_ERR_INVALID, "batch member %d repeats member %d", i, j);
+        if (h->device != members[0]->device || h->precision != members[0]->precision || h->ko6 != members[0]->ko6)
+            return fail(NUOSC_ERR_UNSUPPORTED, "batch members must share device, precision and ghost width");
+    }
+    auto tz_ok = [&](int tz) {
+        for (int i = 0; i < n; ++i) {
+            const nuosc_handle *h = members[i];
+            const bool ok = h->precision == NUOSC_FP64 ? xtma_supported<double>(h->g, XTile{tz, 32, 32})
+                                                       : xtma_supported<float>(h->g, XTile{tz, 32, 64});
+            if (!ok) return false;
+        }
+        return true;
+    };
+    nuosc_batch *b = new nuosc_batch;
+    b->device = members[0]->device;
+    b->precision = members[0]->precision;
+    b->ko6 = members[0]->ko6;
+    cudaError_t e = cudaSetDevice(b->device);
+    if (e != cudaSuccess) {
+        delete b;
+        return fail(NUOSC_ERR_CUDA, "cudaSetDevice: %s", cudaGetErrorString(e));
+    }
+    b->tz = tz_ok(16) ? 16 : tz_ok(8) ? 8 : 0;
+    if (!b->tz) {
+        delete b;
+        return fail(NUOSC_ERR_UNSUPPORTED, "batch: every member needs nz %% 8 == 0 and nz >= 14");
+    }
+    b->m.assign(members, members + n);
+    std::stable_sort(b->m.begin(), b->m.end(), [](const nuosc_handle *x, const nuosc_handle *y) {
+        return x->g.ncell * x->g.nvs > y->g.ncell * y->g.nvs;
+    });
+    for (const nuosc_handle *h : b->m) {
+        b->cells += h->g.ncell;
+        b->cellv += h->g.ncell * h->g.nv;
+    }
+    auto bail = [&](int rc) {
+        nuosc_batch_destroy(b);
+        return rc;
+    };
+    e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return bail(fail(NUOSC_ERR_CUDA, "cudaStreamCreate: %s", cudaGetErrorString(e)));
+    e = cudaEventCreateWithFlags(&b->ev, cudaEventDisableTiming);
+    if (e != cudaSuccess) return bail(fail(NUOSC_ERR_CUDA, "cudaEventCreate: %s", cudaGetErrorString(e)));
+    for (nuosc_handle *h : b->m) {  // the tables read the members' buffers: let pending work finish
+        e = cudaStreamSynchronize(h->stream);
+        if (e != cudaSuccess) return bail(fail(NUOSC_ERR_CUDA, "batch_create: %s", cudaGetErrorString(e)));
+    }
+    const int rc = b->precision == NUOSC_FP64 ? batch_build<double>(b) : batch_build<float>(b);
+    if (rc) return bail(rc);
+    for (nuosc_handle *h : b->m) h->batch = b;
+    *out = b;
+    return NUOSC_OK;
+}
+
+int nuosc_batch_step(nuosc_batch *b, int nsteps) {
+    if (!b) return fail(NUOSC_ERR_INVALID, "null batch");
+    if (nsteps < 0) return fail(NUOSC_ERR_INVALID, "nsteps %d", nsteps);
+    CUDA_TRY(cudaSetDevice(b->device));
+    const int rc = b->precision == NUOSC_FP64 ? batch_step_impl<double>(b, nsteps) : batch_step_impl<float>(b, nsteps);
+    if (rc) return rc;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(NUOSC_ERR_CUDA, "batch_step: %s", cudaGetErrorString(e));
+    return NUOSC_OK;
+}
+
+int nuosc_batch_synchronize(nuosc_batch *b) {
+    if (!b) return fail(NUOSC_ERR_INVALID, "null batch");
+    CUDA_TRY(cudaSetDevice(b->device));
+    CUDA_TRY(cudaStreamSynchronize(b->stream));
+    for (nuosc_handle *h : b->m)
+        if (int rc = check_status(h)) return rc;
+    return NUOSC_OK;
+}
+
+int nuosc_batch_get_info(const nuosc_batch *b, nuosc_batch_info *o) {
+    if (!b || !o) return fail(NUOSC_ERR_INVALID, "null argument");
+    o->n = (int)b->m.size();
+    o->tz = b->tz;
+    o->ctas = b->grid[1];
+    o->tiles = b->ntiles;
+    o->cells = b->cells;
+    o->cell_velocities = b->cellv;
+    o->device_bytes = 0;
+    for (const nuosc_handle *h : b->m) o->device_bytes += h->device_bytes;
+    o->graph_launches = b->graph_launches;
+    o->kernel_launches = b->kernel_launches;
+    return NUOSC_OK;
+}
+
+void *nuosc_batch_stream(nuosc_batch *b) { return b ? (void *)b->stream : nullptr; }
+
+int nuosc_batch_destroy(nuosc_batch *b) {
+    if (!b) return NUOSC_OK;
+    cudaSetDevice(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    batch_release_graph(b);
+    for (nuosc_handle *h : b->m)
+        if (h->batch == b) h->batch = nullptr;
+    if (b->d_buf) cudaFree(b->d_buf);
+    if (b->ev) cudaEventDestroy(b->ev);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
     return NUOSC_OK;
 }
 

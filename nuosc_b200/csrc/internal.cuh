@@ -87,6 +87,38 @@ cudaError_t launch_stage_xtma(const StageArgs<T> &a, int mode, bool ko6, XTile t
 // velocity blocks of the TMA kernel's moment partials (32 velocities per block in FP64, 64 in FP32)
 template <typename T>
 int xtma_num_vblocks(const Geom &g);
+// Batched TMA stage (xtma.cu): one persistent launch runs one RK stage of many
+// instances.  Each instance has an entry (its tensor maps and StageArgs) in a
+// device table; CTAs take tiles of all instances from an atomic work counter.
+// Tile k of an instance is the tile its own launch runs as CTA k, so each
+// instance gets the same bits as when stepped alone.
+template <typename T>
+size_t xtma_batch_item_bytes();
+// Encodes the table entry of one instance into `item` (host memory,
+// xtma_batch_item_bytes bytes); returns the instance's tile count, or -1 when
+// the instance cannot run with this tz.
+template <typename T>
+long long xtma_batch_fill(void *item, const StageArgs<T> &a, bool ko6, int tz, int lx);
+// CTAs of a persistent launch on `device` (also sets the kernel's dynamic
+// shared-memory limit); -1 on failure
+template <typename T>
+int xtma_batch_grid(int mode, bool ko6, int tz, int device);
+// starts[i] = tiles of instances 0..i-1 (instances ordered as the caller
+// wants them served); counter must be 0 before the launch
+template <typename T>
+cudaError_t launch_stage_xtma_batch(const void *items, const long long *starts, int n, long long ntiles,
+                                    unsigned long long *counter, int mode, bool ko6, int tz, int grid,
+                                    cudaStream_t s);
+// moment_finalize of many instances in one launch (xmarch.cu); starts[i] =
+// sum over instances 0..i-1 of ncell * 12
+struct FinalizeItem {
+    const double *part;
+    double *mom;
+    long long ncell;
+    int nvb;
+};
+cudaError_t launch_moment_finalize_batch(const FinalizeItem *items, const long long *starts, int n, long long total,
+                                         cudaStream_t s);
 // value a kernel writes into StageArgs::status when a bounded wait expires
 constexpr int NUOSC_TIMEOUT_CODE = 1;
 

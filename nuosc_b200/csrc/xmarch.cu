@@ -396,6 +396,36 @@ cudaError_t launch_moment_finalize(const double *part, double *mom, Geom g, int 
     return cudaGetLastError();
 }
 
+namespace {
+// k_moment_finalize over the cells of many instances (same summation order)
+__global__ void k_moment_finalize_batch(const FinalizeItem *__restrict__ items, const long long *__restrict__ starts,
+                                        int n, long long total) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= total) return;
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (starts[mid] <= t) lo = mid;
+        else hi = mid - 1;
+    }
+    const FinalizeItem e = items[lo];
+    const long long u = t - starts[lo];
+    const long long cell = u / NMOM;
+    const int k = (int)(u - cell * NMOM);
+    const double *p = e.part + cell * e.nvb * 2 * NMOM + k;
+    double s = 0.0;
+    for (int b = 0; b < 2 * e.nvb; ++b) s += p[(long long)b * NMOM];
+    e.mom[u] = s;
+}
+}  // namespace
+
+cudaError_t launch_moment_finalize_batch(const FinalizeItem *items, const long long *starts, int n, long long total,
+                                         cudaStream_t s) {
+    if (n < 1 || total < 1) return cudaErrorInvalidValue;
+    k_moment_finalize_batch<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(items, starts, n, total);
+    return cudaGetLastError();
+}
+
 template bool xmarch_supported<double>(const Geom &, bool, XTile);
 template bool xmarch_supported<float>(const Geom &, bool, XTile);
 template cudaError_t launch_stage_xmarch<double>(const StageArgs<double> &, int, bool, XTile, cudaStream_t);

@@ -23,10 +23,16 @@
 // All mbarrier waits are bounded: on expiry the kernel records the timeout in
 // the status word, stops marching and, before returning, waits (again
 // bounded) for the copies it issued.  Requires nz % TZ == 0.
+//
+// The march of one tile is a device function shared by two kernels: k_xtma
+// (one tile per CTA, one instance per launch) and k_xtma_batch (a persistent
+// grid whose CTAs take tiles of many instances from a work-list).
 #include "internal.cuh"
 #include "physics.cuh"
 
 #include <cuda.h>
+
+#include <cstring>
 
 namespace nuosc {
 
@@ -73,6 +79,13 @@ __device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity) {
         if (ok) return true;
     }
     return false;
+}
+// make generic-proxy writes of a tensor map in global memory visible to the TMA
+__device__ __forceinline__ void tensormap_acquire(const CUtensorMap *m) {
+    asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;\n" ::"l"(m) : "memory");
+}
+__device__ __forceinline__ void mbar_inval(unsigned bar) {
+    asm volatile("mbarrier.inval.shared::cta.b64 [%0];\n" ::"r"(bar) : "memory");
 }
 __device__ __forceinline__ void tma_load_4d(unsigned dst, const CUtensorMap *map, int c0, int c1, int c2, int c3,
                                             unsigned bar) {
@@ -131,7 +144,7 @@ __device__ __forceinline__ T axis_terms(const T (&s)[2 * R + 1], T f, T k3, T k2
 
 template <typename T, bool VAC>
 __device__ __forceinline__ void rhs_half(const T (&c)[4], T a, T b, T e, T mu, T p2s, T p2c, T ps, const T (&sten)[4],
-                                         T (&out)[4]) {
+                                         T (&out)[4], bool vac) {
     const T ee = c[0], mm = c[1], emr = c[2], emi = c[3];
     const T Iee = T(2) * mu * (emi * a + emr * b);
     const T Iemr = -mu * ((ee - mm) * b + e * emi);
@@ -140,7 +153,7 @@ __device__ __forceinline__ void rhs_half(const T (&c)[4], T a, T b, T e, T mu, T
     out[1] = -Iee + sten[1];
     out[2] = Iemr + sten[2];
     out[3] = Iemi + sten[3];
-    if (VAC) {  // pmo * [H_vac, rho] (nuosc_class.cpp:280-287); p2s = 2 pmo st, p2c = 2 pmo ct, ps = pmo st
+    if (VAC && vac) {  // pmo * [H_vac, rho] (nuosc_class.cpp:280-287); p2s = 2 pmo st, p2c = 2 pmo ct, ps = pmo st
         out[0] -= p2s * emi;
         out[1] += p2s * emi;
         out[2] -= p2c * emi;
@@ -156,6 +169,17 @@ __device__ __forceinline__ void rs_step(double (&m)[16]) {
     for (int i = 0; i < N / 2; ++i) m[i] += __shfl_xor_sync(0xffffffffu, m[i + N / 2], O);
 }
 
+// statically allocated per-CTA scratch of the march: the abort flag and, with
+// two velocities per thread (FP32), the FP64 per-velocity constants
+template <typename T>
+struct MarchShared {
+    static constexpr bool kShared = vpt<T>() == 2;
+    static constexpr int VB = vblock<T>();
+    double vq[kShared ? 3 : 1][kShared ? VB : 2];           // vx, vy, vz
+    double wp[kShared ? 32 : 1][kShared ? vpt<T>() * 4 : 2];  // lane-permuted weights
+    int abort;
+};
+
 template <typename T, int TZ>
 constexpr int tma_ctas_per_sm() {
     return TZ == 16 ? 1 : 2;
@@ -163,9 +187,26 @@ constexpr int tma_ctas_per_sm() {
 
 }  // namespace
 
-template <typename T, int R, int MODE, int TZ, bool VAC>
-__global__ void __launch_bounds__(32 * TZ, tma_ctas_per_sm<T, TZ>())
-    k_xtma(const __grid_constant__ TmaMaps maps, const StageArgs<T> a, int LX) {
+// value of x, re-read from (shared) memory at each use when V: keeps values
+// that are loop-invariant but cheap to re-read out of the register file
+template <bool V, typename P>
+__device__ __forceinline__ P rd(const P &x) {
+    if constexpr (V) return *(const volatile P *)&x;
+    else return x;
+}
+
+// One tile of work: z rows z0..z0+TZ-1, velocity block vb (of nvb), x planes
+// xs..xe-1, flavour half `half`, of the instance described by (*mp, a).
+// Called by the single-instance kernel (one tile per CTA; a and *mp in kernel
+// parameter space) and by the persistent batched kernel (many tiles per CTA,
+// of many instances; SA: a and mp in shared memory); the arithmetic per
+// (cell, velocity) does not depend on which.  VAC compiles the vacuum term in
+// (it then runs where a.c.pmo != 0).  Returns true when a bounded wait
+// expired (the status word is set and the tile is incomplete).
+template <typename T, int R, int MODE, int TZ, bool VAC, bool SA>
+__device__ __forceinline__ bool xtma_march(const TmaMaps *const &mp, const StageArgs<T> &a, const int z0, const int vb,
+                                           const int nvb, const int xs, const int xe, const int half,
+                                           unsigned char *smem, MarchShared<T> &sh) {
     using S = Slot<T, TZ, R>;
     constexpr int NP = vpt<T>();       // velocities per thread
     constexpr int VB = S::VB;          // velocities per CTA
@@ -173,20 +214,13 @@ __global__ void __launch_bounds__(32 * TZ, tma_ctas_per_sm<T, TZ>())
     constexpr int ZR = S::ZR;
     constexpr int D = 2;               // boxes issued ahead of their first use
     constexpr int NS = R + D + 2;      // a box lives from its front use to its centre use, plus slack
-    extern __shared__ __align__(1024) unsigned char smem[];
     unsigned long long *bars = (unsigned long long *)(smem + NS * S::bytes);  // full[NS], empty[NS]
-    __shared__ int s_abort;
+    int &s_abort = sh.abort;
 
     const Geom g = a.g;
     const int tid = threadIdx.x, lane = tid & 31, r = tid >> 5;
-    const int z0 = blockIdx.x * TZ;
-    const int vb = blockIdx.y;
     const int v = vb * VB + NP * lane;  // first of this thread's NP velocities
     const bool vact = v < g.nvs;        // nvs is a multiple of NP, so all NP are active together
-    const int seg = blockIdx.z >> 1, half = blockIdx.z & 1;
-    const int xs = seg * LX;
-    if (xs >= g.nx) return;
-    const int xe = min(xs + LX, g.nx);
     const int nplanes = xe - xs;
     const int nboxes = nplanes + R;    // centres xs..xe-1 and fronts up to xe-1+R
     const int zr = z0 + r;             // < nz since nz % TZ == 0
@@ -196,8 +230,8 @@ __global__ void __launch_bounds__(32 * TZ, tma_ctas_per_sm<T, TZ>())
     const T *in = a.in + hoff;
     const int vc = vact ? v : 0;
     const long long own = (long long)zr * g.nvs + vc;
-    const int nvb = gridDim.y;
 
+    __syncthreads();  // the previous tile of this CTA (batched kernel) is done with the ring
     if (tid == 0) {
         s_abort = 0;
         for (int s = 0; s < 2 * NS; ++s) mbar_init(smem_u32(&bars[s]), s < NS ? 1u : (unsigned)TZ);
@@ -212,19 +246,21 @@ __global__ void __launch_bounds__(32 * TZ, tma_ctas_per_sm<T, TZ>())
         const unsigned full = smem_u32(&bars[s]);
         unsigned char *sp = smem + s * S::bytes;
         mbar_expect_tx(full, S::tx);
-        const int x = (xs + j) % g.nx;
+        const int x = (xs + j) % rd<SA>(a.g.nx);
+        const int nz = rd<SA>(a.g.nz);
+        const TmaMaps &maps = *rd<SA>(mp);
         const int c1 = 4 * half, c0 = vb * VB;
         int zstart = z0 - R, dst = 0;
         while (dst < ZR) {
-            const int zw = zstart < 0 ? zstart + g.nz : (zstart >= g.nz ? zstart - g.nz : zstart);
-            int len = g.nz - zw;
+            const int zw = zstart < 0 ? zstart + nz : (zstart >= nz ? zstart - nz : zstart);
+            int len = nz - zw;
             if (len > ZR - dst) len = ZR - dst;
             const CUtensorMap *m = len == ZR ? &maps.zr : len == TZ + R ? &maps.tzr : len == TZ ? &maps.tz : &maps.r;
             tma_load_4d(smem_u32(sp + S::box + dst * 4 * VB * sizeof(T)), m, c0, c1, zw, x, full);
             zstart += len;
             dst += len;
         }
-        bulk_load(smem_u32(sp + S::mb), a.mom_in + ((long long)x * g.nz + z0) * NMOM, 8u * TZ * NMOM, full);
+        bulk_load(smem_u32(sp + S::mb), rd<SA>(a.mom_in) + ((long long)x * nz + z0) * NMOM, 8u * TZ * NMOM, full);
         return true;
     };
 
@@ -234,9 +270,9 @@ __global__ void __launch_bounds__(32 * TZ, tma_ctas_per_sm<T, TZ>())
     // (FP32) the FP64 per-velocity constants live in shared memory and are
     // read per plane, which keeps the register queue clear of spills.
     const int perm = (lane >> 1) & 15;
-    constexpr bool kShared = NP == 2;
-    __shared__ __align__(16) double s_vq[kShared ? 3 : 1][kShared ? VB : 2];          // vx, vy, vz
-    __shared__ __align__(16) double s_wp[kShared ? 32 : 1][kShared ? NP * 4 : 2];     // permuted weights
+    constexpr bool kShared = MarchShared<T>::kShared;
+    auto &s_vq = sh.vq;
+    auto &s_wp = sh.wp;
     double vxd[NP], vyd[NP], vzd[NP], wperm[NP][4];
     T fx[NP], fz[NP];
 #pragma unroll
@@ -271,6 +307,7 @@ __global__ void __launch_bounds__(32 * TZ, tma_ctas_per_sm<T, TZ>())
     const T kx3 = T(a.c.kx3), kx2 = T(a.c.kx2), kx1 = T(a.c.kx1), kc = T(a.c.kc);
     const T mu = T(a.c.mu), p2s = T(2 * a.c.pmo * a.c.st), p2c = T(2 * a.c.pmo * a.c.ct), ps = T(a.c.pmo * a.c.st);
     const T cA = T(a.cA), cY = T(a.cY);
+    const bool vac = VAC && a.c.pmo != 0.0;  // batched launches: instances without a vacuum term skip it
     const bool sw1 = (perm >> 2) & 1, sw2 = (perm >> 3) & 1;
 
     // prime the register queue with planes xs-R .. xs+R-1
@@ -303,8 +340,8 @@ __global__ void __launch_bounds__(32 * TZ, tma_ctas_per_sm<T, TZ>())
 #pragma unroll
             for (int p = 0; p < NP; ++p) uin[f][p] = ain[f][p] = T(0);
             if (vact) {
-                if (MODE == MODE_S23) ldv<T, NP>(a.u + oc + f * fs, uin[f]);
-                if (MODE != MODE_S1) ldv<T, NP>(a.acc_src + oc + f * fs, ain[f]);
+                if (MODE == MODE_S23) ldv<T, NP>(rd<SA>(a.u) + oc + f * fs, uin[f]);
+                if (MODE != MODE_S1) ldv<T, NP>(rd<SA>(a.acc_src) + oc + f * fs, ain[f]);
             }
         }
         const int jf = i + R, sf = jf % NS, sc = i % NS;
@@ -366,7 +403,7 @@ __global__ void __launch_bounds__(32 * TZ, tma_ctas_per_sm<T, TZ>())
             const T cen[4] = {q[0][R][p], q[1][R][p], q[2][R][p], q[3][R][p]};
             const T st4[4] = {sten[0][p], sten[1][p], sten[2][p], sten[3][p]};
             T kk[4];
-            rhs_half<T, VAC>(cen, ia, ib, ie, mu, p2s, p2c, ps, st4, kk);
+            rhs_half<T, VAC>(cen, ia, ib, ie, mu, p2s, p2c, ps, st4, kk, vac);
 #pragma unroll
             for (int f = 0; f < 4; ++f) {
                 if (MODE == MODE_S1) {
@@ -384,13 +421,13 @@ __global__ void __launch_bounds__(32 * TZ, tma_ctas_per_sm<T, TZ>())
 #pragma unroll
             for (int f = 0; f < 4; ++f) {
                 if (MODE == MODE_S1) {
-                    stv<T, NP>(a.acc_dst + oc + f * fs, uin[f]);
-                    stv<T, NP>(a.y_dst + oc + f * fs, outm[f]);
+                    stv<T, NP>(rd<SA>(a.acc_dst) + oc + f * fs, uin[f]);
+                    stv<T, NP>(rd<SA>(a.y_dst) + oc + f * fs, outm[f]);
                 } else if (MODE == MODE_S23) {
-                    stv<T, NP>(a.acc_dst + oc + f * fs, ain[f]);
-                    stv<T, NP>(a.y_dst + oc + f * fs, outm[f]);
+                    stv<T, NP>(rd<SA>(a.acc_dst) + oc + f * fs, ain[f]);
+                    stv<T, NP>(rd<SA>(a.y_dst) + oc + f * fs, outm[f]);
                 } else {
-                    stv<T, NP>(a.acc_dst + oc + f * fs, outm[f]);
+                    stv<T, NP>(rd<SA>(a.acc_dst) + oc + f * fs, outm[f]);
                 }
             }
         }
@@ -421,8 +458,8 @@ __global__ void __launch_bounds__(32 * TZ, tma_ctas_per_sm<T, TZ>())
             rs_step<2, 2>(mp);
             mp[0] += __shfl_xor_sync(0xffffffffu, mp[0], 1);
             if ((lane & 1) == 0 && perm < NMOM) {  // lanes 2k, 2k+1 hold moment perm
-                const long long cell = (long long)x * g.nz + zr;
-                a.mom_part[((cell * nvb + vb) * 2 + half) * NMOM + perm] = mp[0];
+                const long long cell = (long long)x * rd<SA>(a.g.nz) + zr;
+                rd<SA>(a.mom_part)[((cell * nvb + vb) * 2 + half) * NMOM + perm] = mp[0];
             }
         }
 #pragma unroll
@@ -433,14 +470,108 @@ __global__ void __launch_bounds__(32 * TZ, tma_ctas_per_sm<T, TZ>())
                 for (int p = 0; p < NP; ++p) q[f][k][p] = q[f][k + 1][p];
     }
     __syncthreads();
-    if (tid == 0 && s_abort) {
-        // a wait expired: report it, then drain (bounded) every slot that may
-        // still receive a copy before the CTA's shared memory is released
-        atomicExch(a.status, NUOSC_TIMEOUT_CODE);
-        for (int s = 0; s < NS; ++s) {
-            mbar_wait(smem_u32(&bars[s]), 0);
-            mbar_wait(smem_u32(&bars[s]), 1);
+    const bool aborted = s_abort != 0;
+    if (tid == 0) {
+        if (aborted) {
+            // a wait expired: report it, then drain (bounded) every slot that may
+            // still receive a copy before the CTA's shared memory is reused or released
+            atomicExch(a.status, NUOSC_TIMEOUT_CODE);
+            for (int s = 0; s < NS; ++s) {
+                mbar_wait(smem_u32(&bars[s]), 0);
+                mbar_wait(smem_u32(&bars[s]), 1);
+            }
         }
+        for (int s = 0; s < 2 * NS; ++s) mbar_inval(smem_u32(&bars[s]));
+    }
+    return aborted;
+}
+
+template <typename T, int R, int MODE, int TZ, bool VAC>
+__global__ void __launch_bounds__(32 * TZ, tma_ctas_per_sm<T, TZ>())
+    k_xtma(const __grid_constant__ TmaMaps maps, const StageArgs<T> a, int LX) {
+    extern __shared__ __align__(1024) unsigned char smem[];
+    __shared__ MarchShared<T> sh;
+    const int xs = (blockIdx.z >> 1) * LX;
+    if (xs >= a.g.nx) return;
+    const TmaMaps *mp = &maps;
+    xtma_march<T, R, MODE, TZ, VAC, false>(mp, a, blockIdx.y * TZ, blockIdx.x, gridDim.x, xs,
+                                           min(xs + LX, a.g.nx), blockIdx.z & 1, smem, sh);
+}
+
+// One instance's stage in a batched launch: its tensor maps (over the stage's
+// input register), stage arguments and tile counts.  Lives in device memory;
+// the TMA reads the maps from there.
+template <typename T>
+struct __align__(64) BatchItem {
+    TmaMaps maps;
+    StageArgs<T> a;
+    int ntz, nvb, lx, nseg;
+};
+
+// Persistent batched stage kernel: the CTAs of one launch (as many as fit on
+// the SMs at once) take tiles of all instances from a work-list, largest
+// instances first, through an atomic counter.  Tile k of instance i is the
+// tile the single-instance kernel runs as its CTA k, so each instance's
+// result is the same bits as its own launch.  The tile's StageArgs are copied
+// to shared memory and re-read there at each use (the single-instance kernel
+// reads them from the constant bank), which keeps them out of the register
+// file that the march's x-queue fills; the vacuum term is switched per
+// instance at run time.
+template <typename T, int R, int MODE, int TZ>
+__global__ void __launch_bounds__(32 * TZ, tma_ctas_per_sm<T, TZ>())
+    k_xtma_batch(const BatchItem<T> *items, const long long *__restrict__ starts, int ninst, long long nitems,
+                 unsigned long long *counter) {
+    extern __shared__ __align__(1024) unsigned char smem[];
+    __shared__ MarchShared<T> sh;
+    __shared__ __align__(16) StageArgs<T> s_a;
+    __shared__ const TmaMaps *s_mp;
+    __shared__ int s_t[6];  // instance, z0, vb, xs, xe, half
+    constexpr int NW = (int)(sizeof(StageArgs<T>) / 8);
+    static_assert(sizeof(StageArgs<T>) % 8 == 0 && NW <= 32 * TZ, "StageArgs copy: one 8-byte word per thread");
+    for (;;) {
+        __syncthreads();  // every thread is done with the previous tile's arguments
+        if (threadIdx.x == 0) {
+            const long long it = (long long)atomicAdd(counter, 1ull);
+            s_t[0] = -1;
+            if (it < nitems) {
+                int lo = 0, hi = ninst - 1;  // last instance whose first tile is <= it
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (starts[mid] <= it) lo = mid;
+                    else hi = mid - 1;
+                }
+                const BatchItem<T> &e = items[lo];
+                long long loc = it - starts[lo];  // ((seg * 2 + half) * ntz + zt) * nvb + vb
+                const int vb = (int)(loc % e.nvb);
+                loc /= e.nvb;
+                const int zt = (int)(loc % e.ntz);
+                loc /= e.ntz;
+                const int xs = (int)(loc >> 1) * e.lx;
+                s_t[0] = lo;
+                s_t[1] = zt * TZ;
+                s_t[2] = vb;
+                s_t[3] = xs;
+                s_t[4] = min(xs + e.lx, e.a.g.nx);
+                s_t[5] = (int)(loc & 1);
+                s_mp = &e.maps;
+                // the maps were written through the generic proxy (a host copy
+                // when the work-list was built); thread 0 issues every TMA load
+                tensormap_acquire(&e.maps.zr);
+                tensormap_acquire(&e.maps.tzr);
+                tensormap_acquire(&e.maps.tz);
+                tensormap_acquire(&e.maps.r);
+            }
+        }
+        __syncthreads();
+        const int lo = s_t[0];
+        if (lo < 0) break;
+        if (threadIdx.x < NW)
+            reinterpret_cast<long long *>(&s_a)[threadIdx.x] =
+                reinterpret_cast<const long long *>(&items[lo].a)[threadIdx.x];
+        const int nvb = items[lo].nvb;
+        const int z0 = s_t[1], vb = s_t[2], xs = s_t[3], xe = s_t[4], half = s_t[5];
+        __syncthreads();
+        if (xtma_march<T, R, MODE, TZ, true, true>(s_mp, s_a, z0, vb, nvb, xs, xe, half, smem, sh)) break;
     }
 }
 
@@ -481,21 +612,29 @@ bool make_map(CUtensorMap *m, const T *base, const Geom &g, int rows) {
               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+template <typename T>
+bool make_maps(TmaMaps *m, const T *base, const Geom &g, int tz, int r) {
+    return make_map<T>(&m->zr, base, g, tz + 2 * r) && make_map<T>(&m->tzr, base, g, tz + r) &&
+           make_map<T>(&m->tz, base, g, tz) && make_map<T>(&m->r, base, g, r);
+}
+
 template <typename T, int R, int MODE, int TZ, bool VAC>
 cudaError_t launch_t(const StageArgs<T> &a, XTile t, cudaStream_t s) {
     constexpr int NS = R + 2 + 2;
     using Sl = Slot<T, TZ, R>;
-    static_assert(tma_ctas_per_sm<T, TZ>() * ((R + 4) * Sl::bytes + 2048) <= 227 * 1024, "ring exceeds shared memory");
+    static_assert(tma_ctas_per_sm<T, TZ>() * (NS * Sl::bytes + 2 * NS * 8 + sizeof(MarchShared<T>) + 64 + 1024) <=
+                      228 * 1024,
+                  "ring exceeds shared memory");
     TmaMaps maps;
-    if (!make_map<T>(&maps.zr, a.in, a.g, TZ + 2 * R) || !make_map<T>(&maps.tzr, a.in, a.g, TZ + R) ||
-        !make_map<T>(&maps.tz, a.in, a.g, TZ) || !make_map<T>(&maps.r, a.in, a.g, R))
-        return cudaErrorInvalidValue;
+    if (!make_maps<T>(&maps, a.in, a.g, TZ, R)) return cudaErrorInvalidValue;
     const size_t smem = (size_t)NS * Sl::bytes + 2 * NS * 8;
     cudaError_t e = cudaFuncSetAttribute(k_xtma<T, R, MODE, TZ, VAC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e != cudaSuccess) return e;
     const int nseg = (a.g.nx + t.lx - 1) / t.lx;
-    dim3 grid(a.g.nz / TZ, (a.g.nvs + Sl::VB - 1) / Sl::VB, nseg * 2);
+    // velocity blocks fastest: the CTAs resident at once read whole velocity
+    // rows of a few z rows (DRAM page locality) rather than one block of many rows
+    dim3 grid((a.g.nvs + Sl::VB - 1) / Sl::VB, a.g.nz / TZ, nseg * 2);
     k_xtma<T, R, MODE, TZ, VAC><<<grid, 32 * TZ, smem, s>>>(maps, a, t.lx);
     return cudaGetLastError();
 }
@@ -515,12 +654,101 @@ cudaError_t launch_tv(const StageArgs<T> &a, int mode, XTile t, cudaStream_t s) 
     return a.c.pmo != 0.0 ? launch_tm<T, R, TZ, true>(a, mode, t, s) : launch_tm<T, R, TZ, false>(a, mode, t, s);
 }
 
+// ---- batched launch: one persistent grid per stage over many instances
+template <typename T, int R, int MODE, int TZ>
+constexpr size_t batch_smem() {
+    return (size_t)(R + 4) * Slot<T, TZ, R>::bytes + 2 * (R + 4) * 8;
+}
+
+template <typename T, int R, int MODE, int TZ>
+int batch_grid_t(int device) {
+    const size_t smem = batch_smem<T, R, MODE, TZ>();
+    if (cudaFuncSetAttribute(k_xtma_batch<T, R, MODE, TZ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+        cudaSuccess)
+        return -1;
+    int per_sm = 0, sms = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_xtma_batch<T, R, MODE, TZ>, 32 * TZ, smem) !=
+            cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess || per_sm < 1)
+        return -1;
+    return per_sm * sms;
+}
+
+template <typename T, int R, int MODE, int TZ>
+cudaError_t batch_launch_t(const void *items, const long long *starts, int n, long long ntiles,
+                           unsigned long long *counter, int grid, cudaStream_t s) {
+    k_xtma_batch<T, R, MODE, TZ><<<grid, 32 * TZ, batch_smem<T, R, MODE, TZ>(), s>>>(
+        (const BatchItem<T> *)items, starts, n, ntiles, counter);
+    return cudaGetLastError();
+}
+
+// dispatch of (mode, ko6, tz) onto the template instances of F
+template <typename T, template <typename, int, int, int> class F, typename... Args>
+auto batch_dispatch(int mode, bool ko6, int tz, Args... args) {
+#define NUOSC_BATCH_TZ(R, M)                                                  \
+    (tz == 16 ? F<T, R, M, 16>::run(args...) : F<T, R, M, 8>::run(args...))
+#define NUOSC_BATCH_MODE(R)                                                   \
+    (mode == MODE_S1 ? NUOSC_BATCH_TZ(R, MODE_S1)                             \
+                     : mode == MODE_S23 ? NUOSC_BATCH_TZ(R, MODE_S23) : NUOSC_BATCH_TZ(R, MODE_S4))
+    return ko6 ? NUOSC_BATCH_MODE(3) : NUOSC_BATCH_MODE(2);
+#undef NUOSC_BATCH_MODE
+#undef NUOSC_BATCH_TZ
+}
+
+template <typename T, int R, int MODE, int TZ>
+struct BatchGrid {
+    static int run(int device) { return batch_grid_t<T, R, MODE, TZ>(device); }
+};
+template <typename T, int R, int MODE, int TZ>
+struct BatchLaunch {
+    static cudaError_t run(const void *items, const long long *starts, int n, long long ntiles,
+                           unsigned long long *counter, int grid, cudaStream_t s) {
+        return batch_launch_t<T, R, MODE, TZ>(items, starts, n, ntiles, counter, grid, s);
+    }
+};
+
 }  // namespace
 
 template <typename T>
 bool xtma_supported(const Geom &g, XTile t) {
-    return (t.tz == 8 || t.tz == 16) && g.nz % t.tz == 0 && g.nx >= 4 && g.nvs % vpt<T>() == 0 &&
-           encode_fn() != nullptr;
+    // nz >= tz + 6: the widest box (tz + 2R rows, R <= 3) fits in the z extent
+    return (t.tz == 8 || t.tz == 16) && g.nz % t.tz == 0 && g.nz >= t.tz + 6 && g.nx >= 4 &&
+           g.nvs % vpt<T>() == 0 && encode_fn() != nullptr;
+}
+
+template <typename T>
+size_t xtma_batch_item_bytes() {
+    return sizeof(BatchItem<T>);
+}
+
+template <typename T>
+long long xtma_batch_fill(void *item, const StageArgs<T> &a, bool ko6, int tz, int lx) {
+    if (!xtma_supported<T>(a.g, XTile{tz, lx, vblock<T>()}) || lx < 1 || !a.mom_part) return -1;
+    BatchItem<T> e;
+    memset((void *)&e, 0, sizeof e);
+    if (!make_maps<T>(&e.maps, a.in, a.g, tz, ko6 ? 3 : 2)) return -1;
+    e.a = a;
+    e.ntz = a.g.nz / tz;
+    e.nvb = xtma_num_vblocks<T>(a.g);
+    e.lx = lx;
+    e.nseg = (a.g.nx + lx - 1) / lx;
+    memcpy(item, (const void *)&e, sizeof e);
+    return (long long)e.ntz * e.nvb * 2 * e.nseg;
+}
+
+template <typename T>
+int xtma_batch_grid(int mode, bool ko6, int tz, int device) {
+    if ((tz != 8 && tz != 16) || (mode != MODE_S1 && mode != MODE_S23 && mode != MODE_S4)) return -1;
+    return batch_dispatch<T, BatchGrid>(mode, ko6, tz, device);
+}
+
+template <typename T>
+cudaError_t launch_stage_xtma_batch(const void *items, const long long *starts, int n, long long ntiles,
+                                    unsigned long long *counter, int mode, bool ko6, int tz, int grid,
+                                    cudaStream_t s) {
+    if ((tz != 8 && tz != 16) || (mode != MODE_S1 && mode != MODE_S23 && mode != MODE_S4) || n < 1 || grid < 1)
+        return cudaErrorInvalidValue;
+    return batch_dispatch<T, BatchLaunch>(mode, ko6, tz, items, starts, n, ntiles, counter, grid, s);
 }
 
 template <typename T>
@@ -541,5 +769,15 @@ template int xtma_num_vblocks<double>(const Geom &);
 template int xtma_num_vblocks<float>(const Geom &);
 template cudaError_t launch_stage_xtma<double>(const StageArgs<double> &, int, bool, XTile, cudaStream_t);
 template cudaError_t launch_stage_xtma<float>(const StageArgs<float> &, int, bool, XTile, cudaStream_t);
+template size_t xtma_batch_item_bytes<double>();
+template size_t xtma_batch_item_bytes<float>();
+template long long xtma_batch_fill<double>(void *, const StageArgs<double> &, bool, int, int);
+template long long xtma_batch_fill<float>(void *, const StageArgs<float> &, bool, int, int);
+template int xtma_batch_grid<double>(int, bool, int, int);
+template int xtma_batch_grid<float>(int, bool, int, int);
+template cudaError_t launch_stage_xtma_batch<double>(const void *, const long long *, int, long long,
+                                                     unsigned long long *, int, bool, int, int, cudaStream_t);
+template cudaError_t launch_stage_xtma_batch<float>(const void *, const long long *, int, long long,
+                                                    unsigned long long *, int, bool, int, int, cudaStream_t);
 
 }  // namespace nuosc

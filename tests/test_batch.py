@@ -1,0 +1,132 @@
+"""Batched stepping (nuosc_batch_*): every member of a batch must end up with
+exactly the bits it gets when stepped alone.
+
+Instances differ in nx, nz, nv (42, 162, 642, 12), mu, pmo (vacuum term on
+and off), renormalisation, x-segment length and initial data; each has a twin
+built identically and stepped with NuOsc.step_rk4.  States are compared as
+raw bit patterns (uint64 view, so even the sign of a zero counts), the
+analysis records and phy_time exactly.  The cell spacing 0.125 makes every
+box an exact number of cells.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+DX = 0.125
+
+
+@pytest.fixture(scope="module")
+def nb(gpu):
+    import nuosc_b200
+    return nuosc_b200
+
+
+def build(nb, nx, nz, nn, precision=0, mu=1.0, pmo=0.0, alpha=0.9, eps0=0.1, sigma=0.6, renorm=False,
+          lx=None, seed=11, gx=3):
+    s = nb.NuOsc(1, 1, nn, 0, gx, gx, -nx * DX / 2, nx * DX / 2, -nz * DX / 2, nz * DX / 2, DX, DX, 0.4, 0.1,
+                 precision=precision)
+    g = s.grid
+    assert (g.nx, g.nz) == (nx, nz)
+    s.set_mu(mu)
+    s.set_pmo(pmo)
+    s.set_renorm(renorm)
+    if lx is not None:
+        tz, _ = s.get_tile()
+        s.set_tile(tz, lx)
+    s.fillInitValue(1, alpha, eps0, sigma, 0.6, 0.5, seed=seed)
+    return s
+
+
+def bits(s):
+    return s.get_state().view(np.uint64)
+
+
+def assert_same(a, b):
+    assert a.phy_time == b.phy_time
+    assert np.array_equal(bits(a), bits(b))
+    assert a.analysis() == b.analysis()
+
+
+SPECS_TZ16 = [dict(nx=48, nz=32, nn=2),
+              dict(nx=96, nz=64, nn=4, mu=0.5, pmo=0.1, alpha=1.2, seed=3),
+              dict(nx=40, nz=48, nn=8, alpha=0.8, renorm=True, lx=16, seed=5),
+              dict(nx=200, nz=32, nn=1, sigma=0.4, seed=9)]
+SPECS_TZ8 = [dict(nx=24, nz=16, nn=2, seed=21),
+             dict(nx=64, nz=40, nn=4, pmo=0.1, seed=22),
+             dict(nx=33, nz=24, nn=8, lx=7, seed=23)]
+
+
+def run_pair(nb, specs, precision, tz):
+    members = [build(nb, precision=precision, **sp) for sp in specs]
+    twins = [build(nb, precision=precision, **sp) for sp in specs]
+    b = nb.Batch(members)
+    try:
+        info = b.info()
+        assert info["n"] == len(specs) and info["tz"] == tz and info["ctas"] > 0
+        # 3 batched steps against 3 solo steps
+        b.step_rk4(3)
+        b.synchronize()
+        for t in twins:
+            t.step_rk4(3)
+        for m, t in zip(members, twins):
+            assert_same(m, t)
+        # members continue alone after batched steps
+        for m, t in zip(members, twins):
+            m.step_rk4(1)
+            t.step_rk4(1)
+            assert_same(m, t)
+        # a setting changed between batch steps is picked up
+        members[0].set_mu(0.7)
+        twins[0].set_mu(0.7)
+        b.step_rk4(2)
+        b.synchronize()
+        for t in twins:
+            t.step_rk4(2)
+        for m, t in zip(members, twins):
+            assert_same(m, t)
+        info = b.info()
+        assert info["graph_launches"] == 5
+        assert info["kernel_launches"] >= 5 * 8
+    finally:
+        b.close()
+    for s in members + twins:
+        s.close()
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_batch_equals_solo_tz16(nb, precision):
+    run_pair(nb, SPECS_TZ16, precision, 16)
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_batch_equals_solo_tz8(nb, precision):
+    run_pair(nb, SPECS_TZ8, precision, 8)
+
+
+def test_batch_ko4_equals_solo(nb):
+    specs = [dict(nx=48, nz=32, nn=2, gx=2), dict(nx=32, nz=64, nn=4, gx=2, pmo=0.1, seed=4)]
+    run_pair(nb, specs, 0, 16)
+
+
+def test_batch_rejects_bad_membership(nb):
+    a = build(nb, 32, 32, 2)
+    c = build(nb, 32, 32, 2, precision=1)
+    d = build(nb, 32, 20, 2)  # nz % 8 != 0
+    try:
+        for members, code in (([a, c], nb._lib.ERR_UNSUPPORTED), ([a, a], nb._lib.ERR_INVALID),
+                              ([a, d], nb._lib.ERR_UNSUPPORTED)):
+            with pytest.raises(nb.NuoscError) as e:
+                nb.Batch(members)
+            assert e.value.code == code
+        b = nb.Batch([a])
+        with pytest.raises(nb.NuoscError) as e:
+            a.close()  # a member of a live batch is not destroyed
+        assert e.value.code == nb._lib.ERR_INVALID
+        with pytest.raises(nb.NuoscError) as e:
+            nb.Batch([a])  # already in a batch
+        assert e.value.code == nb._lib.ERR_INVALID
+        b.close()
+    finally:
+        for s in (a, c, d):
+            s.close()

@@ -53,6 +53,13 @@ def test_bad_arguments_return_codes():
     assert lib.nuosc_step_rk4(None, 1) == _lib.ERR_INVALID
     assert lib.nuosc_analysis(None, None) == _lib.ERR_INVALID
     assert b"null" in lib.nuosc_last_error()
+    b = C.c_void_p()
+    assert lib.nuosc_batch_create(None, 0, C.byref(b)) == _lib.ERR_INVALID
+    assert lib.nuosc_batch_create((C.c_void_p * 1)(None), 1, C.byref(b)) == _lib.ERR_INVALID
+    assert not b.value
+    assert lib.nuosc_batch_step(None, 1) == _lib.ERR_INVALID
+    assert lib.nuosc_batch_synchronize(None) == _lib.ERR_INVALID
+    assert lib.nuosc_batch_destroy(None) == _lib.OK
     base = dict(px=1, pz=1, nv=2, nphi=0, gx=3, gz=3, x0=-0.4, x1=0.4, z0=-0.4, z1=0.4, dx=0.1, dz=0.1, cfl=0.4,
                 ko=0.1, precision=0, device=0)
     for bad, code in ((dict(px=2), _lib.ERR_UNSUPPORTED), (dict(gx=4, gz=4), _lib.ERR_INVALID),
