@@ -964,15 +964,16 @@ struct nuosc_batch {
     int precision = NUOSC_FP64;
     bool ko6 = true;
     int tz = 16;
+    bool vac = false;               // some member has a vacuum term (pmo != 0)
     std::vector<nuosc_handle *> m;  // service order: largest first
     cudaStream_t stream = nullptr;
     cudaEvent_t ev = nullptr;
-    char *d_buf = nullptr;          // stage tables | tile starts | finalize table | cell starts | counters
+    char *d_buf = nullptr;          // stage tables | tile starts | cell starts | finalize table | cursors
     size_t item_bytes = 0;
     long long *d_starts = nullptr;
     FinalizeItem *d_fin = nullptr;
+    unsigned long long *d_counter = nullptr;  // work-list cursors of the 4 stage launches
     long long *d_fstarts = nullptr;
-    unsigned long long *d_counter = nullptr;
     long long ntiles = 0, nmom = 0, cells = 0, cellv = 0;
     int grid[4] = {0, 0, 0, 0};
     cudaGraph_t graph = nullptr;
@@ -1078,18 +1079,21 @@ int batch_build(nuosc_batch *b) {
     CUDA_TRY(cudaStreamSynchronize(b->stream));  // host staging is freed on return
     b->ntiles = tiles;
     b->nmom = nmom;
+    b->vac = false;
+    for (const nuosc_handle *h : b->m) b->vac = b->vac || h->pmo != 0.0;
     for (int k = 0; k < 4; ++k) {
-        b->grid[k] = xtma_batch_grid<T>(kStages[k].mode, b->ko6, b->tz, b->device);
+        b->grid[k] = xtma_batch_grid<T>(kStages[k].mode, b->ko6, b->tz, b->vac, b->device);
         if (b->grid[k] < 1) return fail(NUOSC_ERR_CUDA, "batch: cannot size the persistent stage grid");
     }
 
-    // one step: reset the work counters, 4 x (stage kernel, finalize), renormalisation
+    // one step: reset the work-list cursors, 4 x (stage kernel, finalize), renormalisation
     CUDA_TRY(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
     long long per_step = 0;
     cudaError_t e = cudaMemsetAsync(b->d_counter, 0, 4 * sizeof(unsigned long long), b->stream);
     for (int k = 0; k < 4 && e == cudaSuccess; ++k) {
         e = launch_stage_xtma_batch<T>(b->d_buf + (size_t)k * n * b->item_bytes, b->d_starts, n, tiles,
-                                       b->d_counter + k, kStages[k].mode, b->ko6, b->tz, b->grid[k], b->stream);
+                                       b->d_counter + k, kStages[k].mode, b->ko6, b->tz, b->vac, b->grid[k],
+                                       b->stream);
         if (e == cudaSuccess) e = launch_moment_finalize_batch(b->d_fin, b->d_fstarts, n, nmom, b->stream);
         per_step += 2;
     }

@@ -89,7 +89,8 @@ template <typename T>
 int xtma_num_vblocks(const Geom &g);
 // Batched TMA stage (xtma.cu): one persistent launch runs one RK stage of many
 // instances.  Each instance has an entry (its tensor maps and StageArgs) in a
-// device table; CTAs take tiles of all instances from an atomic work counter.
+// device table; the CTAs of a persistent grid take the tiles of all
+// instances from an atomic work-list cursor.
 // Tile k of an instance is the tile its own launch runs as CTA k, so each
 // instance gets the same bits as when stepped alone.
 template <typename T>
@@ -100,14 +101,15 @@ size_t xtma_batch_item_bytes();
 template <typename T>
 long long xtma_batch_fill(void *item, const StageArgs<T> &a, bool ko6, int tz, int lx);
 // CTAs of a persistent launch on `device` (also sets the kernel's dynamic
-// shared-memory limit); -1 on failure
+// shared-memory limit); -1 on failure.  vac: some instance has pmo != 0.
 template <typename T>
-int xtma_batch_grid(int mode, bool ko6, int tz, int device);
+int xtma_batch_grid(int mode, bool ko6, int tz, bool vac, int device);
 // starts[i] = tiles of instances 0..i-1 (instances ordered as the caller
-// wants them served); counter must be 0 before the launch
+// wants them served); grid = xtma_batch_grid(...); *counter must be 0 at the
+// launch (the work-list cursor)
 template <typename T>
 cudaError_t launch_stage_xtma_batch(const void *items, const long long *starts, int n, long long ntiles,
-                                    unsigned long long *counter, int mode, bool ko6, int tz, int grid,
+                                    unsigned long long *counter, int mode, bool ko6, int tz, bool vac, int grid,
                                     cudaStream_t s);
 // moment_finalize of many instances in one launch (xmarch.cu); starts[i] =
 // sum over instances 0..i-1 of ncell * 12

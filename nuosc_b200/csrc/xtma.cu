@@ -131,15 +131,27 @@ struct Slot {
     static constexpr unsigned tx = sizeof(T) * ZR * 4 * VB + 8 * TZ * NMOM;  // bytes landing per plane
 };
 
+// One axis of the stencil over s[0..2R] (centre s[R]):
+//   ko  = KO difference with unit strength, the centre term included:
+//         6th: s[0]+s[6] - 6 (s[1]+s[5]) + 15 (s[2]+s[4]) - 20 s[3]
+//         4th: s[0]+s[4] - 4 (s[1]+s[3]) + 6 s[2]
+//   adv = s[C-2] - s[C+2] - 8 (s[C-1] - s[C+1]), the 4th-order central
+//         difference of the advection term before its factor -v/(12 dx).
+// The stencil value is eps_z ko_z + eps_x ko_x + fz adv_z + fx adv_x, so
+// only two uniform coefficients (eps_x, eps_z) enter per field; the integer
+// weights are compile-time constants.
 template <typename T, int R>
-__device__ __forceinline__ T axis_terms(const T (&s)[2 * R + 1], T f, T k3, T k2, T k1, T acc) {
+__device__ __forceinline__ void axis_parts(const T (&s)[2 * R + 1], T &ko, T &adv) {
     constexpr int C = R;
-    const T t2 = s[C - 2] + s[C + 2], t1 = s[C - 1] + s[C + 1];
     const T d2 = s[C - 2] - s[C + 2], d1 = s[C - 1] - s[C + 1];
-    if (R == 3) acc = fma(k3, s[0] + s[6], acc);
-    acc = fma(k2, t2, acc);
-    acc = fma(k1, t1, acc);
-    return fma(f, fma(T(-8), d1, d2), acc);
+    adv = fma(T(-8), d1, d2);
+    if constexpr (R == 3) {
+        const T t3 = s[0] + s[6], t2 = s[1] + s[5], t1 = s[2] + s[4];
+        ko = fma(T(-20), s[3], fma(T(15), t1, fma(T(-6), t2, t3)));
+    } else {
+        const T t2 = s[0] + s[4], t1 = s[1] + s[3];
+        ko = fma(T(6), s[2], fma(T(-4), t1, t2));
+    }
 }
 
 template <typename T, bool VAC>
@@ -303,10 +315,17 @@ __device__ __forceinline__ bool xtma_march(const TmaMaps *const &mp, const Stage
         }
         __syncthreads();
     }
-    const T kz3 = T(a.c.kz3), kz2 = T(a.c.kz2), kz1 = T(a.c.kz1);
-    const T kx3 = T(a.c.kx3), kx2 = T(a.c.kx2), kx1 = T(a.c.kx1), kc = T(a.c.kc);
-    const T mu = T(a.c.mu), p2s = T(2 * a.c.pmo * a.c.st), p2c = T(2 * a.c.pmo * a.c.ct), ps = T(a.c.pmo * a.c.st);
-    const T cA = T(a.cA), cY = T(a.cY);
+    // uniform coefficients: hoisted (kernel parameters in the single-instance
+    // kernel; FP32 values in registers), except for the FP64 batched kernel,
+    // which re-reads them from shared memory at each use
+    constexpr bool RR = SA && sizeof(T) == 8;
+    const T kz = RR ? T(0) : T(a.c.kz), kx = RR ? T(0) : T(a.c.kx), mu = RR ? T(0) : T(a.c.mu);
+    const T cA0 = RR ? T(0) : T(a.cA), cY0 = RR ? T(0) : T(a.cY);
+    auto K = [&](const double &x, T hoisted) -> T {
+        if constexpr (RR) return T(rd<true>(x));
+        else return hoisted;
+    };
+    const T p2s = T(2 * a.c.pmo * a.c.st), p2c = T(2 * a.c.pmo * a.c.ct), ps = T(a.c.pmo * a.c.st);
     const bool vac = VAC && a.c.pmo != 0.0;  // batched launches: instances without a vacuum term skip it
     const bool sw1 = (perm >> 2) & 1, sw2 = (perm >> 3) & 1;
 
@@ -334,14 +353,16 @@ __device__ __forceinline__ bool xtma_march(const TmaMaps *const &mp, const Stage
         const int x = xs + i;
         const long long oc = hoff + (long long)x * P + own;
         // pointwise epilogue inputs first (they are not in the ring)
+        const T *up = MODE == MODE_S23 ? rd<SA>(a.u) + oc : nullptr;
+        const T *ap = MODE != MODE_S1 ? rd<SA>(a.acc_src) + oc : nullptr;
         T uin[4][NP], ain[4][NP];
 #pragma unroll
         for (int f = 0; f < 4; ++f) {
 #pragma unroll
             for (int p = 0; p < NP; ++p) uin[f][p] = ain[f][p] = T(0);
             if (vact) {
-                if (MODE == MODE_S23) ldv<T, NP>(rd<SA>(a.u) + oc + f * fs, uin[f]);
-                if (MODE != MODE_S1) ldv<T, NP>(rd<SA>(a.acc_src) + oc + f * fs, ain[f]);
+                if (MODE == MODE_S23) ldv<T, NP>(up + f * fs, uin[f]);
+                if (MODE != MODE_S1) ldv<T, NP>(ap + f * fs, ain[f]);
             }
         }
         const int jf = i + R, sf = jf % NS, sc = i % NS;
@@ -362,6 +383,7 @@ __device__ __forceinline__ bool xtma_march(const TmaMaps *const &mp, const Stage
         const double *mb = (const double *)(sp + S::mb);
 
         T sten[4][NP];
+        const T kzp = K(a.c.kz, kz), kxp = K(a.c.kx, kx);
 #pragma unroll
         for (int f = 0; f < 4; ++f) {
             T zs[W][NP];
@@ -375,9 +397,13 @@ __device__ __forceinline__ bool xtma_march(const TmaMaps *const &mp, const Stage
                     zsp[k] = zs[k][p];
                     xsp[k] = q[f][k][p];
                 }
-                T acc = kc * xsp[R];
-                acc = axis_terms<T, R>(zsp, fz[p], kz3, kz2, kz1, acc);
-                sten[f][p] = axis_terms<T, R>(xsp, fx[p], kx3, kx2, kx1, acc);
+                T koz, advz, kox, advx;
+                axis_parts<T, R>(zsp, koz, advz);
+                axis_parts<T, R>(xsp, kox, advx);
+                T acc = kzp * koz;
+                acc = fma(kxp, kox, acc);
+                acc = fma(fz[p], advz, acc);
+                sten[f][p] = fma(fx[p], advx, acc);
             }
         }
         double m[NMOM];
@@ -403,7 +429,8 @@ __device__ __forceinline__ bool xtma_march(const TmaMaps *const &mp, const Stage
             const T cen[4] = {q[0][R][p], q[1][R][p], q[2][R][p], q[3][R][p]};
             const T st4[4] = {sten[0][p], sten[1][p], sten[2][p], sten[3][p]};
             T kk[4];
-            rhs_half<T, VAC>(cen, ia, ib, ie, mu, p2s, p2c, ps, st4, kk, vac);
+            rhs_half<T, VAC>(cen, ia, ib, ie, K(a.c.mu, mu), p2s, p2c, ps, st4, kk, vac);
+            const T cA = K(a.cA, cA0), cY = K(a.cY, cY0);
 #pragma unroll
             for (int f = 0; f < 4; ++f) {
                 if (MODE == MODE_S1) {
@@ -418,16 +445,18 @@ __device__ __forceinline__ bool xtma_march(const TmaMaps *const &mp, const Stage
             }
         }
         if (vact) {
+            T *dp = rd<SA>(a.acc_dst) + oc;
+            T *yp = MODE != MODE_S4 ? rd<SA>(a.y_dst) + oc : nullptr;
 #pragma unroll
             for (int f = 0; f < 4; ++f) {
                 if (MODE == MODE_S1) {
-                    stv<T, NP>(rd<SA>(a.acc_dst) + oc + f * fs, uin[f]);
-                    stv<T, NP>(rd<SA>(a.y_dst) + oc + f * fs, outm[f]);
+                    stv<T, NP>(dp + f * fs, uin[f]);
+                    stv<T, NP>(yp + f * fs, outm[f]);
                 } else if (MODE == MODE_S23) {
-                    stv<T, NP>(rd<SA>(a.acc_dst) + oc + f * fs, ain[f]);
-                    stv<T, NP>(rd<SA>(a.y_dst) + oc + f * fs, outm[f]);
+                    stv<T, NP>(dp + f * fs, ain[f]);
+                    stv<T, NP>(yp + f * fs, outm[f]);
                 } else {
-                    stv<T, NP>(rd<SA>(a.acc_dst) + oc + f * fs, outm[f]);
+                    stv<T, NP>(dp + f * fs, outm[f]);
                 }
             }
         }
@@ -508,26 +537,30 @@ struct __align__(64) BatchItem {
     int ntz, nvb, lx, nseg;
 };
 
-// Persistent batched stage kernel: the CTAs of one launch (as many as fit on
-// the SMs at once) take tiles of all instances from a work-list, largest
-// instances first, through an atomic counter.  Tile k of instance i is the
-// tile the single-instance kernel runs as its CTA k, so each instance's
-// result is the same bits as its own launch.  The tile's StageArgs are copied
-// to shared memory and re-read there at each use (the single-instance kernel
-// reads them from the constant bank), which keeps them out of the register
-// file that the march's x-queue fills; the vacuum term is switched per
+// Persistent batched stage kernel.  The tiles of all instances form one list
+// (instances in the order of the table -- largest first --, each instance's
+// tiles in the single-instance kernel's CTA order: velocity block fastest,
+// then z rows, then flavour half and x segment) that the CTAs take from an
+// atomic cursor, so the tiles in flight stay a narrow window of the list, as
+// in a hardware-scheduled grid (neighbouring tiles share halo rows in L2 and
+// DRAM pages).  Tile k of instance i is the tile the single-instance kernel
+// runs as its CTA k, so each instance's result is the same bits as its own
+// launch.  The tile's StageArgs are copied to shared memory and re-read there at each use
+// (the single-instance kernel reads them from the constant bank), which keeps
+// them out of the register file that the march's x-queue fills.  VAC compiles
+// the vacuum term in (for batches with any pmo != 0); it is then switched per
 // instance at run time.
-template <typename T, int R, int MODE, int TZ>
+template <typename T, int R, int MODE, int TZ, bool VAC>
 __global__ void __launch_bounds__(32 * TZ, tma_ctas_per_sm<T, TZ>())
     k_xtma_batch(const BatchItem<T> *items, const long long *__restrict__ starts, int ninst, long long nitems,
                  unsigned long long *counter) {
+    constexpr int NW = (int)(sizeof(StageArgs<T>) / 8);
+    static_assert(sizeof(StageArgs<T>) % 8 == 0 && NW <= 32 * TZ, "StageArgs copy: one 8-byte word per thread");
     extern __shared__ __align__(1024) unsigned char smem[];
     __shared__ MarchShared<T> sh;
     __shared__ __align__(16) StageArgs<T> s_a;
     __shared__ const TmaMaps *s_mp;
     __shared__ int s_t[6];  // instance, z0, vb, xs, xe, half
-    constexpr int NW = (int)(sizeof(StageArgs<T>) / 8);
-    static_assert(sizeof(StageArgs<T>) % 8 == 0 && NW <= 32 * TZ, "StageArgs copy: one 8-byte word per thread");
     for (;;) {
         __syncthreads();  // every thread is done with the previous tile's arguments
         if (threadIdx.x == 0) {
@@ -554,8 +587,8 @@ __global__ void __launch_bounds__(32 * TZ, tma_ctas_per_sm<T, TZ>())
                 s_t[4] = min(xs + e.lx, e.a.g.nx);
                 s_t[5] = (int)(loc & 1);
                 s_mp = &e.maps;
-                // the maps were written through the generic proxy (a host copy
-                // when the work-list was built); thread 0 issues every TMA load
+                // thread 0 issues every TMA load of the tile; the maps were written
+                // through the generic proxy (a host copy when the work-list was built)
                 tensormap_acquire(&e.maps.zr);
                 tensormap_acquire(&e.maps.tzr);
                 tensormap_acquire(&e.maps.tz);
@@ -570,8 +603,8 @@ __global__ void __launch_bounds__(32 * TZ, tma_ctas_per_sm<T, TZ>())
                 reinterpret_cast<const long long *>(&items[lo].a)[threadIdx.x];
         const int nvb = items[lo].nvb;
         const int z0 = s_t[1], vb = s_t[2], xs = s_t[3], xe = s_t[4], half = s_t[5];
-        __syncthreads();
-        if (xtma_march<T, R, MODE, TZ, true, true>(s_mp, s_a, z0, vb, nvb, xs, xe, half, smem, sh)) break;
+        __syncthreads();  // s_a is complete
+        if (xtma_march<T, R, MODE, TZ, VAC, true>(s_mp, s_a, z0, vb, nvb, xs, xe, half, smem, sh)) break;
     }
 }
 
@@ -660,50 +693,49 @@ constexpr size_t batch_smem() {
     return (size_t)(R + 4) * Slot<T, TZ, R>::bytes + 2 * (R + 4) * 8;
 }
 
-template <typename T, int R, int MODE, int TZ>
+template <typename T, int R, int MODE, int TZ, bool VAC>
 int batch_grid_t(int device) {
     const size_t smem = batch_smem<T, R, MODE, TZ>();
-    if (cudaFuncSetAttribute(k_xtma_batch<T, R, MODE, TZ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-        cudaSuccess)
-        return -1;
+    auto kern = k_xtma_batch<T, R, MODE, TZ, VAC>;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return -1;
     int per_sm = 0, sms = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_xtma_batch<T, R, MODE, TZ>, 32 * TZ, smem) !=
-            cudaSuccess ||
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * TZ, smem) != cudaSuccess ||
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess || per_sm < 1)
         return -1;
     return per_sm * sms;
 }
 
-template <typename T, int R, int MODE, int TZ>
+template <typename T, int R, int MODE, int TZ, bool VAC>
 cudaError_t batch_launch_t(const void *items, const long long *starts, int n, long long ntiles,
                            unsigned long long *counter, int grid, cudaStream_t s) {
-    k_xtma_batch<T, R, MODE, TZ><<<grid, 32 * TZ, batch_smem<T, R, MODE, TZ>(), s>>>(
+    k_xtma_batch<T, R, MODE, TZ, VAC><<<grid, 32 * TZ, batch_smem<T, R, MODE, TZ>(), s>>>(
         (const BatchItem<T> *)items, starts, n, ntiles, counter);
     return cudaGetLastError();
 }
 
-// dispatch of (mode, ko6, tz) onto the template instances of F
-template <typename T, template <typename, int, int, int> class F, typename... Args>
-auto batch_dispatch(int mode, bool ko6, int tz, Args... args) {
-#define NUOSC_BATCH_TZ(R, M)                                                  \
-    (tz == 16 ? F<T, R, M, 16>::run(args...) : F<T, R, M, 8>::run(args...))
+// dispatch of (mode, ko6, tz, vac) onto the template instances of F
+template <typename T, template <typename, int, int, int, bool> class F, typename... Args>
+auto batch_dispatch(int mode, bool ko6, int tz, bool vac, Args... args) {
+#define NUOSC_BATCH_V(R, M, Z) (vac ? F<T, R, M, Z, true>::run(args...) : F<T, R, M, Z, false>::run(args...))
+#define NUOSC_BATCH_TZ(R, M) (tz == 16 ? NUOSC_BATCH_V(R, M, 16) : NUOSC_BATCH_V(R, M, 8))
 #define NUOSC_BATCH_MODE(R)                                                   \
     (mode == MODE_S1 ? NUOSC_BATCH_TZ(R, MODE_S1)                             \
                      : mode == MODE_S23 ? NUOSC_BATCH_TZ(R, MODE_S23) : NUOSC_BATCH_TZ(R, MODE_S4))
     return ko6 ? NUOSC_BATCH_MODE(3) : NUOSC_BATCH_MODE(2);
 #undef NUOSC_BATCH_MODE
 #undef NUOSC_BATCH_TZ
+#undef NUOSC_BATCH_V
 }
 
-template <typename T, int R, int MODE, int TZ>
+template <typename T, int R, int MODE, int TZ, bool VAC>
 struct BatchGrid {
-    static int run(int device) { return batch_grid_t<T, R, MODE, TZ>(device); }
+    static int run(int device) { return batch_grid_t<T, R, MODE, TZ, VAC>(device); }
 };
-template <typename T, int R, int MODE, int TZ>
+template <typename T, int R, int MODE, int TZ, bool VAC>
 struct BatchLaunch {
     static cudaError_t run(const void *items, const long long *starts, int n, long long ntiles,
                            unsigned long long *counter, int grid, cudaStream_t s) {
-        return batch_launch_t<T, R, MODE, TZ>(items, starts, n, ntiles, counter, grid, s);
+        return batch_launch_t<T, R, MODE, TZ, VAC>(items, starts, n, ntiles, counter, grid, s);
     }
 };
 
@@ -737,18 +769,18 @@ long long xtma_batch_fill(void *item, const StageArgs<T> &a, bool ko6, int tz, i
 }
 
 template <typename T>
-int xtma_batch_grid(int mode, bool ko6, int tz, int device) {
+int xtma_batch_grid(int mode, bool ko6, int tz, bool vac, int device) {
     if ((tz != 8 && tz != 16) || (mode != MODE_S1 && mode != MODE_S23 && mode != MODE_S4)) return -1;
-    return batch_dispatch<T, BatchGrid>(mode, ko6, tz, device);
+    return batch_dispatch<T, BatchGrid>(mode, ko6, tz, vac, device);
 }
 
 template <typename T>
 cudaError_t launch_stage_xtma_batch(const void *items, const long long *starts, int n, long long ntiles,
-                                    unsigned long long *counter, int mode, bool ko6, int tz, int grid,
+                                    unsigned long long *counter, int mode, bool ko6, int tz, bool vac, int grid,
                                     cudaStream_t s) {
     if ((tz != 8 && tz != 16) || (mode != MODE_S1 && mode != MODE_S23 && mode != MODE_S4) || n < 1 || grid < 1)
         return cudaErrorInvalidValue;
-    return batch_dispatch<T, BatchLaunch>(mode, ko6, tz, items, starts, n, ntiles, counter, grid, s);
+    return batch_dispatch<T, BatchLaunch>(mode, ko6, tz, vac, items, starts, n, ntiles, counter, grid, s);
 }
 
 template <typename T>
@@ -773,11 +805,11 @@ template size_t xtma_batch_item_bytes<double>();
 template size_t xtma_batch_item_bytes<float>();
 template long long xtma_batch_fill<double>(void *, const StageArgs<double> &, bool, int, int);
 template long long xtma_batch_fill<float>(void *, const StageArgs<float> &, bool, int, int);
-template int xtma_batch_grid<double>(int, bool, int, int);
-template int xtma_batch_grid<float>(int, bool, int, int);
+template int xtma_batch_grid<double>(int, bool, int, bool, int);
+template int xtma_batch_grid<float>(int, bool, int, bool, int);
 template cudaError_t launch_stage_xtma_batch<double>(const void *, const long long *, int, long long,
-                                                     unsigned long long *, int, bool, int, int, cudaStream_t);
+                                                     unsigned long long *, int, bool, int, bool, int, cudaStream_t);
 template cudaError_t launch_stage_xtma_batch<float>(const void *, const long long *, int, long long,
-                                                    unsigned long long *, int, bool, int, int, cudaStream_t);
+                                                    unsigned long long *, int, bool, int, bool, int, cudaStream_t);
 
 }  // namespace nuosc
