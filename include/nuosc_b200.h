@@ -190,6 +190,8 @@ int nuosc_synchronize(nuosc_handle *h);
 void *nuosc_stream(nuosc_handle *h);
 /* number of kernel launches issued by step_rk4/calrhs of this handle so far */
 long long nuosc_kernel_launches(const nuosc_handle *h);
+/* RK4 steps taken since the initial data (fill_init resets it; -1 for NULL) */
+long long nuosc_step_count(const nuosc_handle *h);
 
 /* Per-kernel timing with CUDA events on the handle's stream (no counterpart
  * in the reference, which prints wall time per step, nuosc.cpp:222-235).
@@ -265,6 +267,28 @@ typedef struct nuosc_batch_info {
 int nuosc_batch_create(nuosc_handle *const *members, int n, nuosc_batch **out);
 /* nsteps RK4 steps of every member (nuosc_step_rk4 on each); asynchronous */
 int nuosc_batch_step(nuosc_batch *b, int nsteps);
+/* Streamed diagnostics: as nuosc_batch_step, and whenever a member's step
+ * count (nuosc_step_count) reaches a multiple of `every`, the analysis of
+ * that member is queued on the batch stream right after that step and its raw
+ * sums are copied into the next record of `out` -- no host synchronisation.
+ * *n_out = records queued (at most max_out, else NUOSC_ERR_INVALID); they are
+ * complete after nuosc_batch_synchronize.  `out` should be page-locked
+ * (nuosc_host_alloc): a pageable buffer makes each copy synchronous.
+ * nuosc_batch_record_diag turns a record into the nuosc_diag that
+ * nuosc_analysis gives at that step (and its NUOSC_ERR_NUMERIC check). */
+typedef struct nuosc_batch_record {
+    int member;       /* index into the members array given to nuosc_batch_create */
+    int reserved;
+    long long step;   /* the member's step count after the step the record follows */
+    double phy_time;
+    double q[12];     /* raw analysis sums */
+} nuosc_batch_record;
+int nuosc_batch_step_stream(nuosc_batch *b, int nsteps, int every, nuosc_batch_record *out, int max_out,
+                            int *n_out);
+int nuosc_batch_record_diag(const nuosc_batch *b, const nuosc_batch_record *r, nuosc_diag *d);
+/* page-locked host memory for record buffers (NULL on failure) */
+void *nuosc_host_alloc(size_t bytes);
+void nuosc_host_free(void *p);
 /* wait for the batch and check every member's in-kernel status word */
 int nuosc_batch_synchronize(nuosc_batch *b);
 int nuosc_batch_get_info(const nuosc_batch *b, nuosc_batch_info *info);

@@ -228,6 +228,11 @@ class NuOsc:
     def kernel_launches(self):
         return lib().nuosc_kernel_launches(self._h)
 
+    @property
+    def step_count(self):
+        """RK4 steps since the initial data."""
+        return lib().nuosc_step_count(self._h)
+
     def set_profiling(self, on=True):
         check(lib().nuosc_set_profiling(self._h, int(bool(on))))
 
@@ -267,6 +272,28 @@ class NuOsc:
         out = np.zeros((len(xidx), self.grid.nz, len(vidx)))
         check(lib().nuosc_gather(self._h, f, _ip(xidx), len(xidx), _ip(vidx), len(vidx), _dp(out)))
         return out
+
+
+class _PinnedRecords:
+    """Page-locked nuosc_batch_record buffer (nuosc_host_alloc)."""
+
+    def __init__(self, n):
+        self.n = n
+        self.used = 0
+        self.ptr = lib().nuosc_host_alloc(n * C.sizeof(_lib.BatchRecord))
+        if not self.ptr:
+            raise MemoryError("nuosc_host_alloc failed")
+
+    def at(self, k):
+        return _lib.BatchRecord.from_address(self.ptr + k * C.sizeof(_lib.BatchRecord))
+
+    def free(self):
+        if self.ptr:
+            lib().nuosc_host_free(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        self.free()
 
 
 class Batch:
@@ -310,6 +337,31 @@ class Batch:
 
     def step_rk4(self, nsteps=1):
         check(lib().nuosc_batch_step(self._b, int(nsteps)))
+
+    def step_stream(self, nsteps, every):
+        """nsteps steps; the analysis of each member is queued on the device
+        whenever its step count reaches a multiple of `every`.  Returns a
+        handle for collect(), valid after synchronize()."""
+        nmax = len(self.members) * (int(nsteps) // max(1, int(every)) + 1)
+        buf = _PinnedRecords(max(1, nmax))
+        n = C.c_int()
+        check(lib().nuosc_batch_step_stream(self._b, int(nsteps), int(every), buf.ptr, buf.n, C.byref(n)))
+        buf.used = n.value
+        return buf
+
+    def collect(self, records):
+        """[(member index, step, analysis dict or None if the state blew up)]
+        of a step_stream() handle; call after synchronize()."""
+        out = []
+        for k in range(records.used):
+            r = records.at(k)
+            d = _lib.Diag()
+            rc = lib().nuosc_batch_record_diag(self._b, C.byref(r), C.byref(d))
+            if rc not in (_lib.OK, _lib.ERR_NUMERIC):
+                check(rc)
+            out.append((r.member, r.step, d.as_dict() if rc == _lib.OK else None))
+        records.free()
+        return out
 
     def synchronize(self):
         check(lib().nuosc_batch_synchronize(self._b))

@@ -59,6 +59,11 @@ class BatchInfo(C.Structure):
         return {n: getattr(self, n) for n, _ in self._fields_}
 
 
+class BatchRecord(C.Structure):
+    _fields_ = [("member", C.c_int), ("reserved", C.c_int), ("step", C.c_longlong), ("phy_time", C.c_double),
+                ("q", C.c_double * 12)]
+
+
 _P = C.c_void_p
 _I = C.c_int
 _D = C.c_double
@@ -102,6 +107,8 @@ _SIGS = {
     "nuosc_batch_synchronize": [_P],
     "nuosc_batch_get_info": [_P, C.POINTER(BatchInfo)],
     "nuosc_batch_destroy": [_P],
+    "nuosc_batch_step_stream": [_P, _I, _I, _P, _I, _IP],
+    "nuosc_batch_record_diag": [_P, C.POINTER(BatchRecord), C.POINTER(Diag)],
 }
 PROF_KINDS = ["stage_s1", "stage_s23", "stage_s4", "calrhs", "moments", "moment_finalize"]
 
@@ -127,6 +134,12 @@ def lib():
         L.nuosc_kernel_launches.argtypes = [_P]
         L.nuosc_batch_stream.restype = _P
         L.nuosc_batch_stream.argtypes = [_P]
+        L.nuosc_step_count.restype = C.c_longlong
+        L.nuosc_step_count.argtypes = [_P]
+        L.nuosc_host_alloc.restype = _P
+        L.nuosc_host_alloc.argtypes = [C.c_size_t]
+        L.nuosc_host_free.restype = None
+        L.nuosc_host_free.argtypes = [_P]
         _lib = L
     return _lib
 

@@ -88,6 +88,7 @@ struct nuosc_handle {
     XTile tile{16, 64, 32};
     long long launches = 0;
     bool mom_valid = false;  // d_mom holds the moments of v_stat
+    long long steps_done = 0;  // RK4 steps since the initial data
     nuosc_batch *batch = nullptr;  // the live batch this handle belongs to
 
     std::vector<double> vx, vy, vz, vw, G0, G0b;  // host copies (length nv)
@@ -329,6 +330,7 @@ int step_impl(nuosc_handle *h, int nsteps) {
             h->mom_valid = false;
         }
         h->phy_time += dt;
+        h->steps_done++;
     }
     return 0;
 }
@@ -504,6 +506,29 @@ int check_indices(const nuosc_handle *h, const int *fields, int nfields, const i
     for (int k = 0; k < nv_; ++k)
         if (vidx[k] < 0 || vidx[k] >= h->g.nv) return fail(NUOSC_ERR_INVALID, "v index %d out of range", vidx[k]);
     return 0;
+}
+
+// analysis record from the raw sums of k_analysis (nuosc_ana.cpp:110-117)
+void diag_from_sums(const nuosc_handle *h, const double *q, double phy_time, nuosc_diag *o) {
+    nuosc_diag d;
+    d.phy_time = phy_time;
+    d.maxdP = q[0];
+    d.surv = q[1] / q[8];
+    d.survb = q[2] / q[9];
+    d.avgP = q[3] / q[8];
+    d.avgPb = q[4] / q[9];
+    d.aM0 = std::sqrt(q[5] * q[5] + q[6] * q[6] + q[7] * q[7]) * h->ds_L;
+    d.Lex = q[7] * h->ds_L;
+    d.ELNe = std::fabs(h->n_nue0[0] * (1.0 - d.surv) - h->n_nue0[1] * (1.0 - d.survb)) / (h->n_nue0[0] + h->n_nue0[1]);
+    d.nonfinite = (long long)q[10];
+    *o = d;
+}
+
+// the reference stops when max||P|-1| leaves 10 (nuosc_ana.cpp:131)
+int diag_check(const nuosc_diag &d) {
+    if (d.nonfinite > 0 || !(d.maxdP < 10))
+        return fail(NUOSC_ERR_NUMERIC, "state blew up: max||P|-1| = %g, %lld non-finite values", d.maxdP, d.nonfinite);
+    return NUOSC_OK;
 }
 
 #define HANDLE_CHECK(h)                                                           \
@@ -743,6 +768,7 @@ int nuosc_fill_init(nuosc_handle *h, int ipt, double alpha, double eps0, double 
                                     seed, h->stream));
     h->mom_valid = false;
     h->phy_time = 0.0;
+    h->steps_done = 0;
     double q[ANA_NQ];
     if (int rc = analysis_dispatch(h, q)) return rc;
     h->n_nue0[0] = q[1] * h->ds_L;  // nuosc_init.cpp:116-130
@@ -826,28 +852,18 @@ int nuosc_analysis(nuosc_handle *h, nuosc_diag *o) {
     if (int rc = check_status(h)) return rc;
     double q[ANA_NQ];
     if (int rc = analysis_dispatch(h, q)) return rc;
-    // nuosc_ana.cpp:110-117
     nuosc_diag d;
-    d.phy_time = h->phy_time;
-    d.maxdP = q[0];
-    d.surv = q[1] / q[8];
-    d.survb = q[2] / q[9];
-    d.avgP = q[3] / q[8];
-    d.avgPb = q[4] / q[9];
-    d.aM0 = std::sqrt(q[5] * q[5] + q[6] * q[6] + q[7] * q[7]) * h->ds_L;
-    d.Lex = q[7] * h->ds_L;
-    d.ELNe = std::fabs(h->n_nue0[0] * (1.0 - d.surv) - h->n_nue0[1] * (1.0 - d.survb)) / (h->n_nue0[0] + h->n_nue0[1]);
-    d.nonfinite = (long long)q[10];
+    diag_from_sums(h, q, h->phy_time, &d);
     if (o) *o = d;
     if (h->anafile.is_open()) {
         // nuosc_ana.cpp:126-129 (precision 13 sticks after the first record)
         h->anafile << d.phy_time << std::setprecision(13) << " " << d.maxdP << " " << d.surv << " " << d.survb << " "
                    << d.avgP << " " << d.avgPb << " " << d.aM0 << " " << d.Lex << " " << d.ELNe << " " << std::endl;
     }
-    if (d.nonfinite > 0 || !(d.maxdP < 10))
-        return fail(NUOSC_ERR_NUMERIC, "state blew up: max||P|-1| = %g, %lld non-finite values", d.maxdP, d.nonfinite);
-    return NUOSC_OK;
+    return diag_check(d);
 }
+
+long long nuosc_step_count(const nuosc_handle *h) { return h ? h->steps_done : -1; }
 
 int nuosc_open_analysis_file(nuosc_handle *h, const char *path) {
     if (!h || !path) return fail(NUOSC_ERR_INVALID, "null argument");
@@ -966,6 +982,8 @@ struct nuosc_batch {
     int tz = 16;
     bool vac = false;               // some member has a vacuum term (pmo != 0)
     std::vector<nuosc_handle *> m;  // service order: largest first
+    std::vector<nuosc_handle *> user;  // the caller's order (record member indices)
+    std::vector<int> user_index;       // user index of m[i]
     cudaStream_t stream = nullptr;
     cudaEvent_t ev = nullptr;
     char *d_buf = nullptr;          // stage tables | tile starts | cell starts | finalize table | cursors
@@ -1117,7 +1135,7 @@ int batch_build(nuosc_batch *b) {
 }
 
 template <typename T>
-int batch_step_impl(nuosc_batch *b, int nsteps) {
+int batch_step_impl(nuosc_batch *b, int nsteps, int every, nuosc_batch_record *out, int max_out, int *n_out) {
     if (batch_signature(b) != b->sig)
         if (int rc = batch_build<T>(b)) return rc;
     // after everything queued on the members' streams
@@ -1131,16 +1149,32 @@ int batch_step_impl(nuosc_batch *b, int nsteps) {
         b->kernel_launches++;
         h->mom_valid = true;
     }
+    int nrec = 0;
     for (int s = 0; s < nsteps; ++s) {
         CUDA_TRY(cudaGraphLaunch(b->exec, b->stream));
         b->graph_launches++;
         b->kernel_launches += b->per_step;
+        for (size_t i = 0; i < b->m.size(); ++i) {
+            nuosc_handle *h = b->m[i];
+            h->phy_time += h->dt;  // as step_impl: dt added once per step
+            h->steps_done++;
+            if (every <= 0 || h->steps_done % every) continue;
+            // streamed analysis record: the sums land in out[nrec] when the batch stream gets there
+            if (nrec >= max_out) return fail(NUOSC_ERR_INVALID, "batch_step_stream: more than %d records", max_out);
+            nuosc_batch_record &r = out[nrec++];
+            r.member = b->user_index[i];
+            r.step = h->steps_done;
+            r.phy_time = h->phy_time;
+            double *fin = h->d_ana + ANA_BLOCKS * ANA_NQ;
+            CUDA_TRY(launch_analysis<T>((const T *)h->reg[0], h->dG0(), h->dG0b(), h->quad().vw, h->g, h->d_ana, fin,
+                                        b->stream));
+            CUDA_TRY(cudaMemcpyAsync(r.q, fin, ANA_NQ * sizeof(double), cudaMemcpyDeviceToHost, b->stream));
+            b->kernel_launches += 2;
+            if (n_out) *n_out = nrec;
+        }
     }
     CUDA_TRY(cudaEventRecord(b->ev, b->stream));
-    for (nuosc_handle *h : b->m) {
-        CUDA_TRY(cudaStreamWaitEvent(h->stream, b->ev, 0));
-        for (int k = 0; k < nsteps; ++k) h->phy_time += h->dt;  // as step_impl: dt added once per step
-    }
+    for (nuosc_handle *h : b->m) CUDA_TRY(cudaStreamWaitEvent(h->stream, b->ev, 0));
     return 0;
 }
 
@@ -1184,10 +1218,16 @@ int nuosc_batch_create(nuosc_handle *const *members, int n, nuosc_batch **out) {
         delete b;
         return fail(NUOSC_ERR_UNSUPPORTED, "batch: every member needs nz %% 8 == 0 and nz >= 14");
     }
-    b->m.assign(members, members + n);
-    std::stable_sort(b->m.begin(), b->m.end(), [](const nuosc_handle *x, const nuosc_handle *y) {
-        return x->g.ncell * x->g.nvs > y->g.ncell * y->g.nvs;
+    b->user.assign(members, members + n);
+    std::vector<int> idx(n);
+    for (int i = 0; i < n; ++i) idx[i] = i;
+    std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) {
+        return members[x]->g.ncell * members[x]->g.nvs > members[y]->g.ncell * members[y]->g.nvs;
     });
+    for (int i : idx) {
+        b->m.push_back(members[i]);
+        b->user_index.push_back(i);
+    }
     for (const nuosc_handle *h : b->m) {
         b->cells += h->g.ncell;
         b->cellv += h->g.ncell * h->g.nv;
@@ -1211,15 +1251,41 @@ int nuosc_batch_create(nuosc_handle *const *members, int n, nuosc_batch **out) {
     return NUOSC_OK;
 }
 
-int nuosc_batch_step(nuosc_batch *b, int nsteps) {
+int nuosc_batch_step_stream(nuosc_batch *b, int nsteps, int every, nuosc_batch_record *out, int max_out,
+                            int *n_out) {
+    if (n_out) *n_out = 0;
     if (!b) return fail(NUOSC_ERR_INVALID, "null batch");
     if (nsteps < 0) return fail(NUOSC_ERR_INVALID, "nsteps %d", nsteps);
+    if (every > 0 && (!out || max_out < 0)) return fail(NUOSC_ERR_INVALID, "batch_step_stream: no record buffer");
     CUDA_TRY(cudaSetDevice(b->device));
-    const int rc = b->precision == NUOSC_FP64 ? batch_step_impl<double>(b, nsteps) : batch_step_impl<float>(b, nsteps);
+    const int rc = b->precision == NUOSC_FP64 ? batch_step_impl<double>(b, nsteps, every, out, max_out, n_out)
+                                              : batch_step_impl<float>(b, nsteps, every, out, max_out, n_out);
     if (rc) return rc;
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return fail(NUOSC_ERR_CUDA, "batch_step: %s", cudaGetErrorString(e));
     return NUOSC_OK;
+}
+
+int nuosc_batch_step(nuosc_batch *b, int nsteps) { return nuosc_batch_step_stream(b, nsteps, 0, nullptr, 0, nullptr); }
+
+int nuosc_batch_record_diag(const nuosc_batch *b, const nuosc_batch_record *r, nuosc_diag *d) {
+    if (!b || !r || !d) return fail(NUOSC_ERR_INVALID, "null argument");
+    if (r->member < 0 || r->member >= (int)b->user.size()) return fail(NUOSC_ERR_INVALID, "record member %d", r->member);
+    diag_from_sums(b->user[r->member], r->q, r->phy_time, d);
+    return diag_check(*d);
+}
+
+void *nuosc_host_alloc(size_t bytes) {
+    void *p = nullptr;
+    if (cudaMallocHost(&p, bytes) != cudaSuccess) {
+        fail(NUOSC_ERR_OOM, "cudaMallocHost(%zu) failed", bytes);
+        return nullptr;
+    }
+    return p;
+}
+
+void nuosc_host_free(void *p) {
+    if (p) cudaFreeHost(p);
 }
 
 int nuosc_batch_synchronize(nuosc_batch *b) {

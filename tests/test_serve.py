@@ -1,0 +1,168 @@
+"""Serving loop (nuosc_b200.serve).
+
+CPU: the scheduling logic with fake solvers -- every request runs exactly
+its step count, analysis records are streamed every `every` steps and at the
+last step, admission keeps the resident footprint within the budget and
+follows arrival order, oversize requests are rejected, and the one-at-a-time
+queue model.
+GPU: a mixed FP32/FP64 stream of overlapping requests through the real
+batched path; every request's final state and every streamed record equals
+the same request run alone with NuOsc.step_rk4 (bit for bit).
+"""
+import numpy as np
+import pytest
+
+from nuosc_b200 import serve
+
+
+class FakeSolver:
+    def __init__(self, req, device=0):
+        self.req = req
+        self.steps = 0
+        self.closed = False
+
+    def step_rk4(self, n):
+        assert not self.closed and n >= 1
+        self.steps += n
+        assert self.steps <= self.req.steps
+
+    @property
+    def step_count(self):
+        return self.steps
+
+    def synchronize(self):
+        pass
+
+    def analysis(self):
+        return {"phy_time": self.steps * 0.04, "step": self.steps}
+
+    def close(self):
+        self.closed = True
+
+
+class FakeBatch:
+    live = []
+
+    def __init__(self, solvers):
+        assert all(not s.closed for s in solvers)
+        self.solvers = list(solvers)
+        FakeBatch.live.append(self)
+
+    def step_rk4(self, n):
+        for s in self.solvers:
+            s.step_rk4(n)
+
+    def step_stream(self, n, every):
+        recs = []
+        for _ in range(n):
+            for m, s in enumerate(self.solvers):
+                s.step_rk4(1)
+                if s.steps % every == 0:
+                    recs.append((m, s.steps, s.analysis()))
+        return recs
+
+    def collect(self, recs):
+        return recs
+
+    def synchronize(self):
+        pass
+
+    def close(self):
+        FakeBatch.live.remove(self)
+
+
+def fake_server(budget, every=100, **kw):
+    made = {}
+
+    def factory(req, device):
+        made[req.rid] = FakeSolver(req)
+        return made[req.rid]
+
+    srv = serve.Server(budget_bytes=budget, stream_every=every, solver_factory=factory, batch_factory=FakeBatch,
+                       **kw)
+    return srv, made
+
+
+def test_draw_requests_distribution():
+    reqs = serve.draw_requests(400, rate=2.0, seed=3)
+    assert all(r.nx in (32, 64, 128, 256) and r.nz in (32, 64, 128, 256) for r in reqs)
+    assert {r.nn for r in reqs} == {2, 4, 8}
+    assert all(100 <= r.steps <= 5000 for r in reqs)
+    assert all(0.5 <= r.mu <= 2 and 0.7 <= r.alpha <= 1.3 for r in reqs)
+    assert all(0.4 <= r.lnue <= 0.8 and 0.3 <= r.lnueb <= 0.7 and 1e-7 <= r.eps0 <= 1e-3 for r in reqs)
+    arr = np.array([r.arrival for r in reqs])
+    assert np.all(np.diff(arr) > 0)
+    assert 0.6 < np.mean([r.precision == 1 for r in reqs]) < 0.8
+    assert 1.5 < len(reqs) / arr[-1] < 2.5  # Poisson rate
+    assert serve.draw_requests(5, 1.0, 3)[0] == serve.draw_requests(5, 1.0, 3)[0]  # seeded
+
+
+def test_footprint_matches_register_layout():
+    # 4 registers x 8 fields x cells x padded velocities x element size dominate
+    assert serve.footprint_bytes(256, 256, 8, 0) >= 4 * 8 * 256 * 256 * 642 * 8
+    assert serve.footprint_bytes(256, 256, 8, 1) >= 4 * 8 * 256 * 256 * 644 * 4
+    assert serve.footprint_bytes(32, 32, 2, 1) < serve.footprint_bytes(32, 32, 2, 0)
+
+
+def test_scheduling_steps_streams_and_budget():
+    reqs = serve.draw_requests(40, rate=0.0, seed=5, steps=(7, 450), sizes=(32, 64), nns=(2, 4))
+    fp = {r.rid: serve.footprint_bytes(r.nx, r.nz, r.nn, r.precision) for r in reqs}
+    budget = 3 * max(fp.values())
+    seen = {}
+    srv, made = fake_server(budget, every=100, on_diag=lambda rid, step, d: seen.setdefault(rid, []).append(step))
+    rep = srv.run(reqs)
+    assert rep["served"] == 40 and rep["rejected"] == 0
+    assert rep["peak_bytes"] <= budget
+    assert 1 < rep["peak_resident"] < 40  # the budget forced queueing
+    for r in reqs:
+        s = made[r.rid]
+        assert s.steps == r.steps and s.closed
+        want = [0] + list(range(100, r.steps, 100)) + [r.steps]
+        assert seen[r.rid] == sorted(set(want))
+    assert not FakeBatch.live
+
+
+def test_admission_order_and_rejection():
+    reqs = serve.draw_requests(6, rate=0.0, seed=9, steps=(10, 20), sizes=(32,), nns=(2,))
+    big = serve.Request(rid=99, arrival=0.0, nx=256, nz=256, nn=8, mu=1, alpha=1, lnue=0.6, lnueb=0.5, eps0=1e-6,
+                        steps=10, precision=0, seed=1)
+    budget = 2.5 * max(serve.footprint_bytes(r.nx, r.nz, r.nn, r.precision) for r in reqs)
+    order = []
+    srv, made = fake_server(budget, on_diag=lambda rid, step, d: order.append(rid) if step == 0 else None)
+    rep = srv.run(reqs + [big])
+    assert rep["rejected"] == 1 and 99 not in made
+    assert order == [r.rid for r in sorted(reqs, key=lambda r: (r.arrival, r.rid))]
+
+
+def test_fifo_model():
+    reqs = [serve.Request(rid=i, arrival=float(i), nx=32, nz=32, nn=2, mu=1, alpha=1, lnue=0.6, lnueb=0.5,
+                          eps0=1e-6, steps=100, precision=0, seed=1) for i in range(3)]
+    m = serve.fifo_one_at_a_time(reqs, {0: 2.0, 1: 2.0, 2: 0.5})
+    # completions at 2, 4, 4.5 -> latencies 2, 3, 2.5
+    assert m["makespan_s"] == pytest.approx(4.5)
+    assert m["latency_p50_s"] == pytest.approx(2.5)
+
+
+@pytest.mark.gpu
+def test_served_results_equal_solo(gpu):
+    reqs = serve.draw_requests(12, rate=40.0, seed=11, steps=(30, 260), sizes=(32, 64), nns=(2, 4))
+    assert {r.precision for r in reqs} == {0, 1}
+    finals, diags = {}, {}
+    srv = serve.Server(budget_bytes=150e9, stream_every=50,
+                       on_diag=lambda rid, step, d: diags.setdefault(rid, []).append((step, d)),
+                       on_complete=lambda rid, s: finals.__setitem__(rid, s.get_state().view(np.uint64)))
+    rep = srv.run(reqs)
+    assert rep["served"] == 12 and rep["batch_builds"] >= 2
+    assert rep["peak_resident"] > 1  # requests overlapped on the device
+    for r in reqs:
+        s = serve.make_solver(r)
+        want = [(0, serve._analysis(s)[0])]
+        done = 0
+        for step, _ in diags[r.rid][1:]:
+            s.step_rk4(step - done)
+            done = step
+            want.append((step, serve._analysis(s)[0]))
+        assert done == r.steps
+        assert diags[r.rid] == want
+        assert np.array_equal(finals[r.rid], s.get_state().view(np.uint64))
+        s.close()
