@@ -25,6 +25,10 @@ N > 1    one independent full-size solve per GPU (the reference's hot path has
 --impl reference   the reference's own CPU build (oracle/_ref, or the C
          oracle where that build is absent) on the host cores, each step one
          RK4 step of a bounded 128 x 128 x 642 sample of the workload.
+extras   (N = 1, skipped with --no-extras) keys "fp32": the same workload
+         with FP32 state; "batch": 64 uneven instances per precision in one
+         persistent-kernel batch; "serving": a bounded continuous-batching
+         run of Poisson-arriving mixed requests with p50/p99 latency.
 """
 import argparse
 import json
@@ -327,16 +331,131 @@ def bench_ours(args, world, rank, local):
         except Exception as ex:  # report, do not fail the GPU number
             cpu = {"value": None, "error": str(ex)[:200]}
 
+    s.close()
+    extras = {}
+    if rank == 0 and world == 1 and not args.no_extras and w["precision"] == nb.FP64:
+        try:
+            extras["fp32"] = bench_fp32(args, local, value)
+            single = {"f64": value, "f32": extras["fp32"]["value"]}
+            extras["batch"] = bench_batch(args, local, single)
+            extras["serving"] = bench_serving(args, local, single)
+        except Exception as ex:  # report, do not fail the headline number
+            extras["extras_error"] = str(ex)[:300]
+
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": dtype, "data": "synthetic (seeded eps per cell)",
                 "config": config_of(w, nv, "inputs larger than L2 (%.1f GB per register)" % (8 * cells * esize / 1e9)),
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(),
-                "gpu_launches": launches, "diag_after": {k: diag[k] for k in ("phy_time", "maxdP", "surv", "aM0")}}
+                "gpu_launches": launches, "diag_after": {k: diag[k] for k in ("phy_time", "maxdP", "surv", "aM0")},
+                **extras}
         print(json.dumps(line))
-    s.close()
     return 0
+
+
+def bench_fp32(args, local, v64):
+    """The FP32 form of the same workload (state and stencil in float, FP64
+    moments and diagnostics): its cell-steps/s and the ratio to FP64."""
+    import torch
+    import nuosc_b200 as nb
+    w = workload(args.size, args.nn, nb.FP32)
+    s = nb.NuOsc(1, 1, w["nn"], 0, 3, 3, w["x0"], w["x1"], w["x0"], w["x1"], w["dx"], w["dx"], w["cfl"], w["ko"],
+                 precision=nb.FP32, device=local)
+    s.set_mu(w["mu"])
+    s.set_pmo(0.0)
+    s.fillInitValue(1, w["alpha"], w["eps0"], 1.0, w["lnue"], w["lnueb"], seed=w["seed"])
+    cells = s.grid.nx * s.grid.nz * s.grid.nv
+    st = torch.cuda.ExternalStream(nb.lib().nuosc_stream(s.handle))
+    s.step_rk4(args.warmup)
+    s.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    s.step_rk4(args.steps)
+    e1.record(st)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    s.close()
+    v = cells / (ms / 1e3)
+    return {"value": v, "unit": METRIC, "ms_per_step": ms, "vs_fp64": v / v64, "steps": args.steps,
+            "note": "same workload, FP32 state; accuracy vs FP64 in profiles/fp32_vs_fp64_256x642.md"}
+
+
+def mixed_instances(n, seed, precision):
+    """n solves of the mixed-instance recipe: nx, nz from {32, 64, 128, 256},
+    nv from {42, 162, 642}, mu, alpha, spectra widths and eps amplitude drawn
+    per solve (nuosc_b200.serve.draw_requests)."""
+    from nuosc_b200 import serve
+    reqs = serve.draw_requests(n, rate=0.0, seed=seed, steps=(100, 100))
+    for r in reqs:
+        r.precision = precision
+    return reqs
+
+
+def bench_batch(args, local, single):
+    """64 uneven instances per precision in one batch (one persistent kernel
+    per RK stage, the step a CUDA graph): cell-steps/s and the ratio to the
+    single large solve of the same precision."""
+    import torch
+    import nuosc_b200 as nb
+    from nuosc_b200 import serve
+    out = {}
+    for prec, key in ((nb.FP64, "f64"), (nb.FP32, "f32")):
+        reqs = mixed_instances(64, 20240607, prec)
+        solvers = [serve.make_solver(r, local) for r in reqs]
+        cells = sum(r.nx * r.nz * r.nv for r in reqs)
+        b = nb.Batch(solvers)
+        st = torch.cuda.ExternalStream(b.stream())
+        b.step_rk4(args.warmup)
+        b.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        b.step_rk4(args.batch_steps)
+        e1.record(st)
+        e1.synchronize()
+        b.synchronize()
+        ms = e0.elapsed_time(e1) / args.batch_steps
+        info = b.info()
+        b.close()
+        for x in solvers:
+            x.close()
+        v = cells / (ms / 1e3)
+        out[key] = {"value": v, "unit": METRIC, "ms_per_step": ms, "vs_single_large_solve": v / single[key],
+                    "instances": len(reqs), "cell_velocities": cells, "tiles_per_stage": info["tiles"],
+                    "ctas": info["ctas"], "steps": args.batch_steps}
+    out["note"] = ("instances drawn with nuosc_b200.serve.draw_requests(seed 20240607): nx, nz in {32,64,128,256}, "
+                   "nv in {42,162,642}, mu U(0.5,2), alpha U(0.7,1.3), widths U(0.4,0.8)/U(0.3,0.7), "
+                   "eps 10^U(-7,-3); each batched result equals its solo run bit for bit (tests/test_batch.py)")
+    return out
+
+
+def bench_serving(args, local, single):
+    """A bounded serving run: Poisson arrivals of mixed requests (70% FP32),
+    admitted under a 150 GB budget, continuous batching; aggregate
+    cell-steps/s, its ratio to the single large solves doing the same
+    cell-steps, p50/p99 completion latency, and the same arrivals served one
+    at a time on the plain FP64 path."""
+    from nuosc_b200 import serve
+    reqs = serve.draw_requests(args.serve_requests, args.serve_rate, 7, steps=(args.serve_min_steps,
+                                                                               args.serve_max_steps))
+    rep = serve.Server(budget_bytes=150e9, device=local).run(reqs)
+    cs64 = sum(r.cell_steps for r in reqs if r.precision == 0)
+    cs32 = sum(r.cell_steps for r in reqs if r.precision == 1)
+    ref = (cs64 + cs32) / (cs64 / single["f64"] + cs32 / single["f32"])
+    t = serve.solo_fp64_step_times(reqs, device=local)
+    one = serve.fifo_one_at_a_time(reqs, {r.rid: t[(r.nx, r.nz, r.nn)] * r.steps for r in reqs})
+    return {"requests": len(reqs), "rate_per_s": args.serve_rate,
+            "steps_range": [args.serve_min_steps, args.serve_max_steps], "budget_gb": 150,
+            "cell_steps_per_s": rep["cell_steps_per_s"], "cell_steps_per_busy_s": rep["cell_steps_per_busy_s"],
+            "busy_vs_single_large_solve": rep["cell_steps_per_busy_s"] / ref,
+            "latency_p50_s": rep["latency_p50_s"], "latency_p99_s": rep["latency_p99_s"],
+            "makespan_s": rep["makespan_s"], "peak_resident": rep["peak_resident"], "quanta": rep["quanta"],
+            "diverged": rep["diverged"],
+            "one_at_a_time_fp64": {k: one[k] for k in ("cell_steps_per_s", "latency_p50_s", "latency_p99_s",
+                                                       "makespan_s")},
+            "note": "single-large-solve reference = the 1024x1024x642 FP64/FP32 solves timed above, weighted by "
+                    "the requests' FP64/FP32 cell-steps; one-at-a-time latencies from measured per-shape FP64 step "
+                    "times; requests whose state blew up keep stepping (same cost) and are counted in 'diverged'"}
 
 
 def main():
@@ -353,6 +472,12 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-sample", type=int, default=128)
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    ap.add_argument("--no-extras", action="store_true", help="skip the FP32, batch and serving sections")
+    ap.add_argument("--batch-steps", type=int, default=20)
+    ap.add_argument("--serve-requests", type=int, default=64)
+    ap.add_argument("--serve-rate", type=float, default=8.0)
+    ap.add_argument("--serve-min-steps", type=int, default=20)
+    ap.add_argument("--serve-max-steps", type=int, default=500)
     # internal: CPU worker subprocess
     ap.add_argument("--cpu-worker", action="store_true")
     ap.add_argument("--cpu-size", type=int, default=128)
