@@ -264,8 +264,16 @@ int run_stage_xmarch(nuosc_handle *h, bool tma, const XTile &tile, int mode, int
         h->launches++;
     }
     int ps = h->prof_begin(prof_kind(mode));
-    if (tma) CUDA_TRY(launch_stage_xtma<T>(a, mode, h->ko6, tile, h->stream));
-    else CUDA_TRY(launch_stage_xmarch<T>(a, mode, h->ko6, tile, h->stream));
+    if (tma) {
+        CUDA_TRY(launch_stage_xtma<T>(a, mode, h->ko6, tile, h->stream));
+        const int v0 = xtma_tail_v0<T>(h->g);
+        if (v0 < h->g.nvs) {  // the nearly empty last velocity block
+            CUDA_TRY(launch_stage_tail<T>(a, mode, h->ko6, v0, xtma_num_vblocks<T>(h->g), h->stream));
+            h->launches++;
+        }
+    } else {
+        CUDA_TRY(launch_stage_xmarch<T>(a, mode, h->ko6, tile, h->stream));
+    }
     h->prof_end(ps);
     ps = h->prof_begin(5);
     const int nvb = tma ? xtma_num_vblocks<T>(h->g) : xmarch_num_vblocks(h->g, tile);
@@ -991,6 +999,9 @@ struct nuosc_batch {
     long long *d_starts = nullptr;
     FinalizeItem *d_fin = nullptr;
     unsigned long long *d_counter = nullptr;  // work-list cursors of the 4 stage launches
+    char *d_tail = nullptr;         // tail tables (4 stages) | thread starts
+    int ntail = 0;                  // members with a tail block
+    long long tail_threads = 0;
     long long *d_fstarts = nullptr;
     long long ntiles = 0, nmom = 0, cells = 0, cellv = 0;
     int grid[4] = {0, 0, 0, 0};
@@ -1048,10 +1059,18 @@ int batch_build(nuosc_batch *b) {
     std::vector<char> host(tab);
     std::vector<long long> starts(n), fstarts(n);
     std::vector<FinalizeItem> fin(n);
-    long long tiles = 0, nmom = 0;
+    std::vector<TailItem<T>> tails[4];
+    std::vector<long long> tstarts;
+    long long tiles = 0, nmom = 0, tthreads = 0;
     for (int i = 0; i < n; ++i) {
         nuosc_handle *h = b->m[i];
         long long ti = -1;
+        const int v0 = xtma_tail_v0<T>(h->g);
+        if (v0 < h->g.nvs) {
+            tstarts.push_back(tthreads);
+            const int twp = tail_lanes(h->g.nvs - v0);
+            tthreads += (h->g.ncell * twp + 31) / 32 * 32;
+        }
         for (int k = 0; k < 4; ++k) {
             const StageSpec &sp = kStages[k];
             StageArgs<T> a{};
@@ -1069,6 +1088,8 @@ int batch_build(nuosc_batch *b) {
             a.cY = sp.fy == 1.0 ? h->dt : sp.fy * h->dt;
             a.status = h->d_status;
             ti = xtma_batch_fill<T>(&host[((size_t)k * n + i) * b->item_bytes], a, b->ko6, b->tz, h->tile.lx);
+            if (v0 < h->g.nvs)
+                tails[k].push_back(TailItem<T>{a, v0, tail_lanes(h->g.nvs - v0), xtma_num_vblocks<T>(h->g), 0});
             if (ti < 0) return fail(NUOSC_ERR_UNSUPPORTED, "batch member %d (%dx%d) cannot run %d-row TMA tiles", i,
                                     h->g.nx, h->g.nz, b->tz);
         }
@@ -1094,6 +1115,17 @@ int batch_build(nuosc_batch *b) {
     CUDA_TRY(cudaMemcpyAsync(b->d_starts, starts.data(), n * sizeof(long long), cudaMemcpyHostToDevice, b->stream));
     CUDA_TRY(cudaMemcpyAsync(b->d_fstarts, fstarts.data(), n * sizeof(long long), cudaMemcpyHostToDevice, b->stream));
     CUDA_TRY(cudaMemcpyAsync(b->d_fin, fin.data(), n * sizeof(FinalizeItem), cudaMemcpyHostToDevice, b->stream));
+    b->ntail = (int)tstarts.size();
+    b->tail_threads = tthreads;
+    if (b->ntail) {
+        const size_t tb = 4 * (size_t)b->ntail * sizeof(TailItem<T>);
+        if (!b->d_tail) CUDA_TRY(cudaMalloc((void **)&b->d_tail, tb + (size_t)b->ntail * sizeof(long long)));
+        for (int k = 0; k < 4; ++k)
+            CUDA_TRY(cudaMemcpyAsync(b->d_tail + (size_t)k * b->ntail * sizeof(TailItem<T>), tails[k].data(),
+                                     b->ntail * sizeof(TailItem<T>), cudaMemcpyHostToDevice, b->stream));
+        CUDA_TRY(cudaMemcpyAsync(b->d_tail + tb, tstarts.data(), b->ntail * sizeof(long long), cudaMemcpyHostToDevice,
+                                 b->stream));
+    }
     CUDA_TRY(cudaStreamSynchronize(b->stream));  // host staging is freed on return
     b->ntiles = tiles;
     b->nmom = nmom;
@@ -1112,6 +1144,13 @@ int batch_build(nuosc_batch *b) {
         e = launch_stage_xtma_batch<T>(b->d_buf + (size_t)k * n * b->item_bytes, b->d_starts, n, tiles,
                                        b->d_counter + k, kStages[k].mode, b->ko6, b->tz, b->vac, b->grid[k],
                                        b->stream);
+        if (e == cudaSuccess && b->ntail) {
+            const size_t tb = 4 * (size_t)b->ntail * sizeof(TailItem<T>);
+            e = launch_stage_tail_batch<T>((const TailItem<T> *)(b->d_tail + (size_t)k * b->ntail * sizeof(TailItem<T>)),
+                                           (const long long *)(b->d_tail + tb), b->ntail, b->tail_threads,
+                                           kStages[k].mode, b->ko6, b->stream);
+            per_step++;
+        }
         if (e == cudaSuccess) e = launch_moment_finalize_batch(b->d_fin, b->d_fstarts, n, nmom, b->stream);
         per_step += 2;
     }
@@ -1322,6 +1361,7 @@ int nuosc_batch_destroy(nuosc_batch *b) {
     for (nuosc_handle *h : b->m)
         if (h->batch == b) h->batch = nullptr;
     if (b->d_buf) cudaFree(b->d_buf);
+    if (b->d_tail) cudaFree(b->d_tail);
     if (b->ev) cudaEventDestroy(b->ev);
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;

@@ -111,6 +111,26 @@ template <typename T>
 cudaError_t launch_stage_xtma_batch(const void *items, const long long *starts, int n, long long ntiles,
                                     unsigned long long *counter, int mode, bool ko6, int tz, bool vac, int grid,
                                     cudaStream_t s);
+// Tail of the TMA x-march stage (tail.cu): when the last velocity block of
+// the TMA kernel would hold at most a quarter block of real velocities, the
+// velocities from xtma_tail_v0 on are computed by a one-thread-per-(cell,
+// velocity) kernel that writes the last block's moment partials; the TMA
+// kernel then runs the full blocks only.  Returns nvs when there is no tail.
+template <typename T>
+int xtma_tail_v0(const Geom &g);
+int tail_lanes(int width);  // lanes per cell: width rounded up to a power of 2
+template <typename T>
+cudaError_t launch_stage_tail(const StageArgs<T> &a, int mode, bool ko6, int v0, int nvb, cudaStream_t s);
+template <typename T>
+struct TailItem {
+    StageArgs<T> a;
+    int v0, twp, nvb, pad;
+};
+// starts[i]: first thread of item i (ranges of ncell * twp threads, each
+// rounded up to a multiple of 32); total: threads of all items
+template <typename T>
+cudaError_t launch_stage_tail_batch(const TailItem<T> *items, const long long *starts, int n, long long total,
+                                    int mode, bool ko6, cudaStream_t s);
 // moment_finalize of many instances in one launch (xmarch.cu); starts[i] =
 // sum over instances 0..i-1 of ncell * 12
 struct FinalizeItem {

@@ -515,16 +515,19 @@ __device__ __forceinline__ bool xtma_march(const TmaMaps *const &mp, const Stage
     return aborted;
 }
 
+// grid (velocity blocks run by this kernel, z tiles, 2 x x-segments); nvb:
+// velocity blocks of the moment partials (one more when a tail kernel runs
+// the last block)
 template <typename T, int R, int MODE, int TZ, bool VAC>
 __global__ void __launch_bounds__(32 * TZ, tma_ctas_per_sm<T, TZ>())
-    k_xtma(const __grid_constant__ TmaMaps maps, const StageArgs<T> a, int LX) {
+    k_xtma(const __grid_constant__ TmaMaps maps, const StageArgs<T> a, int LX, int nvb) {
     extern __shared__ __align__(1024) unsigned char smem[];
     __shared__ MarchShared<T> sh;
     const int xs = (blockIdx.z >> 1) * LX;
     if (xs >= a.g.nx) return;
     const TmaMaps *mp = &maps;
-    xtma_march<T, R, MODE, TZ, VAC, false>(mp, a, blockIdx.y * TZ, blockIdx.x, gridDim.x, xs,
-                                           min(xs + LX, a.g.nx), blockIdx.z & 1, smem, sh);
+    xtma_march<T, R, MODE, TZ, VAC, false>(mp, a, blockIdx.y * TZ, blockIdx.x, nvb, xs, min(xs + LX, a.g.nx),
+                                           blockIdx.z & 1, smem, sh);
 }
 
 // One instance's stage in a batched launch: its tensor maps (over the stage's
@@ -535,6 +538,7 @@ struct __align__(64) BatchItem {
     TmaMaps maps;
     StageArgs<T> a;
     int ntz, nvb, lx, nseg;
+    int nvbm;  // velocity blocks run by the march (nvb - 1 when a tail kernel runs the last)
 };
 
 // Persistent batched stage kernel.  The tiles of all instances form one list
@@ -574,9 +578,9 @@ __global__ void __launch_bounds__(32 * TZ, tma_ctas_per_sm<T, TZ>())
                     else hi = mid - 1;
                 }
                 const BatchItem<T> &e = items[lo];
-                long long loc = it - starts[lo];  // ((seg * 2 + half) * ntz + zt) * nvb + vb
-                const int vb = (int)(loc % e.nvb);
-                loc /= e.nvb;
+                long long loc = it - starts[lo];  // ((seg * 2 + half) * ntz + zt) * nvbm + vb
+                const int vb = (int)(loc % e.nvbm);
+                loc /= e.nvbm;
                 const int zt = (int)(loc % e.ntz);
                 loc /= e.ntz;
                 const int xs = (int)(loc >> 1) * e.lx;
@@ -645,6 +649,13 @@ bool make_map(CUtensorMap *m, const T *base, const Geom &g, int rows) {
               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// velocity blocks the march runs: all of them, or all but the tail block
+template <typename T>
+int march_vblocks(const Geom &g) {
+    const int v0 = xtma_tail_v0<T>(g);
+    return v0 == g.nvs ? xtma_num_vblocks<T>(g) : v0 / vblock<T>();
+}
+
 template <typename T>
 bool make_maps(TmaMaps *m, const T *base, const Geom &g, int tz, int r) {
     return make_map<T>(&m->zr, base, g, tz + 2 * r) && make_map<T>(&m->tzr, base, g, tz + r) &&
@@ -665,10 +676,12 @@ cudaError_t launch_t(const StageArgs<T> &a, XTile t, cudaStream_t s) {
                                          (int)smem);
     if (e != cudaSuccess) return e;
     const int nseg = (a.g.nx + t.lx - 1) / t.lx;
+    const int nvb = xtma_num_vblocks<T>(a.g), nvbm = march_vblocks<T>(a.g);
+    if (nvbm < 1) return cudaSuccess;  // the tail kernel runs every velocity
     // velocity blocks fastest: the CTAs resident at once read whole velocity
     // rows of a few z rows (DRAM page locality) rather than one block of many rows
-    dim3 grid((a.g.nvs + Sl::VB - 1) / Sl::VB, a.g.nz / TZ, nseg * 2);
-    k_xtma<T, R, MODE, TZ, VAC><<<grid, 32 * TZ, smem, s>>>(maps, a, t.lx);
+    dim3 grid(nvbm, a.g.nz / TZ, nseg * 2);
+    k_xtma<T, R, MODE, TZ, VAC><<<grid, 32 * TZ, smem, s>>>(maps, a, t.lx, nvb);
     return cudaGetLastError();
 }
 
@@ -762,10 +775,11 @@ long long xtma_batch_fill(void *item, const StageArgs<T> &a, bool ko6, int tz, i
     e.a = a;
     e.ntz = a.g.nz / tz;
     e.nvb = xtma_num_vblocks<T>(a.g);
+    e.nvbm = march_vblocks<T>(a.g);
     e.lx = lx;
     e.nseg = (a.g.nx + lx - 1) / lx;
     memcpy(item, (const void *)&e, sizeof e);
-    return (long long)e.ntz * e.nvb * 2 * e.nseg;
+    return (long long)e.ntz * e.nvbm * 2 * e.nseg;
 }
 
 template <typename T>
@@ -789,6 +803,12 @@ int xtma_num_vblocks(const Geom &g) {
 }
 
 template <typename T>
+int xtma_tail_v0(const Geom &g) {
+    const int nvb = xtma_num_vblocks<T>(g), last = (nvb - 1) * vblock<T>();
+    return 4 * (g.nvs - last) <= vblock<T>() ? last : g.nvs;
+}
+
+template <typename T>
 cudaError_t launch_stage_xtma(const StageArgs<T> &a, int mode, bool ko6, XTile t, cudaStream_t s) {
     if (!a.mom_part || a.g.nz % t.tz) return cudaErrorInvalidValue;
     if (t.tz == 16) return ko6 ? launch_tv<T, 3, 16>(a, mode, t, s) : launch_tv<T, 2, 16>(a, mode, t, s);
@@ -799,6 +819,8 @@ template bool xtma_supported<double>(const Geom &, XTile);
 template bool xtma_supported<float>(const Geom &, XTile);
 template int xtma_num_vblocks<double>(const Geom &);
 template int xtma_num_vblocks<float>(const Geom &);
+template int xtma_tail_v0<double>(const Geom &);
+template int xtma_tail_v0<float>(const Geom &);
 template cudaError_t launch_stage_xtma<double>(const StageArgs<double> &, int, bool, XTile, cudaStream_t);
 template cudaError_t launch_stage_xtma<float>(const StageArgs<float> &, int, bool, XTile, cudaStream_t);
 template size_t xtma_batch_item_bytes<double>();
