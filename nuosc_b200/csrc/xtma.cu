@@ -95,6 +95,14 @@ __device__ __forceinline__ void tma_load_4d(unsigned dst, const CUtensorMap *map
         "l"((unsigned long long)map), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(bar)
         : "memory");
 }
+// per-thread 8-byte async copy global -> shared and its groups
+template <typename T>
+__device__ __forceinline__ void cp_async8(T *dst, const T *src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 __device__ __forceinline__ void bulk_load(unsigned dst, const void *src, unsigned bytes, unsigned bar) {
     asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(dst),
                  "l"(src), "r"(bytes), "r"(bar)
@@ -197,6 +205,25 @@ constexpr int tma_ctas_per_sm() {
     return TZ == 16 ? 1 : 2;
 }
 
+// Ring geometry of one march.  In the last stage (S4) with 16-row tiles (one
+// CTA per SM) the accumulator input A of the epilogue is prefetched one
+// plane ahead by per-thread cp.async copies into a double-buffered shared
+// region (32 KB beside the 168 KB box ring).  Elsewhere the pointwise inputs
+// are plain loads at the top of each plane: in S2/S3 the prefetch of A, or
+// of A and U with a shallower box ring, measured slower; with 8-row tiles
+// (two CTAs per SM) there is no room for it.
+template <typename T, int R, int MODE, int TZ>
+struct MarchCfg {
+    static constexpr int NIN = 1;  // prefetched inputs per thread and plane (A)
+    static constexpr bool PF = TZ == 16 && MODE == MODE_S4;
+    static constexpr int D = 2;           // boxes issued ahead of their first use
+    static constexpr int NS = R + D + 2;  // a box lives from its front use to its centre use, plus slack
+    // prefetch buffers: [2][4 fields][TZ warps][32 lanes] of vpt<T>() values
+    static constexpr size_t pw = PF ? (size_t)2 * NIN * 4 * TZ * 32 * vpt<T>() * sizeof(T) : 0;
+    static constexpr size_t ring = (size_t)NS * Slot<T, TZ, R>::bytes;
+    static constexpr size_t smem = ring + 2 * NS * 8 + pw;  // box ring | mbarriers | prefetch buffers
+};
+
 }  // namespace
 
 // value of x, re-read from (shared) memory at each use when V: keeps values
@@ -220,13 +247,15 @@ __device__ __forceinline__ bool xtma_march(const TmaMaps *const &mp, const Stage
                                            const int nvb, const int xs, const int xe, const int half,
                                            unsigned char *smem, MarchShared<T> &sh) {
     using S = Slot<T, TZ, R>;
+    using CF = MarchCfg<T, R, MODE, TZ>;
     constexpr int NP = vpt<T>();       // velocities per thread
     constexpr int VB = S::VB;          // velocities per CTA
     constexpr int W = 2 * R + 1;
     constexpr int ZR = S::ZR;
-    constexpr int D = 2;               // boxes issued ahead of their first use
-    constexpr int NS = R + D + 2;      // a box lives from its front use to its centre use, plus slack
-    unsigned long long *bars = (unsigned long long *)(smem + NS * S::bytes);  // full[NS], empty[NS]
+    constexpr int D = CF::D;
+    constexpr int NS = CF::NS;
+    unsigned long long *bars = (unsigned long long *)(smem + CF::ring);  // full[NS], empty[NS]
+    T *pw = (T *)(smem + CF::ring + 2 * NS * 8);  // prefetch buffers (CF::PF)
     int &s_abort = sh.abort;
 
     const Geom g = a.g;
@@ -347,22 +376,41 @@ __device__ __forceinline__ bool xtma_march(const TmaMaps *const &mp, const Stage
         for (int j = 0; j < R + D && j < nboxes; ++j)
             if (j >= R || j < nplanes) ok = ok && issue(j);
 
+    // prefetch of A for plane i into buffer i & 1: this thread's values, at
+    // [buf][field][warp][lane]; one commit group per plane (empty past the
+    // last plane)
+    auto prefetch = [&](int i) {
+        if constexpr (CF::PF) {
+            if (i < nplanes && vact) {
+                const long long o = hoff + (long long)(xs + i) * P + own;
+                T *b = pw + (size_t)(i & 1) * CF::NIN * 4 * TZ * 32 * NP + (size_t)(r * 32 + lane) * NP;
+#pragma unroll
+                for (int f = 0; f < 4; ++f) cp_async8(b + (size_t)f * TZ * 32 * NP, rd<SA>(a.acc_src) + o + f * fs);
+            }
+            cp_async_commit();
+        }
+    };
+    prefetch(0);
+
     for (int i = 0; i < nplanes; ++i) {
         if (tid == 0 && ok && i + R + D < nboxes) ok = issue(i + R + D);
         if (tid == 0 && !ok) s_abort = 1;
         const int x = xs + i;
         const long long oc = hoff + (long long)x * P + own;
-        // pointwise epilogue inputs first (they are not in the ring)
-        const T *up = MODE == MODE_S23 ? rd<SA>(a.u) + oc : nullptr;
-        const T *ap = MODE != MODE_S1 ? rd<SA>(a.acc_src) + oc : nullptr;
         T uin[4][NP], ain[4][NP];
+        prefetch(i + 1);
+        {
+            // pointwise epilogue inputs first (they are not in the ring)
+            const T *up = MODE == MODE_S23 ? rd<SA>(a.u) + oc : nullptr;
+            const T *ap = MODE != MODE_S1 && !CF::PF ? rd<SA>(a.acc_src) + oc : nullptr;
 #pragma unroll
-        for (int f = 0; f < 4; ++f) {
+            for (int f = 0; f < 4; ++f) {
 #pragma unroll
-            for (int p = 0; p < NP; ++p) uin[f][p] = ain[f][p] = T(0);
-            if (vact) {
-                if (MODE == MODE_S23) ldv<T, NP>(up + f * fs, uin[f]);
-                if (MODE != MODE_S1) ldv<T, NP>(ap + f * fs, ain[f]);
+                for (int p = 0; p < NP; ++p) uin[f][p] = ain[f][p] = T(0);
+                if (vact) {
+                    if (MODE == MODE_S23) ldv<T, NP>(up + f * fs, uin[f]);
+                    if (MODE != MODE_S1 && !CF::PF) ldv<T, NP>(ap + f * fs, ain[f]);
+                }
             }
         }
         const int jf = i + R, sf = jf % NS, sc = i % NS;
@@ -418,6 +466,13 @@ __device__ __forceinline__ bool xtma_march(const TmaMaps *const &mp, const Stage
         }
         __syncwarp();
         if (lane == 0) mbar_arrive(smem_u32(&bars[NS + sc]));  // centre use is the box's last use
+        if constexpr (CF::PF) {
+            cp_async_wait1();  // this thread's copies of plane i (plane i + 1's may still fly)
+            const T *b = pw + (size_t)(i & 1) * CF::NIN * 4 * TZ * 32 * NP + (size_t)(r * 32 + lane) * NP;
+#pragma unroll
+            for (int f = 0; f < 4; ++f)
+                if (vact) ldv<T, NP>(b + (size_t)f * TZ * 32 * NP, ain[f]);
+        }
 
         T outm[4][NP];
 #pragma unroll
@@ -499,6 +554,7 @@ __device__ __forceinline__ bool xtma_march(const TmaMaps *const &mp, const Stage
                 for (int p = 0; p < NP; ++p) q[f][k][p] = q[f][k + 1][p];
     }
     __syncthreads();
+    if constexpr (CF::PF) cp_async_wait0();  // no copy into shared memory outlives the tile
     const bool aborted = s_abort != 0;
     if (tid == 0) {
         if (aborted) {
@@ -664,14 +720,12 @@ bool make_maps(TmaMaps *m, const T *base, const Geom &g, int tz, int r) {
 
 template <typename T, int R, int MODE, int TZ, bool VAC>
 cudaError_t launch_t(const StageArgs<T> &a, XTile t, cudaStream_t s) {
-    constexpr int NS = R + 2 + 2;
-    using Sl = Slot<T, TZ, R>;
-    static_assert(tma_ctas_per_sm<T, TZ>() * (NS * Sl::bytes + 2 * NS * 8 + sizeof(MarchShared<T>) + 64 + 1024) <=
-                      228 * 1024,
+    using CF = MarchCfg<T, R, MODE, TZ>;
+    static_assert(tma_ctas_per_sm<T, TZ>() * (CF::smem + sizeof(MarchShared<T>) + 64 + 1024) <= 228 * 1024,
                   "ring exceeds shared memory");
     TmaMaps maps;
     if (!make_maps<T>(&maps, a.in, a.g, TZ, R)) return cudaErrorInvalidValue;
-    const size_t smem = (size_t)NS * Sl::bytes + 2 * NS * 8;
+    const size_t smem = CF::smem;
     cudaError_t e = cudaFuncSetAttribute(k_xtma<T, R, MODE, TZ, VAC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e != cudaSuccess) return e;
@@ -703,7 +757,7 @@ cudaError_t launch_tv(const StageArgs<T> &a, int mode, XTile t, cudaStream_t s) 
 // ---- batched launch: one persistent grid per stage over many instances
 template <typename T, int R, int MODE, int TZ>
 constexpr size_t batch_smem() {
-    return (size_t)(R + 4) * Slot<T, TZ, R>::bytes + 2 * (R + 4) * 8;
+    return MarchCfg<T, R, MODE, TZ>::smem;
 }
 
 template <typename T, int R, int MODE, int TZ, bool VAC>
