@@ -1069,7 +1069,7 @@ int batch_build(nuosc_batch *b) {
         if (v0 < h->g.nvs) {
             tstarts.push_back(tthreads);
             const int twp = tail_lanes(h->g.nvs - v0);
-            tthreads += (h->g.ncell * twp + 31) / 32 * 32;
+            tthreads += (h->g.ncell * 2 * twp + 31) / 32 * 32;
         }
         for (int k = 0; k < 4; ++k) {
             const StageSpec &sp = kStages[k];

@@ -126,8 +126,9 @@ struct TailItem {
     StageArgs<T> a;
     int v0, twp, nvb, pad;
 };
-// starts[i]: first thread of item i (ranges of ncell * twp threads, each
-// rounded up to a multiple of 32); total: threads of all items
+// starts[i]: first thread of item i (ranges of 2 * ncell * twp threads, one
+// per (cell, flavour half, tail lane), each rounded up to a multiple of 32);
+// total: threads of all items
 template <typename T>
 cudaError_t launch_stage_tail_batch(const TailItem<T> *items, const long long *starts, int n, long long total,
                                     int mode, bool ko6, cudaStream_t s);

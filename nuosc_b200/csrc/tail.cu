@@ -5,12 +5,12 @@
 // (642 = 20 x 32 + 2 in FP64, 644 = 10 x 64 + 4 in FP32), a CTA for that
 // block would issue a full block's instructions for a handful of active
 // lanes -- up to a tenth of the stage's issue slots.  Those tail velocities
-// are computed here instead, one thread per (cell, tail velocity) with all 8
-// fields, the stencil read through the read-only cache (the tail columns of
-// a few planes stay in L2), the same fused RK epilogue, and the velocity-
-// moment partials of the written state summed over the tail lanes of the
-// cell into the last block's slots of the partial array, so the fixed-order
-// moment_finalize is unchanged.
+// are computed here instead, one thread per (cell, tail velocity, flavour
+// half) with 4 fields, the stencil read through the read-only cache (the
+// tail columns of a few planes stay in L2), the same fused RK epilogue, and
+// the velocity-moment partials of the written state summed over the tail
+// lanes of the (cell, half) into the last block's slots of the partial
+// array, so the fixed-order moment_finalize is unchanged.
 #include "internal.cuh"
 #include "physics.cuh"
 
@@ -18,18 +18,19 @@ namespace nuosc {
 
 namespace {
 
-// One (cell, velocity) of the tail; every lane of the warp calls it (the
-// moment reduction shuffles across the twp lanes of a cell), act says
-// whether the lane holds a real point.  twp: lanes per cell (power of 2).
+// One (cell, velocity, flavour half) of the tail; every lane of the warp
+// calls it (the moment reduction shuffles across the twp lanes of a cell and
+// half), act says whether the lane holds a real point.  twp: lanes per
+// (cell, half) (power of 2).  The commutator couples the four fields of a
+// half only to each other once the moments are known, so a half is a
+// complete unit of work.
 template <typename T, bool KO6, int MODE>
-__device__ __forceinline__ void tail_point(const StageArgs<T> &a, const long long cell, const int v, const bool act,
-                                           const int twp, const int nvb, const int lane_in_cell) {
+__device__ __forceinline__ void tail_point(const StageArgs<T> &a, const long long cell, const int half, const int v,
+                                           const bool act, const int twp, const int nvb, const int lane_in_cell) {
     const Geom g = a.g;
-    double mom[2][NMOM];
+    double mom[NMOM];
 #pragma unroll
-    for (int h = 0; h < 2; ++h)
-#pragma unroll
-        for (int k = 0; k < NMOM; ++k) mom[h][k] = 0.0;
+    for (int k = 0; k < NMOM; ++k) mom[k] = 0.0;
     if (act) {
         const int i = (int)(cell / g.nz), j = (int)(cell - (long long)i * g.nz);
         constexpr int R = KO6 ? 3 : 2;
@@ -45,39 +46,32 @@ __device__ __forceinline__ void tail_point(const StageArgs<T> &a, const long lon
         const T kx = T(a.c.kx), kz = T(a.c.kz);
         const double *m = a.mom_in + cell * NMOM;
         const T ia = T(inp(m, vxd, vyd, vzd)), ib = T(inp(m + 4, vxd, vyd, vzd)), ie = T(inp(m + 8, vxd, vyd, vzd));
-        T cen[NF], adv[NF], ko[NF];
+        const long long hoff = (long long)half * 4 * g.fs;
+        T c4[4], a4[4], k4[4];
 #pragma unroll
-        for (int f = 0; f < NF; ++f) {
-            const T *F = a.in + f * g.fs;
+        for (int f = 0; f < 4; ++f) {
+            const T *F = a.in + hoff + f * g.fs;
             T zs[7], xs[7];
 #pragma unroll
             for (int k = 0; k < 7; ++k) {
                 zs[k] = __ldg(F + oz[k]);
                 xs[k] = __ldg(F + ox[k]);
             }
-            cen[f] = zs[3];
-            adv[f] = adv_axis(zs, fz) + adv_axis(xs, fx);
-            ko[f] = ko_axis<T, KO6>(zs, kz) + ko_axis<T, KO6>(xs, kx);
+            c4[f] = zs[3];
+            a4[f] = adv_axis(zs, fz) + adv_axis(xs, fx);
+            k4[f] = ko_axis<T, KO6>(zs, kz) + ko_axis<T, KO6>(xs, kx);
         }
-        T kv[NF];
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            T c4[4] = {cen[4 * h], cen[4 * h + 1], cen[4 * h + 2], cen[4 * h + 3]};
-            T a4[4] = {adv[4 * h], adv[4 * h + 1], adv[4 * h + 2], adv[4 * h + 3]};
-            T k4[4] = {ko[4 * h], ko[4 * h + 1], ko[4 * h + 2], ko[4 * h + 3]}, o4[4];
-            commutator_half(c4, ia, ib, ie, a.c, o4, a4, k4);
-#pragma unroll
-            for (int f = 0; f < 4; ++f) kv[4 * h + f] = o4[f];
-        }
-        const long long o = oz[3];
+        T kv[4];
+        commutator_half(c4, ia, ib, ie, a.c, kv, a4, k4);
+        const long long o = oz[3] + hoff;
         const T cA = T(a.cA), cY = T(a.cY);
-        T outm[NF];  // the written state whose moments the next stage needs
+        T outm[4];  // the written state whose moments the next stage needs
 #pragma unroll
-        for (int f = 0; f < NF; ++f) {
+        for (int f = 0; f < 4; ++f) {
             const long long idx = o + f * g.fs;
             if (MODE == MODE_S1) {
-                a.acc_dst[idx] = cen[f] + cA * kv[f];
-                outm[f] = cen[f] + cY * kv[f];
+                a.acc_dst[idx] = c4[f] + cA * kv[f];
+                outm[f] = c4[f] + cY * kv[f];
                 a.y_dst[idx] = outm[f];
             } else if (MODE == MODE_S23) {
                 a.acc_dst[idx] = a.acc_src[idx] + cA * kv[f];
@@ -91,48 +85,42 @@ __device__ __forceinline__ void tail_point(const StageArgs<T> &a, const long lon
         // velocity-moment contributions (nuosc_class.cpp:69-71): moment 4c + j
         // = weight j (w, w vx, w vy, w vz) x combination c of the half
         const double w4[4] = {wd, vxd * wd, vyd * wd, vzd * wd};
+        double d[3];
+        if (half == 0) moment_terms<false>(outm[0], outm[1], outm[2], outm[3], d[0], d[1], d[2]);
+        else moment_terms<true>(outm[0], outm[1], outm[2], outm[3], d[0], d[1], d[2]);
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            double d[3];
-            if (h == 0) moment_terms<false>(outm[0], outm[1], outm[2], outm[3], d[0], d[1], d[2]);
-            else moment_terms<true>(outm[4], outm[5], outm[6], outm[7], d[0], d[1], d[2]);
+        for (int c = 0; c < 3; ++c)
 #pragma unroll
-            for (int c = 0; c < 3; ++c)
-#pragma unroll
-                for (int jw = 0; jw < 4; ++jw) mom[h][4 * c + jw] = w4[jw] * d[c];
-        }
+            for (int jw = 0; jw < 4; ++jw) mom[4 * c + jw] = w4[jw] * d[c];
     }
-    // sum over the cell's lanes (xor offsets below twp stay inside its group)
+    // sum over the lanes of the (cell, half) (xor offsets below twp stay inside its group)
     for (int off = twp >> 1; off > 0; off >>= 1)
 #pragma unroll
-        for (int h = 0; h < 2; ++h)
-#pragma unroll
-            for (int k = 0; k < NMOM; ++k) mom[h][k] += __shfl_xor_sync(0xffffffffu, mom[h][k], off);
+        for (int k = 0; k < NMOM; ++k) mom[k] += __shfl_xor_sync(0xffffffffu, mom[k], off);
     if (lane_in_cell == 0 && cell < g.ncell) {
-        double *p = a.mom_part + (cell * nvb + (nvb - 1)) * 2 * NMOM;
+        double *p = a.mom_part + ((cell * nvb + (nvb - 1)) * 2 + half) * NMOM;
 #pragma unroll
-        for (int h = 0; h < 2; ++h)
-#pragma unroll
-            for (int k = 0; k < NMOM; ++k) p[h * NMOM + k] = mom[h][k];
+        for (int k = 0; k < NMOM; ++k) p[k] = mom[k];
     }
 }
 
 constexpr int TAIL_BLOCK = 256;
 
+// thread t: lane l = t % twp of (cell, half) = (t / twp) / 2, (t / twp) % 2
 template <typename T, bool KO6, int MODE>
-__global__ void __launch_bounds__(TAIL_BLOCK) k_stage_tail(const StageArgs<T> a, int v0, int twp, int nvb) {
+__global__ void __launch_bounds__(TAIL_BLOCK, 3) k_stage_tail(const StageArgs<T> a, int v0, int twp, int nvb) {
     const long long t = (long long)blockIdx.x * TAIL_BLOCK + threadIdx.x;
     const int l = (int)(t & (twp - 1));
-    const long long cell = t / twp;
+    const long long ch = t / twp, cell = ch >> 1;
     const int v = v0 + l;
-    tail_point<T, KO6, MODE>(a, cell, v, cell < a.g.ncell && v < a.g.nvs, twp, nvb, l);
+    tail_point<T, KO6, MODE>(a, cell, (int)(ch & 1), v, cell < a.g.ncell && v < a.g.nvs, twp, nvb, l);
 }
 
 // many instances' tails in one launch: item i covers threads [starts[i],
-// starts[i] + ncell_i * twp_i), each range a multiple of 32 threads so that
+// starts[i] + 2 ncell_i twp_i), each range a multiple of 32 threads so that
 // no warp spans two instances
 template <typename T, bool KO6, int MODE>
-__global__ void __launch_bounds__(TAIL_BLOCK) k_stage_tail_batch(const TailItem<T> *__restrict__ items,
+__global__ void __launch_bounds__(TAIL_BLOCK, 2) k_stage_tail_batch(const TailItem<T> *__restrict__ items,
                                                                  const long long *__restrict__ starts, int n,
                                                                  long long total) {
     const long long t = (long long)blockIdx.x * TAIL_BLOCK + threadIdx.x;
@@ -146,14 +134,14 @@ __global__ void __launch_bounds__(TAIL_BLOCK) k_stage_tail_batch(const TailItem<
     const TailItem<T> &e = items[lo];
     const long long u = t - starts[lo];
     const int l = (int)(u & (e.twp - 1));
-    const long long cell = u / e.twp;
+    const long long ch = u / e.twp, cell = ch >> 1;
     const int v = e.v0 + l;
-    tail_point<T, KO6, MODE>(e.a, cell, v, cell < e.a.g.ncell && v < e.a.g.nvs, e.twp, e.nvb, l);
+    tail_point<T, KO6, MODE>(e.a, cell, (int)(ch & 1), v, cell < e.a.g.ncell && v < e.a.g.nvs, e.twp, e.nvb, l);
 }
 
 template <typename T, bool KO6>
 cudaError_t launch_tail_ko(const StageArgs<T> &a, int mode, int v0, int twp, int nvb, cudaStream_t s) {
-    const long long threads = a.g.ncell * twp;
+    const long long threads = a.g.ncell * 2 * twp;
     const unsigned blocks = (unsigned)((threads + TAIL_BLOCK - 1) / TAIL_BLOCK);
     switch (mode) {
     case MODE_S1: k_stage_tail<T, KO6, MODE_S1><<<blocks, TAIL_BLOCK, 0, s>>>(a, v0, twp, nvb); break;
