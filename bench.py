@@ -17,9 +17,9 @@ e2e      the same metric through the public C ABI with host buffers: upload
          the state from pinned host memory, K steps each followed by
          analysis() (diagnostics read back), download the final state.
 roofline the dominant kernel (the S2/S3 stage kernel) timed live with CUDA
-         events: algorithmic bytes per launch (5 state passes x 8 fields x
-         8 B per cell-velocity) / mean launch time, against the measured HBM
-         copy bandwidth in MEASURED_PEAKS.json.
+         events: algorithmic bytes per launch (4.5 state passes on average --
+         S2 4, S3 5 -- x 8 fields x 8 B per cell-velocity) / mean launch
+         time, against the measured HBM copy bandwidth in MEASURED_PEAKS.json.
 N > 1    one independent full-size solve per GPU (the reference's hot path has
          no exchange on one GPU); value = all ranks' cell-steps / max time.
 --impl reference   the reference's own CPU build (oracle/_ref, or the C
@@ -43,8 +43,8 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "cell-steps/s"
-BYTES_PER_CELL_STEP = {"f64": 1024, "f32": 512}  # 16 state passes x 8 fields x sizeof(real)
-STAGE_S23_PASSES = 5
+BYTES_PER_CELL_STEP = {"f64": 960, "f32": 480}  # 15 state passes x 8 fields x sizeof(real)
+STAGE_S23_PASSES = 4.5  # S2 reads A and Ya, writes A and Yb (4); S3 also reads U (5)
 
 
 def workload(size, nn, precision):

@@ -77,6 +77,12 @@ __device__ __forceinline__ void tail_point(const StageArgs<T> &a, const long lon
                 a.acc_dst[idx] = a.acc_src[idx] + cA * kv[f];
                 outm[f] = a.u[idx] + cY * kv[f];
                 a.y_dst[idx] = outm[f];
+            } else if (MODE == MODE_S2) {
+                const T a1 = a.acc_src[idx];
+                const T u = fma(T(1.5), a1, T(-0.5) * c4[f]);  // U = 1.5 A1 - 0.5 Y2
+                a.acc_dst[idx] = a1 + cA * kv[f];
+                outm[f] = u + cY * kv[f];
+                a.y_dst[idx] = outm[f];
             } else {
                 outm[f] = a.acc_src[idx] + cA * kv[f];
                 a.acc_dst[idx] = outm[f];
@@ -146,6 +152,7 @@ cudaError_t launch_tail_ko(const StageArgs<T> &a, int mode, int v0, int twp, int
     switch (mode) {
     case MODE_S1: k_stage_tail<T, KO6, MODE_S1><<<blocks, TAIL_BLOCK, 0, s>>>(a, v0, twp, nvb); break;
     case MODE_S23: k_stage_tail<T, KO6, MODE_S23><<<blocks, TAIL_BLOCK, 0, s>>>(a, v0, twp, nvb); break;
+    case MODE_S2: k_stage_tail<T, KO6, MODE_S2><<<blocks, TAIL_BLOCK, 0, s>>>(a, v0, twp, nvb); break;
     case MODE_S4: k_stage_tail<T, KO6, MODE_S4><<<blocks, TAIL_BLOCK, 0, s>>>(a, v0, twp, nvb); break;
     default: return cudaErrorInvalidValue;
     }
@@ -159,6 +166,7 @@ cudaError_t launch_tail_batch_ko(const TailItem<T> *items, const long long *star
     switch (mode) {
     case MODE_S1: k_stage_tail_batch<T, KO6, MODE_S1><<<blocks, TAIL_BLOCK, 0, s>>>(items, starts, n, total); break;
     case MODE_S23: k_stage_tail_batch<T, KO6, MODE_S23><<<blocks, TAIL_BLOCK, 0, s>>>(items, starts, n, total); break;
+    case MODE_S2: k_stage_tail_batch<T, KO6, MODE_S2><<<blocks, TAIL_BLOCK, 0, s>>>(items, starts, n, total); break;
     case MODE_S4: k_stage_tail_batch<T, KO6, MODE_S4><<<blocks, TAIL_BLOCK, 0, s>>>(items, starts, n, total); break;
     default: return cudaErrorInvalidValue;
     }

@@ -494,6 +494,10 @@ __device__ __forceinline__ bool xtma_march(const TmaMaps *const &mp, const Stage
                 } else if (MODE == MODE_S23) {
                     ain[f][p] = ain[f][p] + cA * kk[f];
                     outm[f][p] = uin[f][p] + cY * kk[f];
+                } else if (MODE == MODE_S2) {
+                    const T u = fma(T(1.5), ain[f][p], T(-0.5) * cen[f]);  // U = 1.5 A1 - 0.5 Y2
+                    ain[f][p] = ain[f][p] + cA * kk[f];
+                    outm[f][p] = u + cY * kk[f];
                 } else {
                     outm[f][p] = ain[f][p] + cA * kk[f];
                 }
@@ -507,7 +511,7 @@ __device__ __forceinline__ bool xtma_march(const TmaMaps *const &mp, const Stage
                 if (MODE == MODE_S1) {
                     stv<T, NP>(dp + f * fs, uin[f]);
                     stv<T, NP>(yp + f * fs, outm[f]);
-                } else if (MODE == MODE_S23) {
+                } else if (MODE == MODE_S23 || MODE == MODE_S2) {
                     stv<T, NP>(dp + f * fs, ain[f]);
                     stv<T, NP>(yp + f * fs, outm[f]);
                 } else {
@@ -744,6 +748,7 @@ cudaError_t launch_tm(const StageArgs<T> &a, int mode, XTile t, cudaStream_t s) 
     switch (mode) {
     case MODE_S1: return launch_t<T, R, MODE_S1, TZ, VAC>(a, t, s);
     case MODE_S23: return launch_t<T, R, MODE_S23, TZ, VAC>(a, t, s);
+    case MODE_S2: return launch_t<T, R, MODE_S2, TZ, VAC>(a, t, s);
     case MODE_S4: return launch_t<T, R, MODE_S4, TZ, VAC>(a, t, s);
     default: return cudaErrorInvalidValue;
     }
@@ -785,9 +790,11 @@ template <typename T, template <typename, int, int, int, bool> class F, typename
 auto batch_dispatch(int mode, bool ko6, int tz, bool vac, Args... args) {
 #define NUOSC_BATCH_V(R, M, Z) (vac ? F<T, R, M, Z, true>::run(args...) : F<T, R, M, Z, false>::run(args...))
 #define NUOSC_BATCH_TZ(R, M) (tz == 16 ? NUOSC_BATCH_V(R, M, 16) : NUOSC_BATCH_V(R, M, 8))
-#define NUOSC_BATCH_MODE(R)                                                   \
-    (mode == MODE_S1 ? NUOSC_BATCH_TZ(R, MODE_S1)                             \
-                     : mode == MODE_S23 ? NUOSC_BATCH_TZ(R, MODE_S23) : NUOSC_BATCH_TZ(R, MODE_S4))
+#define NUOSC_BATCH_MODE(R)                                                                                   \
+    (mode == MODE_S1    ? NUOSC_BATCH_TZ(R, MODE_S1)                                                          \
+     : mode == MODE_S2  ? NUOSC_BATCH_TZ(R, MODE_S2)                                                          \
+     : mode == MODE_S23 ? NUOSC_BATCH_TZ(R, MODE_S23)                                                         \
+                        : NUOSC_BATCH_TZ(R, MODE_S4))
     return ko6 ? NUOSC_BATCH_MODE(3) : NUOSC_BATCH_MODE(2);
 #undef NUOSC_BATCH_MODE
 #undef NUOSC_BATCH_TZ
@@ -838,7 +845,8 @@ long long xtma_batch_fill(void *item, const StageArgs<T> &a, bool ko6, int tz, i
 
 template <typename T>
 int xtma_batch_grid(int mode, bool ko6, int tz, bool vac, int device) {
-    if ((tz != 8 && tz != 16) || (mode != MODE_S1 && mode != MODE_S23 && mode != MODE_S4)) return -1;
+    if ((tz != 8 && tz != 16) || (mode != MODE_S1 && mode != MODE_S2 && mode != MODE_S23 && mode != MODE_S4))
+        return -1;
     return batch_dispatch<T, BatchGrid>(mode, ko6, tz, vac, device);
 }
 
@@ -846,7 +854,8 @@ template <typename T>
 cudaError_t launch_stage_xtma_batch(const void *items, const long long *starts, int n, long long ntiles,
                                     unsigned long long *counter, int mode, bool ko6, int tz, bool vac, int grid,
                                     cudaStream_t s) {
-    if ((tz != 8 && tz != 16) || (mode != MODE_S1 && mode != MODE_S23 && mode != MODE_S4) || n < 1 || grid < 1)
+    if ((tz != 8 && tz != 16) || (mode != MODE_S1 && mode != MODE_S2 && mode != MODE_S23 && mode != MODE_S4) ||
+        n < 1 || grid < 1)
         return cudaErrorInvalidValue;
     return batch_dispatch<T, BatchLaunch>(mode, ko6, tz, vac, items, starts, n, ntiles, counter, grid, s);
 }
