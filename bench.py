@@ -43,8 +43,8 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "cell-steps/s"
-BYTES_PER_CELL_STEP = {"f64": 960, "f32": 480}  # 15 state passes x 8 fields x sizeof(real)
-STAGE_S23_PASSES = 4.5  # S2 reads A and Ya, writes A and Yb (4); S3 also reads U (5)
+BYTES_PER_CELL_STEP = {"f64": 896, "f32": 448}  # 14 state passes x 8 fields x sizeof(real)
+STAGE_S23_PASSES = 4.5  # S2 reads U and Ya, writes A and Yb (4); S3 also reads A (5)
 
 
 def workload(size, nn, precision):

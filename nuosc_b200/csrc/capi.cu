@@ -10,9 +10,11 @@
 //   S4: k4 = L(Ya) ; U = A + dt/6 k4
 // which is U + dt/6 (k1 + 2k2 + 2k3 + k4), the reference's update, with
 // 16 state passes per step instead of the reference's 4 calRHS + 6 vectorize.
-// On the TMA path S2 takes U as 1.5 A - 0.5 Ya (both already in hand: A is
-// read for the update, Ya is the stencil input) instead of reading it: 15
-// passes per step.
+// On the TMA path S1 stores only Ya, and S2 forms A1 = U + dt/6 k1 as
+// U + (Ya - U)/3 from the U it reads and its stencil input Ya:
+//   S1: Ya = U + dt/2 k1                                     2 passes
+//   S2: A = U + (Ya - U)/3 + dt/3 k2 ; Yb = U + dt/2 k2     4
+// 14 state passes per step.
 #include "../../include/nuosc_b200.h"
 #include "internal.cuh"
 
@@ -206,6 +208,7 @@ int ensure(void **p, size_t *cap, size_t bytes, nuosc_handle *h) {
 int prof_kind(int mode) {
     switch (mode) {
     case MODE_S1: return 0;
+    case MODE_S1Y: return 0;
     case MODE_S23: return 1;
     case MODE_S2: return 1;
     case MODE_S4: return 2;
@@ -251,7 +254,7 @@ int run_stage_xmarch(nuosc_handle *h, bool tma, const XTile &tile, int mode, int
     a.in = (const T *)h->reg[in];
     a.u = u >= 0 ? (const T *)h->reg[u] : nullptr;
     a.acc_src = acc_src >= 0 ? (const T *)h->reg[acc_src] : nullptr;
-    a.acc_dst = (T *)h->reg[acc_dst];
+    a.acc_dst = acc_dst >= 0 ? (T *)h->reg[acc_dst] : nullptr;
     a.y_dst = y_dst >= 0 ? (T *)h->reg[y_dst] : nullptr;
     a.mom_in = h->d_mom;
     a.mom_part = h->d_part;
@@ -325,11 +328,14 @@ int step_impl(nuosc_handle *h, int nsteps) {
     for (int n = 0; n < nsteps; ++n) {
         int rc;
         if (xm) {
-            if ((rc = run_stage_xmarch<T>(h, tma, tile, MODE_S1, 0, -1, -1, 1, 2, dt / 6.0, 0.5 * dt))) return rc;
-            // S2 on the TMA path does not read U (MODE_S2)
-            if ((rc = run_stage_xmarch<T>(h, tma, tile, tma ? MODE_S2 : MODE_S23, 2, tma ? -1 : 0, 1, 1, 3, dt / 3.0,
+            if ((rc = run_stage_xmarch<T>(h, tma, tile, tma ? MODE_S1Y : MODE_S1, 0, -1, -1, tma ? -1 : 1, 2, dt / 6.0,
                                           0.5 * dt)))
                 return rc;
+            if (tma) {  // 14-pass sequence: S1 stores only Ya, S2 forms A1 from U and Ya
+                if ((rc = run_stage_xmarch<T>(h, tma, tile, MODE_S2, 2, 0, -1, 1, 3, dt / 3.0, 0.5 * dt))) return rc;
+            } else {
+                if ((rc = run_stage_xmarch<T>(h, tma, tile, MODE_S23, 2, 0, 1, 1, 3, dt / 3.0, 0.5 * dt))) return rc;
+            }
             if ((rc = run_stage_xmarch<T>(h, tma, tile, MODE_S23, 3, 0, 1, 1, 2, dt / 3.0, dt))) return rc;
             if ((rc = run_stage_xmarch<T>(h, tma, tile, MODE_S4, 2, -1, 1, 0, -1, dt / 6.0, 0.0))) return rc;
         } else {
@@ -1026,8 +1032,8 @@ struct StageSpec {
     int mode, in, u, acc_src, acc_dst, y_dst;
     double da, fy;
 };
-constexpr StageSpec kStages[4] = {{MODE_S1, 0, -1, -1, 1, 2, 6.0, 0.5},
-                                  {MODE_S2, 2, -1, 1, 1, 3, 3.0, 0.5},
+constexpr StageSpec kStages[4] = {{MODE_S1Y, 0, -1, -1, -1, 2, 6.0, 0.5},
+                                  {MODE_S2, 2, 0, -1, 1, 3, 3.0, 0.5},
                                   {MODE_S23, 3, 0, 1, 1, 2, 3.0, 1.0},
                                   {MODE_S4, 2, -1, 1, 0, -1, 6.0, 0.0}};
 
@@ -1084,7 +1090,7 @@ int batch_build(nuosc_batch *b) {
             a.in = (const T *)h->reg[sp.in];
             a.u = sp.u >= 0 ? (const T *)h->reg[sp.u] : nullptr;
             a.acc_src = sp.acc_src >= 0 ? (const T *)h->reg[sp.acc_src] : nullptr;
-            a.acc_dst = (T *)h->reg[sp.acc_dst];
+            a.acc_dst = sp.acc_dst >= 0 ? (T *)h->reg[sp.acc_dst] : nullptr;
             a.y_dst = sp.y_dst >= 0 ? (T *)h->reg[sp.y_dst] : nullptr;
             a.mom_in = h->d_mom;
             a.mom_part = h->d_part;

@@ -44,11 +44,11 @@ struct Quad {
 //   MODE_S1  : acc_dst = in + cA*k ;          y_dst = in + cY*k
 //   MODE_S23 : acc_dst = acc_src + cA*k ;     y_dst = u  + cY*k
 //   MODE_S4  : acc_dst = acc_src + cA*k
-//   MODE_S2  : acc_dst = acc_src + cA*k ;     y_dst = (1.5 acc_src - 0.5 in) + cY*k
-// MODE_S2 is the second RK4 stage without reading U: there acc_src = A1 =
-// U + dt/6 k1 and in = Y2 = U + dt/2 k1, so 1.5 A1 - 0.5 Y2 = U up to
-// rounding (one state pass fewer per step; the TMA path uses it).
-enum StageMode { MODE_RHS = 0, MODE_S1 = 1, MODE_S23 = 2, MODE_S4 = 3, MODE_S2 = 4 };
+// and the 14-pass sequence of the TMA path, which never stores A1:
+//   MODE_S1Y : y_dst = in + cY*k                       (Y2 = U + dt/2 k1)
+//   MODE_S2  : acc_dst = (u + (in - u)/3) + cA*k ;    y_dst = u + cY*k
+// In S2, in = Y2 = U + dt/2 k1, so u + (in - u)/3 = U + dt/6 k1 = A1.
+enum StageMode { MODE_RHS = 0, MODE_S1 = 1, MODE_S23 = 2, MODE_S4 = 3, MODE_S2 = 4, MODE_S1Y = 5 };
 
 template <typename T>
 struct StageArgs {

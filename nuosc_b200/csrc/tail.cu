@@ -69,8 +69,7 @@ __device__ __forceinline__ void tail_point(const StageArgs<T> &a, const long lon
 #pragma unroll
         for (int f = 0; f < 4; ++f) {
             const long long idx = o + f * g.fs;
-            if (MODE == MODE_S1) {
-                a.acc_dst[idx] = c4[f] + cA * kv[f];
+            if (MODE == MODE_S1Y) {
                 outm[f] = c4[f] + cY * kv[f];
                 a.y_dst[idx] = outm[f];
             } else if (MODE == MODE_S23) {
@@ -78,8 +77,8 @@ __device__ __forceinline__ void tail_point(const StageArgs<T> &a, const long lon
                 outm[f] = a.u[idx] + cY * kv[f];
                 a.y_dst[idx] = outm[f];
             } else if (MODE == MODE_S2) {
-                const T a1 = a.acc_src[idx];
-                const T u = fma(T(1.5), a1, T(-0.5) * c4[f]);  // U = 1.5 A1 - 0.5 Y2
+                const T u = a.u[idx];
+                const T a1 = u + (c4[f] - u) * T(1.0 / 3.0);  // A1 = U + dt/6 k1 from Y2 = U + dt/2 k1
                 a.acc_dst[idx] = a1 + cA * kv[f];
                 outm[f] = u + cY * kv[f];
                 a.y_dst[idx] = outm[f];
@@ -150,7 +149,7 @@ cudaError_t launch_tail_ko(const StageArgs<T> &a, int mode, int v0, int twp, int
     const long long threads = a.g.ncell * 2 * twp;
     const unsigned blocks = (unsigned)((threads + TAIL_BLOCK - 1) / TAIL_BLOCK);
     switch (mode) {
-    case MODE_S1: k_stage_tail<T, KO6, MODE_S1><<<blocks, TAIL_BLOCK, 0, s>>>(a, v0, twp, nvb); break;
+    case MODE_S1Y: k_stage_tail<T, KO6, MODE_S1Y><<<blocks, TAIL_BLOCK, 0, s>>>(a, v0, twp, nvb); break;
     case MODE_S23: k_stage_tail<T, KO6, MODE_S23><<<blocks, TAIL_BLOCK, 0, s>>>(a, v0, twp, nvb); break;
     case MODE_S2: k_stage_tail<T, KO6, MODE_S2><<<blocks, TAIL_BLOCK, 0, s>>>(a, v0, twp, nvb); break;
     case MODE_S4: k_stage_tail<T, KO6, MODE_S4><<<blocks, TAIL_BLOCK, 0, s>>>(a, v0, twp, nvb); break;
@@ -164,7 +163,7 @@ cudaError_t launch_tail_batch_ko(const TailItem<T> *items, const long long *star
                                  cudaStream_t s) {
     const unsigned blocks = (unsigned)((total + TAIL_BLOCK - 1) / TAIL_BLOCK);
     switch (mode) {
-    case MODE_S1: k_stage_tail_batch<T, KO6, MODE_S1><<<blocks, TAIL_BLOCK, 0, s>>>(items, starts, n, total); break;
+    case MODE_S1Y: k_stage_tail_batch<T, KO6, MODE_S1Y><<<blocks, TAIL_BLOCK, 0, s>>>(items, starts, n, total); break;
     case MODE_S23: k_stage_tail_batch<T, KO6, MODE_S23><<<blocks, TAIL_BLOCK, 0, s>>>(items, starts, n, total); break;
     case MODE_S2: k_stage_tail_batch<T, KO6, MODE_S2><<<blocks, TAIL_BLOCK, 0, s>>>(items, starts, n, total); break;
     case MODE_S4: k_stage_tail_batch<T, KO6, MODE_S4><<<blocks, TAIL_BLOCK, 0, s>>>(items, starts, n, total); break;

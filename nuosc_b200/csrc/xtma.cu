@@ -401,15 +401,17 @@ __device__ __forceinline__ bool xtma_march(const TmaMaps *const &mp, const Stage
         prefetch(i + 1);
         {
             // pointwise epilogue inputs first (they are not in the ring)
-            const T *up = MODE == MODE_S23 ? rd<SA>(a.u) + oc : nullptr;
-            const T *ap = MODE != MODE_S1 && !CF::PF ? rd<SA>(a.acc_src) + oc : nullptr;
+            constexpr bool LU = MODE == MODE_S23 || MODE == MODE_S2;           // reads U
+            constexpr bool LA = (MODE == MODE_S23 || MODE == MODE_S4) && !CF::PF;  // reads A here
+            const T *up = LU ? rd<SA>(a.u) + oc : nullptr;
+            const T *ap = LA ? rd<SA>(a.acc_src) + oc : nullptr;
 #pragma unroll
             for (int f = 0; f < 4; ++f) {
 #pragma unroll
                 for (int p = 0; p < NP; ++p) uin[f][p] = ain[f][p] = T(0);
                 if (vact) {
-                    if (MODE == MODE_S23) ldv<T, NP>(up + f * fs, uin[f]);
-                    if (MODE != MODE_S1 && !CF::PF) ldv<T, NP>(ap + f * fs, ain[f]);
+                    if (LU) ldv<T, NP>(up + f * fs, uin[f]);
+                    if (LA) ldv<T, NP>(ap + f * fs, ain[f]);
                 }
             }
         }
@@ -488,15 +490,15 @@ __device__ __forceinline__ bool xtma_march(const TmaMaps *const &mp, const Stage
             const T cA = K(a.cA, cA0), cY = K(a.cY, cY0);
 #pragma unroll
             for (int f = 0; f < 4; ++f) {
-                if (MODE == MODE_S1) {
-                    uin[f][p] = cen[f] + cA * kk[f];  // A
-                    outm[f][p] = cen[f] + cY * kk[f];  // Y
+                if (MODE == MODE_S1Y) {
+                    outm[f][p] = cen[f] + cY * kk[f];  // Y2
                 } else if (MODE == MODE_S23) {
                     ain[f][p] = ain[f][p] + cA * kk[f];
                     outm[f][p] = uin[f][p] + cY * kk[f];
                 } else if (MODE == MODE_S2) {
-                    const T u = fma(T(1.5), ain[f][p], T(-0.5) * cen[f]);  // U = 1.5 A1 - 0.5 Y2
-                    ain[f][p] = ain[f][p] + cA * kk[f];
+                    const T u = uin[f][p];
+                    const T a1 = u + (cen[f] - u) * T(1.0 / 3.0);  // A1 = U + dt/6 k1 from Y2 = U + dt/2 k1
+                    ain[f][p] = a1 + cA * kk[f];
                     outm[f][p] = u + cY * kk[f];
                 } else {
                     outm[f][p] = ain[f][p] + cA * kk[f];
@@ -504,12 +506,11 @@ __device__ __forceinline__ bool xtma_march(const TmaMaps *const &mp, const Stage
             }
         }
         if (vact) {
-            T *dp = rd<SA>(a.acc_dst) + oc;
+            T *dp = MODE != MODE_S1Y ? rd<SA>(a.acc_dst) + oc : nullptr;
             T *yp = MODE != MODE_S4 ? rd<SA>(a.y_dst) + oc : nullptr;
 #pragma unroll
             for (int f = 0; f < 4; ++f) {
-                if (MODE == MODE_S1) {
-                    stv<T, NP>(dp + f * fs, uin[f]);
+                if (MODE == MODE_S1Y) {
                     stv<T, NP>(yp + f * fs, outm[f]);
                 } else if (MODE == MODE_S23 || MODE == MODE_S2) {
                     stv<T, NP>(dp + f * fs, ain[f]);
@@ -746,7 +747,7 @@ cudaError_t launch_t(const StageArgs<T> &a, XTile t, cudaStream_t s) {
 template <typename T, int R, int TZ, bool VAC>
 cudaError_t launch_tm(const StageArgs<T> &a, int mode, XTile t, cudaStream_t s) {
     switch (mode) {
-    case MODE_S1: return launch_t<T, R, MODE_S1, TZ, VAC>(a, t, s);
+    case MODE_S1Y: return launch_t<T, R, MODE_S1Y, TZ, VAC>(a, t, s);
     case MODE_S23: return launch_t<T, R, MODE_S23, TZ, VAC>(a, t, s);
     case MODE_S2: return launch_t<T, R, MODE_S2, TZ, VAC>(a, t, s);
     case MODE_S4: return launch_t<T, R, MODE_S4, TZ, VAC>(a, t, s);
@@ -791,7 +792,7 @@ auto batch_dispatch(int mode, bool ko6, int tz, bool vac, Args... args) {
 #define NUOSC_BATCH_V(R, M, Z) (vac ? F<T, R, M, Z, true>::run(args...) : F<T, R, M, Z, false>::run(args...))
 #define NUOSC_BATCH_TZ(R, M) (tz == 16 ? NUOSC_BATCH_V(R, M, 16) : NUOSC_BATCH_V(R, M, 8))
 #define NUOSC_BATCH_MODE(R)                                                                                   \
-    (mode == MODE_S1    ? NUOSC_BATCH_TZ(R, MODE_S1)                                                          \
+    (mode == MODE_S1Y   ? NUOSC_BATCH_TZ(R, MODE_S1Y)                                                         \
      : mode == MODE_S2  ? NUOSC_BATCH_TZ(R, MODE_S2)                                                          \
      : mode == MODE_S23 ? NUOSC_BATCH_TZ(R, MODE_S23)                                                         \
                         : NUOSC_BATCH_TZ(R, MODE_S4))
@@ -845,7 +846,7 @@ long long xtma_batch_fill(void *item, const StageArgs<T> &a, bool ko6, int tz, i
 
 template <typename T>
 int xtma_batch_grid(int mode, bool ko6, int tz, bool vac, int device) {
-    if ((tz != 8 && tz != 16) || (mode != MODE_S1 && mode != MODE_S2 && mode != MODE_S23 && mode != MODE_S4))
+    if ((tz != 8 && tz != 16) || (mode != MODE_S1Y && mode != MODE_S2 && mode != MODE_S23 && mode != MODE_S4))
         return -1;
     return batch_dispatch<T, BatchGrid>(mode, ko6, tz, vac, device);
 }
@@ -854,7 +855,7 @@ template <typename T>
 cudaError_t launch_stage_xtma_batch(const void *items, const long long *starts, int n, long long ntiles,
                                     unsigned long long *counter, int mode, bool ko6, int tz, bool vac, int grid,
                                     cudaStream_t s) {
-    if ((tz != 8 && tz != 16) || (mode != MODE_S1 && mode != MODE_S2 && mode != MODE_S23 && mode != MODE_S4) ||
+    if ((tz != 8 && tz != 16) || (mode != MODE_S1Y && mode != MODE_S2 && mode != MODE_S23 && mode != MODE_S4) ||
         n < 1 || grid < 1)
         return cudaErrorInvalidValue;
     return batch_dispatch<T, BatchLaunch>(mode, ko6, tz, vac, items, starts, n, ntiles, counter, grid, s);
