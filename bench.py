@@ -136,7 +136,9 @@ def traffic_per_launch(kernel_key):
         return None
 
 
-def dist_setup(args):
+def dist_setup(args=None, backend=None):
+    """One process per GPU from the torchrun environment (RANK, LOCAL_RANK,
+    WORLD_SIZE, MASTER_*): NCCL when CUDA is present, else gloo (CPU tests)."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -145,8 +147,10 @@ def dist_setup(args):
         import torch
         import torch.distributed as dist
         os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        backend = backend or ("nccl" if torch.cuda.is_available() else "gloo")
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
     return world, rank, local
 
 
@@ -155,9 +159,15 @@ def max_over_ranks(x, world):
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([float(x)], device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(x)], device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def replica_value(cells_per_rank, steps, max_ms, world):
+    """Whole-job cell-steps/s of N replicas: all ranks' cell-steps / the slowest rank's time."""
+    return world * cells_per_rank * steps / (max_ms / 1e3)
 
 
 def barrier(world):
@@ -273,7 +283,7 @@ def bench_ours(args, world, rank, local):
     s.set_profiling(False)
     ms = max_over_ranks(e0.elapsed_time(e1), world)
     ms_per_step = ms / args.steps
-    value = world * cells * args.steps / (ms / 1e3)
+    value = replica_value(cells, args.steps, ms, world)
     diag = s.analysis()
 
     # dominant kernel: the S2/S3 stage kernel (two of four stages, five state passes)
