@@ -440,32 +440,41 @@ def bench_batch(args, local, single):
 
 
 def bench_serving(args, local, single):
-    """A bounded serving run: Poisson arrivals of mixed requests (70% FP32),
-    admitted under a 150 GB budget, continuous batching; aggregate
-    cell-steps/s, its ratio to the single large solves doing the same
-    cell-steps, p50/p99 completion latency, and the same arrivals served one
-    at a time on the plain FP64 path."""
+    """Two bounded serving runs of mixed requests (70% FP32) under a 150 GB
+    budget with continuous batching: all requests at once (throughput: its
+    ratio to the single large solves doing the same cell-steps) and Poisson
+    arrivals (p50/p99 completion latency, beside the same arrivals served one
+    at a time on the plain FP64 path)."""
     from nuosc_b200 import serve
-    reqs = serve.draw_requests(args.serve_requests, args.serve_rate, 7, steps=(args.serve_min_steps,
-                                                                               args.serve_max_steps))
-    rep = serve.Server(budget_bytes=150e9, device=local).run(reqs)
-    cs64 = sum(r.cell_steps for r in reqs if r.precision == 0)
-    cs32 = sum(r.cell_steps for r in reqs if r.precision == 1)
-    ref = (cs64 + cs32) / (cs64 / single["f64"] + cs32 / single["f32"])
+
+    def ref_rate(reqs):
+        cs64 = sum(r.cell_steps for r in reqs if r.precision == 0)
+        cs32 = sum(r.cell_steps for r in reqs if r.precision == 1)
+        return (cs64 + cs32) / (cs64 / single["f64"] + cs32 / single["f32"])
+
+    steps = (args.serve_min_steps, args.serve_max_steps)
+    sat = serve.draw_requests(args.serve_requests, 0.0, 7, steps=steps)
+    rs = serve.Server(budget_bytes=150e9, device=local).run(sat)
+    reqs = serve.draw_requests(args.serve_requests, args.serve_rate, 7, steps=steps)
+    rp = serve.Server(budget_bytes=150e9, device=local).run(reqs)
     t = serve.solo_fp64_step_times(reqs, device=local)
     one = serve.fifo_one_at_a_time(reqs, {r.rid: t[(r.nx, r.nz, r.nn)] * r.steps for r in reqs})
-    return {"requests": len(reqs), "rate_per_s": args.serve_rate,
-            "steps_range": [args.serve_min_steps, args.serve_max_steps], "budget_gb": 150,
-            "cell_steps_per_s": rep["cell_steps_per_s"], "cell_steps_per_busy_s": rep["cell_steps_per_busy_s"],
-            "busy_vs_single_large_solve": rep["cell_steps_per_busy_s"] / ref,
-            "latency_p50_s": rep["latency_p50_s"], "latency_p99_s": rep["latency_p99_s"],
-            "makespan_s": rep["makespan_s"], "peak_resident": rep["peak_resident"], "quanta": rep["quanta"],
-            "diverged": rep["diverged"],
-            "one_at_a_time_fp64": {k: one[k] for k in ("cell_steps_per_s", "latency_p50_s", "latency_p99_s",
-                                                       "makespan_s")},
+    return {"requests": len(reqs), "steps_range": list(steps), "budget_gb": 150,
+            "saturated": {"cell_steps_per_s": rs["cell_steps_per_s"],
+                          "vs_single_large_solve": rs["cell_steps_per_s"] / ref_rate(sat),
+                          "makespan_s": rs["makespan_s"], "peak_resident": rs["peak_resident"],
+                          "latency_p50_s": rs["latency_p50_s"], "latency_p99_s": rs["latency_p99_s"]},
+            "poisson": {"rate_per_s": args.serve_rate, "cell_steps_per_s": rp["cell_steps_per_s"],
+                        "cell_steps_per_busy_s": rp["cell_steps_per_busy_s"],
+                        "latency_p50_s": rp["latency_p50_s"], "latency_p99_s": rp["latency_p99_s"],
+                        "makespan_s": rp["makespan_s"], "peak_resident": rp["peak_resident"],
+                        "one_at_a_time_fp64": {k: one[k] for k in ("cell_steps_per_s", "latency_p50_s",
+                                                                   "latency_p99_s", "makespan_s")}},
+            "diverged": rp["diverged"],
             "note": "single-large-solve reference = the 1024x1024x642 FP64/FP32 solves timed above, weighted by "
                     "the requests' FP64/FP32 cell-steps; one-at-a-time latencies from measured per-shape FP64 step "
-                    "times; requests whose state blew up keep stepping (same cost) and are counted in 'diverged'"}
+                    "times; requests whose state blew up keep stepping (same cost) and are counted in 'diverged'; "
+                    "the 512-request run is in profiles/serving_512_requests.md"}
 
 
 def main():
