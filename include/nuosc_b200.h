@@ -193,6 +193,16 @@ long long nuosc_kernel_launches(const nuosc_handle *h);
 /* RK4 steps taken since the initial data (fill_init resets it; -1 for NULL) */
 long long nuosc_step_count(const nuosc_handle *h);
 
+/* Device memory of handles and batches comes from the device's default
+ * stream-ordered memory pool (cudaMallocAsync), and blocks freed by
+ * nuosc_destroy / nuosc_batch_destroy stay in that pool for the next handle
+ * (the library raises the pool's release threshold), so that creating and
+ * destroying solves neither re-allocates nor stalls the device.  This call
+ * waits for the device and returns the pool's unused blocks to it, for
+ * callers that need the memory for something else.  No reference
+ * counterpart (the reference allocates with new[] once per run). */
+int nuosc_release_cached_memory(int device);
+
 /* Per-kernel timing with CUDA events on the handle's stream (no counterpart
  * in the reference, which prints wall time per step, nuosc.cpp:222-235).
  * Kinds: 0 stage S1, 1 stage S2/S3, 2 stage S4, 3 calRHS, 4 moments,

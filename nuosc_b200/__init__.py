@@ -24,7 +24,12 @@ from . import _lib
 from ._lib import (FP32, FP64, KERNEL_AUTO, KERNEL_DIRECT, KERNEL_XMARCH, KERNEL_XTMA, LAYOUT_COMPACT,
                    LAYOUT_GHOSTED, REG_COR, REG_PRE, REG_RHS, REG_STAT, FIELDS, NuoscError, check, lib)
 
-__all__ = ["NuOsc", "Batch", "NuoscError", "FP32", "FP64", "REG_STAT", "REG_RHS", "REG_PRE", "REG_COR",
+def release_cached_memory(device=0):
+    """Return the device memory that destroyed handles left in the pool."""
+    check(lib().nuosc_release_cached_memory(int(device)))
+
+
+__all__ = ["NuOsc", "Batch", "release_cached_memory", "NuoscError", "FP32", "FP64", "REG_STAT", "REG_RHS", "REG_PRE", "REG_COR",
            "KERNEL_AUTO", "KERNEL_DIRECT", "KERNEL_XMARCH", "KERNEL_XTMA", "FIELDS", "lib"]
 
 lib()  # fail at import time if the CUDA library is missing
@@ -311,6 +316,7 @@ class Batch:
         self.members = list(members)
         hs = (C.c_void_p * len(self.members))(*[m.handle for m in self.members])
         b = C.c_void_p()
+        self._rec = None
         check(lib().nuosc_batch_create(hs, len(self.members), C.byref(b)))
         self._b = b
 
@@ -318,6 +324,9 @@ class Batch:
         if getattr(self, "_b", None):
             lib().nuosc_batch_destroy(self._b)
             self._b = None
+        if getattr(self, "_rec", None) is not None:
+            self._rec.free()
+            self._rec = None
 
     def __del__(self):
         try:
@@ -341,9 +350,15 @@ class Batch:
     def step_stream(self, nsteps, every):
         """nsteps steps; the analysis of each member is queued on the device
         whenever its step count reaches a multiple of `every`.  Returns a
-        handle for collect(), valid after synchronize()."""
-        nmax = len(self.members) * (int(nsteps) // max(1, int(every)) + 1)
-        buf = _PinnedRecords(max(1, nmax))
+        handle for collect(), valid after synchronize(); the record buffer is
+        the batch's own and is reused by the next step_stream, so collect the
+        records first."""
+        nmax = max(1, len(self.members) * (int(nsteps) // max(1, int(every)) + 1))
+        if self._rec is None or self._rec.n < nmax:
+            if self._rec is not None:
+                self._rec.free()
+            self._rec = _PinnedRecords(max(nmax, 2 * len(self.members)))
+        buf = self._rec
         n = C.c_int()
         check(lib().nuosc_batch_step_stream(self._b, int(nsteps), int(every), buf.ptr, buf.n, C.byref(n)))
         buf.used = n.value
@@ -360,7 +375,7 @@ class Batch:
             if rc not in (_lib.OK, _lib.ERR_NUMERIC):
                 check(rc)
             out.append((r.member, r.step, d.as_dict() if rc == _lib.OK else None))
-        records.free()
+        records.used = 0
         return out
 
     def synchronize(self):

@@ -109,6 +109,7 @@ _SIGS = {
     "nuosc_batch_destroy": [_P],
     "nuosc_batch_step_stream": [_P, _I, _I, _P, _I, _IP],
     "nuosc_batch_record_diag": [_P, C.POINTER(BatchRecord), C.POINTER(Diag)],
+    "nuosc_release_cached_memory": [_I],
 }
 PROF_KINDS = ["stage_s1", "stage_s23", "stage_s4", "calrhs", "moments", "moment_finalize"]
 

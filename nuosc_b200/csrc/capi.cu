@@ -27,6 +27,7 @@
 #include <fstream>
 #include <iomanip>
 #include <list>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -103,7 +104,7 @@ struct nuosc_handle {
     double *d_part = nullptr;  // x-march partial moments
     size_t part_bytes = 0;
     double *d_ana = nullptr;   // analysis partials + final
-    double *h_ana = nullptr;   // pinned
+    double h_ana[ANA_NQ] = {0};  // analysis read-back
     int *d_status = nullptr;
     double *d_stage = nullptr; // host-layout staging
     size_t stage_bytes = 0;
@@ -191,15 +192,61 @@ namespace {
 
 bool valid_reg(int r) { return r >= 0 && r < 4; }
 
+// Device memory of handles and batches comes from the device's default
+// stream-ordered pool (cudaMallocAsync), whose release threshold is raised
+// once per device so that freed blocks stay in the pool for the next handle:
+// a server that creates and destroys solves all the time then neither pays
+// for cudaMalloc nor stalls the device in cudaFree.  nuosc_release_cached_memory
+// returns the pool's unused blocks to the device.
+cudaMemPool_t device_pool(int device) {
+    static std::mutex mu;
+    static std::vector<int> done;
+    cudaMemPool_t pool = nullptr;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) != cudaSuccess) return nullptr;
+    std::lock_guard<std::mutex> lock(mu);
+    if (std::find(done.begin(), done.end(), device) == done.end()) {
+        uint64_t keep = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        done.push_back(device);
+    }
+    return pool;
+}
+
+// bytes the device can still give: free memory plus the pool's unused blocks
+size_t device_available(int device) {
+    size_t free_b = 0, total_b = 0;
+    cudaMemGetInfo(&free_b, &total_b);
+    if (cudaMemPool_t pool = device_pool(device)) {
+        uint64_t reserved = 0, used = 0;
+        cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved);
+        cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used);
+        if (reserved > used) free_b += (size_t)(reserved - used);
+    }
+    return free_b;
+}
+
+// pool allocation, complete (usable from any stream) on return
+cudaError_t dev_alloc(void **p, size_t bytes, int device, cudaStream_t s) {
+    device_pool(device);
+    cudaError_t e = cudaMallocAsync(p, bytes, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    return e;
+}
+
+// back to the pool once the work queued on s is done
+void dev_free(void *p, cudaStream_t s) {
+    if (p) cudaFreeAsync(p, s);
+}
+
 int ensure(void **p, size_t *cap, size_t bytes, nuosc_handle *h) {
     if (*cap >= bytes) return 0;
     if (*p) {
-        cudaFree(*p);
+        dev_free(*p, h->stream);
         h->device_bytes -= *cap;
     }
     *p = nullptr;
     *cap = 0;
-    CUDA_TRY(cudaMalloc(p, bytes));
+    CUDA_TRY(dev_alloc(p, bytes, h->device, h->stream));
     *cap = bytes;
     h->device_bytes += bytes;
     return 0;
@@ -630,14 +677,13 @@ int nuosc_create(const nuosc_params *p, nuosc_handle **out) {
     e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) return bail(fail(NUOSC_ERR_CUDA, "cudaStreamCreate: %s", cudaGetErrorString(e)));
     const size_t reg_bytes = (size_t)h->g.fs * NF * h->esize;
-    size_t free_b = 0, total_b = 0;
-    cudaMemGetInfo(&free_b, &total_b);
+    const size_t free_b = device_available(h->device);
     const size_t need = 4 * reg_bytes + (size_t)h->g.ncell * NMOM * 8;
     if (need > free_b)
         return bail(fail(NUOSC_ERR_OOM, "need %.2f GB for 4 state registers, %.2f GB free", need / 1e9, free_b / 1e9));
     for (int r = 0; r < 4; ++r) {
-        e = cudaMalloc(&h->reg[r], reg_bytes);
-        if (e != cudaSuccess) return bail(fail(NUOSC_ERR_OOM, "cudaMalloc register %d (%.2f GB): %s", r, reg_bytes / 1e9,
+        e = dev_alloc(&h->reg[r], reg_bytes, h->device, h->stream);
+        if (e != cudaSuccess) return bail(fail(NUOSC_ERR_OOM, "allocating register %d (%.2f GB): %s", r, reg_bytes / 1e9,
                                                cudaGetErrorString(e)));
         h->device_bytes += reg_bytes;
         cudaMemsetAsync(h->reg[r], 0, reg_bytes, h->stream);
@@ -645,16 +691,14 @@ int nuosc_create(const nuosc_params *p, nuosc_handle **out) {
     const size_t small = 6 * (size_t)nvs * sizeof(double) + (size_t)h->g.ncell * NMOM * sizeof(double) +
                          (ANA_BLOCKS + 1) * ANA_NQ * sizeof(double) + 256;
     char *blk = nullptr;
-    e = cudaMalloc(&blk, small);
-    if (e != cudaSuccess) return bail(fail(NUOSC_ERR_OOM, "cudaMalloc work buffers: %s", cudaGetErrorString(e)));
+    e = dev_alloc((void **)&blk, small, h->device, h->stream);
+    if (e != cudaSuccess) return bail(fail(NUOSC_ERR_OOM, "allocating work buffers: %s", cudaGetErrorString(e)));
     h->device_bytes += small;
     cudaMemsetAsync(blk, 0, small, h->stream);
     h->d_status = (int *)blk;
     h->d_quad = (double *)(blk + 256);
     h->d_mom = h->d_quad + 6 * nvs;
     h->d_ana = h->d_mom + h->g.ncell * NMOM;
-    e = cudaMallocHost(&h->h_ana, ANA_NQ * sizeof(double));
-    if (e != cudaSuccess) return bail(fail(NUOSC_ERR_CUDA, "cudaMallocHost: %s", cudaGetErrorString(e)));
     cudaMemcpyAsync(h->d_quad, h->vx.data(), nv * 8, cudaMemcpyHostToDevice, h->stream);
     cudaMemcpyAsync(h->d_quad + nvs, h->vy.data(), nv * 8, cudaMemcpyHostToDevice, h->stream);
     cudaMemcpyAsync(h->d_quad + 2 * nvs, h->vz.data(), nv * 8, cudaMemcpyHostToDevice, h->stream);
@@ -674,15 +718,15 @@ int nuosc_destroy(nuosc_handle *h) {
     if (h->stream) cudaStreamSynchronize(h->stream);
     h->prof_collect();
     for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
-    for (int r = 0; r < 4; ++r)
-        if (h->reg[r]) cudaFree(h->reg[r]);
-    if (h->d_status) cudaFree(h->d_status);
-    if (h->d_part) cudaFree(h->d_part);
-    if (h->d_stage) cudaFree(h->d_stage);
-    if (h->d_idx) cudaFree(h->d_idx);
-    if (h->d_gather) cudaFree(h->d_gather);
-    if (h->h_ana) cudaFreeHost(h->h_ana);
-    if (h->stream) cudaStreamDestroy(h->stream);
+    if (h->stream) {  // (no stream: nothing was allocated)
+        for (int r = 0; r < 4; ++r) dev_free(h->reg[r], h->stream);
+        dev_free(h->d_status, h->stream);
+        dev_free(h->d_part, h->stream);
+        dev_free(h->d_stage, h->stream);
+        dev_free(h->d_idx, h->stream);
+        dev_free(h->d_gather, h->stream);
+        cudaStreamDestroy(h->stream);
+    }
     if (h->anafile.is_open()) h->anafile.close();
     delete h;
     return NUOSC_OK;
@@ -1067,6 +1111,35 @@ int batch_build(nuosc_batch *b) {
         const size_t need = (size_t)h->g.ncell * xmarch_num_vblocks(h->g, h->tile) * 2 * NMOM * sizeof(double);
         if (int rc = ensure((void **)&h->d_part, &h->part_bytes, need, h)) return rc;
     }
+    // x-segment length per member: the member's own tile, shortened (halved,
+    // largest members first, down to 8 planes) while the whole work-list would
+    // give the persistent grid fewer than 8 tiles per CTA -- a few small
+    // members alone cannot fill the GPU with full-length segments.  The tile
+    // shape does not change any member's result.
+    std::vector<int> lxs(n);
+    {
+        int sms = 148;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
+        const long long target = 8LL * sms * (b->tz == 16 ? 1 : 2);
+        auto tiles_of = [&](int i, int lx) {
+            const Geom &g = b->m[i]->g;
+            return (long long)(g.nz / b->tz) * xtma_num_vblocks<T>(g) * 2 * ((g.nx + lx - 1) / lx);
+        };
+        long long total = 0;
+        for (int i = 0; i < n; ++i) {
+            lxs[i] = std::min(b->m[i]->tile.lx, b->m[i]->g.nx);  // (the same single segment)
+            total += tiles_of(i, lxs[i]);
+        }
+        while (total < target) {
+            int best = -1;
+            for (int i = 0; i < n; ++i)
+                if (lxs[i] > 8 && (best < 0 || tiles_of(i, lxs[i]) > tiles_of(best, lxs[best]))) best = i;
+            if (best < 0) break;
+            total -= tiles_of(best, lxs[best]);
+            lxs[best] = std::max(8, lxs[best] / 2);
+            total += tiles_of(best, lxs[best]);
+        }
+    }
     b->item_bytes = xtma_batch_item_bytes<T>();
     const size_t tab = 4 * (size_t)n * b->item_bytes;
     std::vector<char> host(tab);
@@ -1100,7 +1173,7 @@ int batch_build(nuosc_batch *b) {
             a.cA = h->dt / sp.da;
             a.cY = sp.fy == 1.0 ? h->dt : sp.fy * h->dt;
             a.status = h->d_status;
-            ti = xtma_batch_fill<T>(&host[((size_t)k * n + i) * b->item_bytes], a, b->ko6, b->tz, h->tile.lx);
+            ti = xtma_batch_fill<T>(&host[((size_t)k * n + i) * b->item_bytes], a, b->ko6, b->tz, lxs[i]);
             if (v0 < h->g.nvs)
                 tails[k].push_back(TailItem<T>{a, v0, tail_lanes(h->g.nvs - v0), xtma_num_vblocks<T>(h->g), 0});
             if (ti < 0) return fail(NUOSC_ERR_UNSUPPORTED, "batch member %d (%dx%d) cannot run %d-row TMA tiles", i,
@@ -1114,7 +1187,7 @@ int batch_build(nuosc_batch *b) {
     }
     if (!b->d_buf) {
         const size_t bytes = tab + 2 * (size_t)n * sizeof(long long) + (size_t)n * sizeof(FinalizeItem) + 256;
-        CUDA_TRY(cudaMalloc((void **)&b->d_buf, bytes));
+        CUDA_TRY(dev_alloc((void **)&b->d_buf, bytes, b->device, b->stream));
         size_t off = tab;
         b->d_starts = (long long *)(b->d_buf + off);
         off += (size_t)n * sizeof(long long);
@@ -1132,7 +1205,8 @@ int batch_build(nuosc_batch *b) {
     b->tail_threads = tthreads;
     if (b->ntail) {
         const size_t tb = 4 * (size_t)b->ntail * sizeof(TailItem<T>);
-        if (!b->d_tail) CUDA_TRY(cudaMalloc((void **)&b->d_tail, tb + (size_t)b->ntail * sizeof(long long)));
+        if (!b->d_tail)
+            CUDA_TRY(dev_alloc((void **)&b->d_tail, tb + (size_t)b->ntail * sizeof(long long), b->device, b->stream));
         for (int k = 0; k < 4; ++k)
             CUDA_TRY(cudaMemcpyAsync(b->d_tail + (size_t)k * b->ntail * sizeof(TailItem<T>), tails[k].data(),
                                      b->ntail * sizeof(TailItem<T>), cudaMemcpyHostToDevice, b->stream));
@@ -1366,6 +1440,13 @@ int nuosc_batch_get_info(const nuosc_batch *b, nuosc_batch_info *o) {
 
 void *nuosc_batch_stream(nuosc_batch *b) { return b ? (void *)b->stream : nullptr; }
 
+int nuosc_release_cached_memory(int device) {
+    CUDA_TRY(cudaSetDevice(device));
+    CUDA_TRY(cudaDeviceSynchronize());
+    if (cudaMemPool_t pool = device_pool(device)) CUDA_TRY(cudaMemPoolTrimTo(pool, 0));
+    return NUOSC_OK;
+}
+
 int nuosc_batch_destroy(nuosc_batch *b) {
     if (!b) return NUOSC_OK;
     cudaSetDevice(b->device);
@@ -1373,8 +1454,10 @@ int nuosc_batch_destroy(nuosc_batch *b) {
     batch_release_graph(b);
     for (nuosc_handle *h : b->m)
         if (h->batch == b) h->batch = nullptr;
-    if (b->d_buf) cudaFree(b->d_buf);
-    if (b->d_tail) cudaFree(b->d_tail);
+    if (b->stream) {
+        dev_free(b->d_buf, b->stream);
+        dev_free(b->d_tail, b->stream);
+    }
     if (b->ev) cudaEventDestroy(b->ev);
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;

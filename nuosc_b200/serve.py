@@ -193,6 +193,7 @@ class Server:
         used = 0.0
         resident = 0.0  # state bytes of one register, summed over the resident solves
         stats = dict(quanta=0, batch_builds=0, peak_bytes=0.0, peak_resident=0, steps_run=0)
+        host = dict(create_s=0.0, build_s=0.0, retire_s=0.0, collect_s=0.0)  # host time per phase
         t0 = time.perf_counter()
         busy = 0.0
         ratio = 1.0  # measured / modelled step time of the last quantum
@@ -224,10 +225,12 @@ class Server:
                 busy += dt_q
                 ratio = max(0.05, min(20.0, dt_q / q / model))
                 stats["quanta"] += 1
+                tc = time.perf_counter()
                 for prec, buf in bufs.items():
                     ids = members[prec]
                     for m, step, d in batches[prec].collect(buf):
                         stream(ids[m], step, d)
+                host["collect_s"] += time.perf_counter() - tc
                 done = []
                 for rid in ran:
                     a = active[rid]
@@ -243,6 +246,7 @@ class Server:
                     recs[rid].completed = now()
                     if self.on_complete:
                         self.on_complete(rid, s)
+                tc = time.perf_counter()
                 if done:
                     for prec in (0, 1):  # a solve leaves its batch before it is freed
                         if batches[prec] is not None and set(done) & set(members[prec]):
@@ -254,9 +258,11 @@ class Server:
                         s.close()
                         used -= fp
                         resident -= register_bytes(recs[rid].req)
+                host["retire_s"] += time.perf_counter() - tc
 
             # 2. launch the next quantum on what is resident
             if active:
+                tc = time.perf_counter()
                 for prec in (0, 1):
                     ids = tuple(sorted(rid for rid, a in active.items() if recs[rid].req.precision == prec))
                     if ids != members[prec]:
@@ -267,6 +273,7 @@ class Server:
                             batches[prec] = self.batch_factory([active[rid][0] for rid in ids])
                             stats["batch_builds"] += 1
                         members[prec] = ids
+                host["build_s"] += time.perf_counter() - tc
                 model = self._step_model([recs[rid].req for rid in active])
                 q = min(recs[rid].req.steps - a[1] for rid, a in active.items())
                 q = max(1, min(q, int(self.quantum_s / (model * ratio))))
@@ -281,8 +288,10 @@ class Server:
                 inflight = (q, bufs, tl, model, tuple(active))
 
             # 3. admit arrived requests while the quantum runs: arrival order,
-            #    while the footprint fits the budget; they join the next quantum
-            while queue and queue[0].arrival <= now():
+            #    while the footprint fits the budget; they join the next quantum.
+            #    With the GPU idle, admit one and go launch it first.
+            tc = time.perf_counter()
+            while queue and queue[0].arrival <= now() and not (inflight is None and active):
                 r = queue[0]
                 fp = footprint_bytes(r.nx, r.nz, r.nn, r.precision)
                 if fp > self.budget:
@@ -298,6 +307,7 @@ class Server:
                 resident += register_bytes(r)
                 recs[r.rid].admitted = now()
                 stream(r.rid, 0, _analysis(s)[0])
+            host["create_s"] += time.perf_counter() - tc
             stats["peak_bytes"] = max(stats["peak_bytes"], used)
             stats["peak_resident"] = max(stats["peak_resident"], len(active))
             if inflight is None and not active and queue:
@@ -306,6 +316,7 @@ class Server:
             if b is not None:
                 b.close()
         makespan = now()
+        stats.update({k: round(v, 3) for k, v in host.items()})
         return self._report(reqs, recs, makespan, busy, stats)
 
     @staticmethod
