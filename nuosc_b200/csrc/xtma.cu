@@ -195,8 +195,10 @@ template <typename T>
 struct MarchShared {
     static constexpr bool kShared = vpt<T>() == 2;
     static constexpr int VB = vblock<T>();
+    // [component][p * 32 + lane] and [4 p + j][lane]: consecutive lanes read
+    // consecutive doubles (a lane-major layout would put 16 lanes on one bank)
     double vq[kShared ? 3 : 1][kShared ? VB : 2];           // vx, vy, vz
-    double wp[kShared ? 32 : 1][kShared ? vpt<T>() * 4 : 2];  // lane-permuted weights
+    double wp[kShared ? vpt<T>() * 4 : 1][kShared ? 32 : 2];  // lane-permuted weights
     int abort;
 };
 
@@ -335,11 +337,11 @@ __device__ __forceinline__ bool xtma_march(const TmaMaps *const &mp, const Stage
         if (r == 0) {
 #pragma unroll
             for (int p = 0; p < NP; ++p) {
-                s_vq[0][NP * lane + p] = vxd[p];
-                s_vq[1][NP * lane + p] = vyd[p];
-                s_vq[2][NP * lane + p] = vzd[p];
+                s_vq[0][p * 32 + lane] = vxd[p];
+                s_vq[1][p * 32 + lane] = vyd[p];
+                s_vq[2][p * 32 + lane] = vzd[p];
 #pragma unroll
-                for (int j = 0; j < 4; ++j) s_wp[lane][4 * p + j] = wperm[p][j];
+                for (int j = 0; j < 4; ++j) s_wp[4 * p + j][lane] = wperm[p][j];
             }
         }
         __syncthreads();
@@ -479,9 +481,9 @@ __device__ __forceinline__ bool xtma_march(const TmaMaps *const &mp, const Stage
         T outm[4][NP];
 #pragma unroll
         for (int p = 0; p < NP; ++p) {
-            const double ux = kShared ? s_vq[0][NP * lane + p] : vxd[p];
-            const double uy = kShared ? s_vq[1][NP * lane + p] : vyd[p];
-            const double uz = kShared ? s_vq[2][NP * lane + p] : vzd[p];
+            const double ux = kShared ? s_vq[0][p * 32 + lane] : vxd[p];
+            const double uy = kShared ? s_vq[1][p * 32 + lane] : vyd[p];
+            const double uz = kShared ? s_vq[2][p * 32 + lane] : vzd[p];
             const T ia = T(inp(m, ux, uy, uz)), ib = T(inp(m + 4, ux, uy, uz)), ie = T(inp(m + 8, ux, uy, uz));
             const T cen[4] = {q[0][R][p], q[1][R][p], q[2][R][p], q[3][R][p]};
             const T st4[4] = {sten[0][p], sten[1][p], sten[2][p], sten[3][p]};
@@ -536,7 +538,7 @@ __device__ __forceinline__ bool xtma_march(const TmaMaps *const &mp, const Stage
                 const double dp[4] = {sw2 ? t2 : t0, sw2 ? t3 : t1, sw2 ? t0 : t2, sw2 ? t1 : t3};
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
-                    const double wj = kShared ? s_wp[lane][4 * p + j] : wperm[p][j];
+                    const double wj = kShared ? s_wp[4 * p + j][lane] : wperm[p][j];
 #pragma unroll
                     for (int c = 0; c < 4; ++c) mp[4 * c + j] = fma(wj, dp[c], mp[4 * c + j]);
                 }
