@@ -15,8 +15,10 @@
 //     march: a warp waits only on full barriers and releases a slot after its
 //     last use by arriving on the slot's "empty" mbarrier; the issuing lane
 //     waits on "empty" before refilling a slot;
-//   * the pointwise U and A inputs of the epilogue are plain coalesced loads
-//     issued at the top of each plane, before the waits and the stencil;
+//   * the pointwise inputs of the epilogue (U in S2, U and A in S3, A in S4;
+//     none in S1) are plain coalesced loads issued at the top of each plane,
+//     before the waits and the stencil -- in S4 with 16-row tiles, cp.async
+//     copies into shared memory one plane ahead instead;
 //   * moment partials: each lane holds its 16 (12 + 4 zero) partial moments in
 //     a lane-dependent permuted order so that the reduce-scatter over the 32
 //     lanes of the warp needs no selects (15 shuffle-adds + 1).
