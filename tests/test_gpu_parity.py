@@ -336,13 +336,15 @@ def test_fp32_tracks_fp64(nb):
 FP32_TOL = 2e-5  # norm-wise, FP32 state after 10 steps against the FP64 oracle
 
 
-@pytest.mark.parametrize("pmo", [0.0, 0.3])
-def test_fp32_kernels_against_oracle(nb, pmo):
+@pytest.mark.parametrize("n,nn,pmo", [(32, 4, 0.0), (32, 4, 0.3), (16, 8, 0.0)])
+def test_fp32_kernels_against_oracle(nb, n, nn, pmo):
     """FP32 state (two velocities per thread in the TMA kernel, one in the
     others), FP64 moments: every stage kernel stays within FP32 rounding of the
-    FP64 oracle on a 32x32 x 162 case."""
-    p = box_params(32, 4, pmo=pmo)
-    o = po.Oracle(nn=4, x0=p[0], x1=p[1], z0=p[0], z1=p[1], dx=0.1, dz=0.1, cfl=0.4, ko=0.1, ko_order=6, pmo=pmo)
+    FP64 oracle on 32x32 x 162 and on 16x16 x 642, where the TMA path hands
+    the last velocity block, 640-641 and the zero padding 642-643, to the tail
+    kernel."""
+    p = box_params(n, nn, pmo=pmo)
+    o = po.Oracle(nn=nn, x0=p[0], x1=p[1], z0=p[0], z1=p[1], dx=0.1, dz=0.1, cfl=0.4, ko=0.1, ko_order=6, pmo=pmo)
     o.fill_init(ipt=1, seed=8, alpha=1.2, eps0=1e-3, sigma=1.0, lnue=0.6, lnueb=0.4)
     o.step(10)
     ref = o.get_state(0)
