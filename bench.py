@@ -384,8 +384,9 @@ def bench_ours(args, world, rank, local):
 
 
 def bench_fp32(args, local, v64):
-    """The FP32 form of the same workload (state and stencil in float, FP64
-    moments and diagnostics): its cell-steps/s and the ratio to FP64."""
+    """The FP32 form of the same workload (state, stencil and the in-block
+    velocity sums in float; the cell moments and diagnostics in FP64): its
+    cell-steps/s and the ratio to FP64."""
     import torch
     import nuosc_b200 as nb
     w = workload(args.size, args.nn, nb.FP32)

@@ -36,7 +36,7 @@ extern "C" {
 
 /* precision of the resident state */
 #define NUOSC_FP64 0 /* state and arithmetic in double (the reference's real, common.h:58) */
-#define NUOSC_FP32 1 /* state and stencil arithmetic in float; moments and diagnostics in double */
+#define NUOSC_FP32 1 /* state and stencil arithmetic in float; cell moments and diagnostics in double */
 
 /* registers (NuOsc FieldVar pointers) */
 #define NUOSC_REG_STAT 0

@@ -301,6 +301,34 @@ class _PinnedRecords:
         self.free()
 
 
+# Record buffers of closed batches, kept for the next batch: freeing page-locked
+# memory (cudaFreeHost) waits for the whole device and measured up to 0.9 s
+# per call in a serving loop, on the path between two quanta.
+_REC_POOL = []
+_REC_MIN = 1024  # records per buffer at least (about 0.2 MB)
+_REC_POOL_MAX = 8
+
+
+def _take_records(n):
+    """A pooled record buffer of at least n records, or a new one."""
+    fit = [b for b in _REC_POOL if b.n >= n]
+    if fit:
+        b = min(fit, key=lambda b: b.n)
+        _REC_POOL.remove(b)
+        return b
+    return _PinnedRecords(max(n, _REC_MIN))
+
+
+def _give_records(buf):
+    """Return a batch's record buffer to the pool (the smallest are freed
+    beyond _REC_POOL_MAX buffers)."""
+    buf.used = 0
+    _REC_POOL.append(buf)
+    if len(_REC_POOL) > _REC_POOL_MAX:
+        _REC_POOL.sort(key=lambda b: b.n)
+        _REC_POOL.pop(0).free()
+
+
 class Batch:
     """Several NuOsc instances stepped together (nuosc_batch_* of the C ABI).
 
@@ -325,7 +353,7 @@ class Batch:
             lib().nuosc_batch_destroy(self._b)
             self._b = None
         if getattr(self, "_rec", None) is not None:
-            self._rec.free()
+            _give_records(self._rec)
             self._rec = None
 
     def __del__(self):
@@ -356,8 +384,8 @@ class Batch:
         nmax = max(1, len(self.members) * (int(nsteps) // max(1, int(every)) + 1))
         if self._rec is None or self._rec.n < nmax:
             if self._rec is not None:
-                self._rec.free()
-            self._rec = _PinnedRecords(max(nmax, 2 * len(self.members)))
+                _give_records(self._rec)
+            self._rec = _take_records(max(nmax, 2 * len(self.members)))
         buf = self._rec
         n = C.c_int()
         check(lib().nuosc_batch_step_stream(self._b, int(nsteps), int(every), buf.ptr, buf.n, C.byref(n)))

@@ -20,7 +20,8 @@
 //     before the waits and the stencil; the issuing lane prefetches their TZ
 //     rows into L2 two planes ahead with a tensor prefetch
 //     (cp.async.bulk.prefetch.tensor), so the loads find them in L2;
-//   * moment partials: each lane holds its 16 (12 + 4 zero) partial moments in
+//   * moment partials (FP64; in FP32 summed in float over the block, stored
+//     as double): each lane holds its 16 (12 + 4 zero) partial moments in
 //     a lane-dependent permuted order (weights permuted once per tile, the
 //     three moment combinations by two selects per plane), so the
 //     reduce-scatter over the 32 lanes of the warp keeps the lower half at
@@ -38,6 +39,7 @@
 #include <cuda.h>
 
 #include <cstring>
+#include <type_traits>
 
 namespace nuosc {
 
@@ -189,22 +191,22 @@ __device__ __forceinline__ void rhs_half(const T (&c)[4], T a, T b, T e, T mu, T
 
 // one reduce-scatter step over lane pairs (lane, lane^O): N values -> N/2;
 // the lane-permuted slot order makes the kept half always the lower one
-template <int N, int O>
-__device__ __forceinline__ void rs_step(double (&m)[16]) {
+template <int N, int O, typename M>
+__device__ __forceinline__ void rs_step(M (&m)[16]) {
 #pragma unroll
     for (int i = 0; i < N / 2; ++i) m[i] += __shfl_xor_sync(0xffffffffu, m[i + N / 2], O);
 }
 
 // statically allocated per-CTA scratch of the march: the abort flag and, with
-// two velocities per thread (FP32), the FP64 per-velocity constants
+// two velocities per thread (FP32), the per-velocity constants
 template <typename T>
 struct MarchShared {
     static constexpr bool kShared = vpt<T>() == 2;
     static constexpr int VB = vblock<T>();
     // [component][p * 32 + lane] and [4 p + j][lane]: consecutive lanes read
-    // consecutive doubles (a lane-major layout would put 16 lanes on one bank)
-    double vq[kShared ? 3 : 1][kShared ? VB : 2];           // vx, vy, vz
-    double wp[kShared ? vpt<T>() * 4 : 1][kShared ? 32 : 2];  // lane-permuted weights
+    // consecutive words (a lane-major layout would put 16 lanes on one bank)
+    double vq[kShared ? 3 : 1][kShared ? VB : 2];          // vx, vy, vz
+    float wp[kShared ? vpt<T>() * 4 : 1][kShared ? 32 : 2];  // lane-permuted weights, rounded to float
     int abort;
 };
 
@@ -324,8 +326,9 @@ __device__ __forceinline__ bool xtma_march(const TmaMaps *const &mp, const Stage
     // per-velocity and uniform constants.  Lane-permuted moment weights: slot i
     // of this lane holds moment (i ^ perm), moment k = (combo k>>2, weight
     // k&3); perm = bits 1..4 of the lane.  With two velocities per thread
-    // (FP32) the FP64 per-velocity constants live in shared memory and are
-    // read per plane, which keeps the register queue clear of spills.
+    // (FP32) the per-velocity constants (FP64 velocities, float weights) live
+    // in shared memory and are read per plane, which keeps the register queue
+    // clear of spills.
     const int perm = (lane >> 1) & 15;
     constexpr bool kShared = MarchShared<T>::kShared;
     auto &s_vq = sh.vq;
@@ -355,7 +358,7 @@ __device__ __forceinline__ bool xtma_march(const TmaMaps *const &mp, const Stage
                 s_vq[1][p * 32 + lane] = vyd[p];
                 s_vq[2][p * 32 + lane] = vzd[p];
 #pragma unroll
-                for (int j = 0; j < 4; ++j) s_wp[4 * p + j][lane] = wperm[p][j];
+                for (int j = 0; j < 4; ++j) s_wp[4 * p + j][lane] = (float)wperm[p][j];
             }
         }
         __syncthreads();
@@ -517,23 +520,33 @@ __device__ __forceinline__ bool xtma_march(const TmaMaps *const &mp, const Stage
                 }
             }
         }
-        // velocity-moment partials of the written state (nuosc_class.cpp:69-71)
+        // velocity-moment partials of the written state (nuosc_class.cpp:69-71).
+        // FP64: products and the warp's reduce-scatter in double.  FP32 (two
+        // velocities per thread): in float -- the float state's products with
+        // float-rounded weights, summed over the block's 64 velocities --, the
+        // block's partial stored as double and the blocks and both halves summed
+        // in FP64 by the finalize; half of the FP32 step's FP64 instructions and
+        // 64-bit shuffles go, which measured 7 % off the FP32 step with no
+        // visible change in the FP32-vs-FP64 error series.
         {
-            double mp[16];
+            using M = std::conditional_t<kShared, float, double>;
+            M mp[16];
 #pragma unroll
-            for (int k = 0; k < 16; ++k) mp[k] = 0.0;
+            for (int k = 0; k < 16; ++k) mp[k] = M(0);
 #pragma unroll
             for (int p = 0; p < NP; ++p) {
-                double d0, d1, d2;
-                if (half == 0) moment_terms<false>(outm[0][p], outm[1][p], outm[2][p], outm[3][p], d0, d1, d2);
-                else moment_terms<true>(outm[0][p], outm[1][p], outm[2][p], outm[3][p], d0, d1, d2);
-                if (!vact) d0 = d1 = d2 = 0.0;
+                // combinations: neutrinos enter with sign -1, antineutrinos +1
+                const M ee = M(outm[0][p]), mm = M(outm[1][p]), emr = M(outm[2][p]), emi = M(outm[3][p]);
+                M d0 = half ? emr : -emr, d1 = emi, d2 = half ? ee - mm : mm - ee;
+                if (!vact) d0 = d1 = d2 = M(0);
                 // combos in slot order: dp[c] = d[c ^ (perm >> 2)], d[3] = 0
-                const double t0 = sw1 ? d1 : d0, t1 = sw1 ? d0 : d1, t2 = sw1 ? 0.0 : d2, t3 = sw1 ? d2 : 0.0;
-                const double dp[4] = {sw2 ? t2 : t0, sw2 ? t3 : t1, sw2 ? t0 : t2, sw2 ? t1 : t3};
+                const M t0 = sw1 ? d1 : d0, t1 = sw1 ? d0 : d1, t2 = sw1 ? M(0) : d2, t3 = sw1 ? d2 : M(0);
+                const M dp[4] = {sw2 ? t2 : t0, sw2 ? t3 : t1, sw2 ? t0 : t2, sw2 ? t1 : t3};
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
-                    const double wj = kShared ? s_wp[4 * p + j][lane] : wperm[p][j];
+                    M wj;
+                    if constexpr (kShared) wj = s_wp[4 * p + j][lane];
+                    else wj = wperm[p][j];
 #pragma unroll
                     for (int c = 0; c < 4; ++c) mp[4 * c + j] = fma(wj, dp[c], mp[4 * c + j]);
                 }
@@ -545,7 +558,7 @@ __device__ __forceinline__ bool xtma_march(const TmaMaps *const &mp, const Stage
             mp[0] += __shfl_xor_sync(0xffffffffu, mp[0], 1);
             if ((lane & 1) == 0 && perm < NMOM) {  // lanes 2k, 2k+1 hold moment perm
                 const long long cell = (long long)x * rd<SA>(a.g.nz) + zr;
-                rd<SA>(a.mom_part)[((cell * nvb + vb) * 2 + half) * NMOM + perm] = mp[0];
+                rd<SA>(a.mom_part)[((cell * nvb + vb) * 2 + half) * NMOM + perm] = (double)mp[0];
             }
         }
 #pragma unroll

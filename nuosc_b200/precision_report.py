@@ -3,8 +3,9 @@
     python -m nuosc_b200.precision_report --size 256 --nn 8 --steps 2000 --every 100 [--hard]
 
 Runs the FP64 solver (parity-checked against the reference) and the FP32
-solver (float state and stencil arithmetic, FP64 velocity moments and FP64
-diagnostics) from the same seeded initial data, one after the other so that
+solver (float state and stencil arithmetic, velocity sums in float within a
+64-velocity block and in FP64 across blocks, FP64 diagnostics) from the same
+seeded initial data, one after the other so that
 each can use the whole GPU, and compares the analysis() record at every
 output time: |dPee| (surv and survb), |d(|P|-1)| (max and weighted average),
 |dM0|.  --hard selects the harder instability case (alpha 1.2, sigma_nubar

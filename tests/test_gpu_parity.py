@@ -315,7 +315,7 @@ def test_error_paths(nb):
 
 
 def test_fp32_tracks_fp64(nb):
-    """FP32 state with FP64 moments and diagnostics stays close to FP64 on
+    """FP32 state (FP64 cell moments and diagnostics) stays close to FP64 on
     config 0 over 100 steps."""
     p = box_params(64, 4)
     runs = {}
@@ -339,7 +339,7 @@ FP32_TOL = 2e-5  # norm-wise, FP32 state after 10 steps against the FP64 oracle
 @pytest.mark.parametrize("n,nn,pmo", [(32, 4, 0.0), (32, 4, 0.3), (16, 8, 0.0)])
 def test_fp32_kernels_against_oracle(nb, n, nn, pmo):
     """FP32 state (two velocities per thread in the TMA kernel, one in the
-    others), FP64 moments: every stage kernel stays within FP32 rounding of the
+    others), FP64 cell moments: every stage kernel stays within FP32 rounding of the
     FP64 oracle on 32x32 x 162 and on 16x16 x 642, where the TMA path hands
     the last velocity block, 640-641 and the zero padding 642-643, to the tail
     kernel."""

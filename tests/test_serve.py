@@ -144,6 +144,39 @@ def test_fifo_model():
 
 
 @pytest.mark.gpu
+def test_record_buffer_pool(monkeypatch):
+    """Closed batches hand their page-locked record buffers to a pool that the
+    next batch takes from (smallest that fits), so the serving loop frees no
+    page-locked memory between quanta; the pool is bounded."""
+    import nuosc_b200 as nb
+
+    made, freed = [], []
+
+    class FakeRecords:
+        def __init__(self, n):
+            self.n, self.used = n, 0
+            made.append(self)
+
+        def free(self):
+            freed.append(self)
+
+    monkeypatch.setattr(nb, "_PinnedRecords", FakeRecords)
+    monkeypatch.setattr(nb, "_REC_POOL", [])
+    a = nb._take_records(10)
+    assert a.n == nb._REC_MIN and len(made) == 1
+    nb._give_records(a)
+    assert nb._take_records(100) is a and len(made) == 1  # reused, no new allocation
+    big = nb._take_records(5000)
+    assert big.n == 5000 and len(made) == 2
+    nb._give_records(big)
+    nb._give_records(a)
+    assert nb._take_records(50) is a  # the smallest that fits
+    for k in range(nb._REC_POOL_MAX + 3):
+        nb._give_records(FakeRecords(2000 + k))
+    assert len(nb._REC_POOL) == nb._REC_POOL_MAX and len(freed) == 4
+    assert all(f.n <= min(b.n for b in nb._REC_POOL) for f in freed)
+
+
 def test_served_results_equal_solo(gpu):
     reqs = serve.draw_requests(12, rate=40.0, seed=11, steps=(30, 260), sizes=(32, 64), nns=(2, 4))
     assert {r.precision for r in reqs} == {0, 1}
