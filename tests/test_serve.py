@@ -143,7 +143,6 @@ def test_fifo_model():
     assert m["latency_p50_s"] == pytest.approx(2.5)
 
 
-@pytest.mark.gpu
 def test_record_buffer_pool(monkeypatch):
     """Closed batches hand their page-locked record buffers to a pool that the
     next batch takes from (smallest that fits), so the serving loop frees no
@@ -177,6 +176,7 @@ def test_record_buffer_pool(monkeypatch):
     assert all(f.n <= min(b.n for b in nb._REC_POOL) for f in freed)
 
 
+@pytest.mark.gpu
 def test_served_results_equal_solo(gpu):
     reqs = serve.draw_requests(12, rate=40.0, seed=11, steps=(30, 260), sizes=(32, 64), nns=(2, 4))
     assert {r.precision for r in reqs} == {0, 1}
