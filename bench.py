@@ -479,15 +479,21 @@ def bench_serving(args, local, single):
     rp = serve.Server(budget_bytes=150e9, device=local).run(reqs)
     t = serve.solo_fp64_step_times(reqs, device=local)
     one = serve.fifo_one_at_a_time(reqs, {r.rid: t[(r.nx, r.nz, r.nn)] * r.steps for r in reqs})
+
+    def loop_stats(r):  # device-busy time, quanta, batch rebuilds, host time per server phase
+        return {"busy_s": r["busy_s"], "quanta": r["quanta"], "batch_builds": r["batch_builds"],
+                "host_s": {k: r[k + "_s"] for k in ("create", "build", "retire", "collect")}}
+
     return {"requests": len(reqs), "steps_range": list(steps), "budget_gb": 150,
             "saturated": {"cell_steps_per_s": rs["cell_steps_per_s"],
                           "vs_single_large_solve": rs["cell_steps_per_s"] / ref_rate(sat),
                           "makespan_s": rs["makespan_s"], "peak_resident": rs["peak_resident"],
-                          "latency_p50_s": rs["latency_p50_s"], "latency_p99_s": rs["latency_p99_s"]},
+                          "latency_p50_s": rs["latency_p50_s"], "latency_p99_s": rs["latency_p99_s"],
+                          **loop_stats(rs)},
             "poisson": {"rate_per_s": args.serve_rate, "cell_steps_per_s": rp["cell_steps_per_s"],
                         "cell_steps_per_busy_s": rp["cell_steps_per_busy_s"],
                         "latency_p50_s": rp["latency_p50_s"], "latency_p99_s": rp["latency_p99_s"],
-                        "makespan_s": rp["makespan_s"], "peak_resident": rp["peak_resident"],
+                        "makespan_s": rp["makespan_s"], "peak_resident": rp["peak_resident"], **loop_stats(rp),
                         "one_at_a_time_fp64": {k: one[k] for k in ("cell_steps_per_s", "latency_p50_s",
                                                                    "latency_p99_s", "makespan_s")}},
             "diverged": rp["diverged"],
