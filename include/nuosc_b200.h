@@ -203,6 +203,14 @@ long long nuosc_step_count(const nuosc_handle *h);
  * counterpart (the reference allocates with new[] once per run). */
 int nuosc_release_cached_memory(int device);
 
+/* Self-test of the in-kernel bounded waits (no reference counterpart): one
+ * warp waits on an mbarrier that nothing completes, gives up after `spins`
+ * polls, records the timeout in a status word and returns, as the stage
+ * kernels do when a copy never lands.  Returns NUOSC_ERR_TIMEOUT when the wait
+ * expired and was reported (the expected outcome), with the kernel's time in
+ * *ms (may be NULL); the device stays usable afterwards. */
+int nuosc_selftest_wait_timeout(int device, unsigned spins, double *ms);
+
 /* Per-kernel timing with CUDA events on the handle's stream (no counterpart
  * in the reference, which prints wall time per step, nuosc.cpp:222-235).
  * Kinds: 0 stage S1, 1 stage S2/S3, 2 stage S4, 3 calRHS, 4 moments,

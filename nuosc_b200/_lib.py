@@ -110,6 +110,7 @@ _SIGS = {
     "nuosc_batch_step_stream": [_P, _I, _I, _P, _I, _IP],
     "nuosc_batch_record_diag": [_P, C.POINTER(BatchRecord), C.POINTER(Diag)],
     "nuosc_release_cached_memory": [_I],
+    "nuosc_selftest_wait_timeout": [_I, C.c_uint, C.POINTER(C.c_double)],
 }
 PROF_KINDS = ["stage_s1", "stage_s23", "stage_s4", "calrhs", "moments", "moment_finalize"]
 

@@ -1440,6 +1440,35 @@ int nuosc_batch_get_info(const nuosc_batch *b, nuosc_batch_info *o) {
 
 void *nuosc_batch_stream(nuosc_batch *b) { return b ? (void *)b->stream : nullptr; }
 
+int nuosc_selftest_wait_timeout(int device, unsigned spins, double *ms) {
+    if (spins < 1) return fail(NUOSC_ERR_INVALID, "selftest: spins must be positive");
+    CUDA_TRY(cudaSetDevice(device));
+    cudaStream_t s = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    int *d = nullptr, st = 0;
+    float el = 0.f;
+    cudaError_t e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreate(&e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&e1);
+    if (e == cudaSuccess) e = dev_alloc((void **)&d, sizeof(int), device, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d, 0, sizeof(int), s);
+    if (e == cudaSuccess) e = cudaEventRecord(e0, s);
+    if (e == cudaSuccess) e = launch_wait_selftest(d, spins, s);
+    if (e == cudaSuccess) e = cudaEventRecord(e1, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&st, d, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&el, e0, e1);
+    if (d) dev_free(d, s);
+    if (s) cudaStreamSynchronize(s);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (s) cudaStreamDestroy(s);
+    if (e != cudaSuccess) return fail(NUOSC_ERR_CUDA, "selftest: %s", cudaGetErrorString(e));
+    if (ms) *ms = el;
+    if (st != NUOSC_TIMEOUT_CODE) return fail(NUOSC_ERR_INVALID, "selftest: the wait did not expire (status %d)", st);
+    return fail(NUOSC_ERR_TIMEOUT, "selftest: the bounded wait expired after %u polls (%.3f ms)", spins, el);
+}
+
 int nuosc_release_cached_memory(int device) {
     CUDA_TRY(cudaSetDevice(device));
     CUDA_TRY(cudaDeviceSynchronize());

@@ -148,6 +148,9 @@ cudaError_t launch_moment_finalize_batch(const FinalizeItem *items, const long l
                                          cudaStream_t s);
 // value a kernel writes into StageArgs::status when a bounded wait expires
 constexpr int NUOSC_TIMEOUT_CODE = 1;
+// one warp waits `spins` polls on an mbarrier that never completes, then sets
+// *status = NUOSC_TIMEOUT_CODE (xtma.cu; the self-test of the bounded waits)
+cudaError_t launch_wait_selftest(int *status, unsigned spins, cudaStream_t s);
 
 // records msg as the calling thread's nuosc_last_error() and returns code (capi.cu)
 int set_last_error(int code, const char *msg);

@@ -45,7 +45,10 @@ namespace nuosc {
 
 namespace {
 
-constexpr unsigned kWaitSpins = 1u << 22;  // bounded mbarrier waits
+// bounded mbarrier waits: a poll of a phase that has not completed suspends
+// the thread for about 4 us on B200 (nuosc_selftest_wait_timeout), so 2^18
+// polls give up after about 1 s
+constexpr unsigned kWaitSpins = 1u << 18;
 
 // velocities per thread and per CTA: FP32 threads take two adjacent velocities
 template <typename T>
@@ -77,8 +80,8 @@ __device__ __forceinline__ void mbar_expect_tx(unsigned bar, unsigned bytes) {
 __device__ __forceinline__ void mbar_arrive(unsigned bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(bar) : "memory");
 }
-__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity) {
-    for (unsigned it = 0; it < kWaitSpins; ++it) {
+__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity, unsigned spins = kWaitSpins) {
+    for (unsigned it = 0; it < spins; ++it) {
         unsigned ok;
         asm volatile(
             "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
@@ -682,6 +685,27 @@ __global__ void __launch_bounds__(32 * TZ, tma_ctas_per_sm<T, TZ>())
         __syncthreads();  // s_a is complete
         if (xtma_march<T, R, MODE, TZ, VAC, true>(s_mp, s_a, z0, vb, nvb, xs, xe, half, smem, sh)) break;
     }
+}
+
+// Self-test of the bounded wait that the march kernels use: one warp waits on
+// an mbarrier that nothing completes (initialised for two arrivals, given
+// one).  The wait gives up after `spins` polls; the kernel then records the
+// timeout in the status word, as a march does, invalidates the barrier and
+// returns.  Nothing else is touched, so the context stays usable.
+__global__ void k_wait_selftest(int *status, unsigned spins) {
+    __shared__ __align__(8) unsigned long long bar;
+    if (threadIdx.x == 0) {
+        mbar_init(smem_u32(&bar), 2u);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+        mbar_arrive(smem_u32(&bar));  // one arrival of two: phase 0 never completes
+        if (!mbar_wait(smem_u32(&bar), 0u, spins)) atomicExch(status, NUOSC_TIMEOUT_CODE);
+        mbar_inval(smem_u32(&bar));
+    }
+}
+
+cudaError_t launch_wait_selftest(int *status, unsigned spins, cudaStream_t s) {
+    k_wait_selftest<<<1, 32, 0, s>>>(status, spins);
+    return cudaGetLastError();
 }
 
 // ------------------------------------------------------------------ host side
