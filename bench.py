@@ -22,7 +22,7 @@ roofline the dominant kernel (the S2/S3 stage kernel) timed live with CUDA
          the measured HBM copy bandwidth in MEASURED_PEAKS.json; step figures
          use 1024 B per cell-step.  The bytes this implementation actually
          moves (14 passes per step: S2 4, S3 5) are reported beside as moved_*,
-         and ncu's DRAM traffic per launch as traffic.
+         and ncu's DRAM traffic per launch as traffic (per step: step_traffic).
 N > 1    one independent full-size solve per GPU (the reference's hot path has
          no exchange on one GPU); value = all ranks' cell-steps / max time.
 --impl reference   the reference's own CPU build (oracle/_ref, or the C
@@ -145,6 +145,13 @@ def traffic_per_launch(kernel_key):
             return json.load(f).get(kernel_key)
     except Exception:
         return None
+
+
+def step_traffic(dtype, nx, nv):
+    """ncu DRAM bytes of one RK4 step's four stage launches (S1, S2, S3, S4;
+    tails and finalize excluded) from the committed per-launch figures, or None."""
+    ks = [traffic_per_launch("stage_%s_%s_%d_%d" % (k, dtype, nx, nv)) for k in ("s1", "s23", "s23", "s4")]
+    return float(sum(ks)) if all(k is not None for k in ks) else None
 
 
 def dist_setup(args=None, backend=None):
@@ -310,6 +317,7 @@ def bench_ours(args, world, rank, local):
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak if achieved else None,
                 "traffic": traffic_per_launch("stage_s23_%s_%d_%d" % (dtype, nx, nv)),
+                "step_traffic": step_traffic(dtype, nx, nv),
                 "kernel": "stage S2/S3 (%s)" % ("x-march" if prof["moment_finalize"][1] else "direct"),
                 "algorithmic_bytes_per_launch": alg_bytes,
                 "moved_bytes_per_launch": moved_bytes,

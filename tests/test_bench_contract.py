@@ -46,3 +46,19 @@ def test_reference_arm_under_torchrun_two_ranks():
     assert len(lines) == 1
     d = json.loads(lines[0])
     assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["value"] > 0
+
+
+def test_step_traffic_from_profiles():
+    """The roofline's per-step DRAM bytes are the four stage launches' ncu
+    figures (S2/S3 counted twice); sizes without a capture give None."""
+    sys.path.insert(0, ROOT)
+    import bench
+    with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+        t = json.load(f)
+    for dt in ("f64", "f32"):
+        want = sum(t["stage_%s_%s_1024_642" % (k, dt)] for k in ("s1", "s23", "s23", "s4"))
+        assert bench.step_traffic(dt, 1024, 642) == want
+        # within 10 % of the bytes the 14-pass step moves (896 / 448 B per cell-step)
+        moved = bench.MOVED_BYTES_PER_CELL_STEP[dt] * 1024 * 1024 * 642
+        assert 1.0 <= want / moved < 1.1
+    assert bench.step_traffic("f64", 512, 642) is None
