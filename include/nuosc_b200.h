@@ -32,7 +32,7 @@ extern "C" {
 #define NUOSC_ERR_OOM 3         /* not enough device memory for the request */
 #define NUOSC_ERR_NUMERIC 4     /* non-finite state or max||P|-1| >= 10 (nuosc_ana.cpp:131 assert) */
 #define NUOSC_ERR_TIMEOUT 5     /* a bounded in-kernel wait expired; the kernel returned early */
-#define NUOSC_ERR_UNSUPPORTED 6 /* a configuration this build does not implement */
+#define NUOSC_ERR_UNSUPPORTED 6 /* a configuration this library does not implement */
 
 /* precision of the resident state */
 #define NUOSC_FP64 0 /* state and arithmetic in double (the reference's real, common.h:58) */

@@ -30,7 +30,7 @@ import pyoracle as po  # noqa: E402
 
 OUT = os.path.dirname(os.path.abspath(__file__))
 
-# the physics configuration shared by all run fixtures (config 0 recipe)
+# the physics shared by all run fixtures: alpha 0.9, eps0 1e-6, spectra widths 0.6 / 0.5
 PHYS = dict(alpha=0.9, eps0=1e-6, lnue=0.6, lnueb=0.5)
 
 

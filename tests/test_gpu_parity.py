@@ -120,7 +120,7 @@ def test_ten_steps_match_reference(nb, ko_order, kernel):
 
 @pytest.mark.parametrize("kernel", KERNELS)
 def test_c0_config_100_steps(nb, kernel):
-    """64x64 cells x 162 velocities, 100 steps, analysis every 10 (config 0):
+    """64x64 cells x 162 velocities, dx 0.1, 100 steps, analysis every 10:
     diagnostics against the reference's series, state against the oracle."""
     g = golden("c0_series.npz")
     p = box_params(64, 4)
@@ -316,7 +316,7 @@ def test_error_paths(nb):
 
 def test_fp32_tracks_fp64(nb):
     """FP32 state (FP64 cell moments and diagnostics) stays close to FP64 on
-    config 0 over 100 steps."""
+    64x64 cells x 162 velocities over 100 steps."""
     p = box_params(64, 4)
     runs = {}
     for prec in (nb.FP64, nb.FP32):
