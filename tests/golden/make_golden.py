@@ -14,7 +14,7 @@ fixtures pin both the oracle and the CUDA path.  Outputs (all .npz):
   run_ko4.npz         10 RK4 steps, with analysis() before and after
   calrhs_ko6.npz      calRHS of a seeded random state (pmo=0.7, mu=1.3)
   calrhs_ko4.npz      same for the 4th-difference KO branch (pmo=0)
-  c0_series.npz       the 64x64 x 162 configuration: analysis() every 10 steps
+  series_64x64x162.npz  the 64x64 x 162 workload: analysis() every 10 steps
                       for 100 steps and per-field checksums of the final state
   snapshot.npz        bytes of the files addSnapShotAtV / addSnapShotAtXV write
 """
@@ -88,7 +88,7 @@ def gen_calrhs(ko_order, pmo, mu):
     r.close()
 
 
-def gen_c0():
+def gen_series():
     x0, x1 = po.box(64, 0.1)
     kw = dict(nn=4, x0=x0, x1=x1, z0=x0, z1=x1, dx=0.1, dz=0.1, cfl=0.4, ko=0.1, ko_order=6, mu=1.0,
               pmo=0.0)
@@ -101,7 +101,7 @@ def gen_c0():
     s = r.get_state(0)
     flat = s.reshape(8, -1)
     sample_idx = np.arange(0, flat.shape[1], 997)
-    np.savez_compressed(os.path.join(OUT, "c0_series.npz"), series=np.array(series), seed=2024,
+    np.savez_compressed(os.path.join(OUT, "series_64x64x162.npz"), series=np.array(series), seed=2024,
                         fsum=flat.sum(axis=1), fsq=(flat * flat).sum(axis=1),
                         fmax=np.abs(flat).max(axis=1), sample_idx=sample_idx, sample=flat[:, sample_idx])
     r.close()
@@ -131,7 +131,7 @@ if __name__ == "__main__":
     gen_run(4)
     gen_calrhs(6, pmo=0.7, mu=1.3)
     gen_calrhs(4, pmo=0.0, mu=1.0)
-    gen_c0()
+    gen_series()
     gen_snapshot()
     for f in sorted(os.listdir(OUT)):
         if f.endswith(".npz"):

@@ -119,10 +119,10 @@ def test_ten_steps_match_reference(nb, ko_order, kernel):
 
 
 @pytest.mark.parametrize("kernel", KERNELS)
-def test_c0_config_100_steps(nb, kernel):
+def test_series_64x64x162_100_steps(nb, kernel):
     """64x64 cells x 162 velocities, dx 0.1, 100 steps, analysis every 10:
     diagnostics against the reference's series, state against the oracle."""
-    g = golden("c0_series.npz")
+    g = golden("series_64x64x162.npz")
     p = box_params(64, 4)
     s = make(nb, p, 6)
     s.fillInitValue(1, seed=int(g["seed"]), **PHYS)

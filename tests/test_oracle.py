@@ -75,9 +75,9 @@ def test_calrhs_matches_reference(ko_order):
 
 
 @pytest.mark.slow
-def test_c0_series_matches_reference():
+def test_series_64x64x162_matches_reference():
     """64x64 cells x 162 velocities, 100 RK4 steps, analysis every 10."""
-    g = golden("c0_series.npz")
+    g = golden("series_64x64x162.npz")
     x0, x1 = po.box(64, 0.1)
     o = po.Oracle(nn=4, x0=x0, x1=x1, z0=x0, z1=x1, dx=0.1, dz=0.1, cfl=0.4, ko=0.1, ko_order=6, mu=1.0, pmo=0.0)
     o.fill_init(ipt=1, seed=int(g["seed"]), **PHYS)
