@@ -16,18 +16,21 @@ value    device-timed (CUDA events on the solver's stream), W warm-up steps,
 e2e      the same metric through the public C ABI with host buffers: upload
          the state from pinned host memory, K steps each followed by
          analysis() (diagnostics read back), download the final state.
-roofline the dominant kernel (the S2/S3 stage kernel) timed live with CUDA
-         events: algorithmic bytes per launch (the classic RK4 stage's 5 state
-         passes x 8 fields x 8 B per cell-velocity) / mean launch time, against
-         the measured HBM copy bandwidth in MEASURED_PEAKS.json; step figures
-         use 1024 B per cell-step.  The bytes this implementation actually
-         moves (14 passes per step: S2 4, S3 5) are reported beside as moved_*,
-         and ncu's DRAM traffic per launch as traffic (per step: step_traffic).
+roofline the dominant stage kernel (largest share of the live step time)
+         timed with CUDA events on the solver's stream: the state passes that
+         stage reads and writes in the 13-pass step (S1 2, S2 and S3 3 each,
+         S4 5) x 8 fields x 8 B per cell-velocity / mean launch time, against
+         the measured HBM copy bandwidth in MEASURED_PEAKS.json.  Step figures
+         use the classic RK4 sequence's 1024 B per cell-step (step_frac,
+         frac_vs_8tbs) and the 832 B this implementation moves (step_moved_*);
+         ncu's DRAM traffic per launch is `traffic` (per step: step_traffic).
 N > 1    one independent full-size solve per GPU (the reference's hot path has
          no exchange on one GPU); value = all ranks' cell-steps / max time.
 --impl reference   the reference's own CPU build (oracle/_ref, or the C
-         oracle where that build is absent) on the host cores, each step one
-         RK4 step of a bounded 128 x 128 x 642 sample of the workload.
+         oracle where that build is absent) on all host cores, each step one
+         RK4 step of a bounded 128 x 128 x 642 sample of the workload (the
+         line's config names that sample); the same sample on one thread is
+         reported beside (cpu_baseline.one_thread).
 extras   (N = 1, skipped with --no-extras) keys "fp32": the same workload
          with FP32 state; "batch": 64 uneven instances per precision in one
          persistent-kernel batch; "serving": a bounded continuous-batching
@@ -51,11 +54,12 @@ METRIC = "cell-steps/s"
 # Y (5 each); S4 reads Y and A, writes U (3) -- 16 passes x 8 fields x
 # sizeof(real) per cell-step, the fixed work figure the roofline counts.
 BYTES_PER_CELL_STEP = {"f64": 1024, "f32": 512}
-STAGE_S23_PASSES = 5
-# Bytes this implementation moves for the same work (the 14-pass sequence of
-# the TMA path: S1 stores only Y, S2 rebuilds A from U and Y): reported beside.
-MOVED_BYTES_PER_CELL_STEP = {"f64": 896, "f32": 448}
-STAGE_S23_MOVED_PASSES = 4.5  # S2 4, S3 5
+# State passes (8 fields each) per stage launch in the 13-pass step of the TMA
+# path: S1 reads U, writes Y2; S2 (S3) reads Y2 (Y3) and U, writes Y3 (Y4); S4
+# reads Y4, U, Y2, Y3 and writes U.  The profile kind "stage_s23" holds S2 and S3.
+STAGE_PASSES = {"stage_s1": 2, "stage_s23": 3, "stage_s4": 5}
+STAGE_NAMES = {"stage_s1": "S1", "stage_s23": "S2/S3", "stage_s4": "S4"}
+MOVED_BYTES_PER_CELL_STEP = {"f64": 13 * 64, "f32": 13 * 32}
 
 
 def workload(size, nn, precision):
@@ -150,7 +154,8 @@ def traffic_per_launch(kernel_key):
 def step_traffic(dtype, nx, nv):
     """ncu DRAM bytes of one RK4 step's four stage launches (S1, S2, S3, S4;
     tails and finalize excluded) from the committed per-launch figures, or None."""
-    ks = [traffic_per_launch("stage_%s_%s_%d_%d" % (k, dtype, nx, nv)) for k in ("s1", "s23", "s23", "s4")]
+    ks = [traffic_per_launch("%s_%s_%d_%d" % (k, dtype, nx, nv)) for k in ("stage_s1", "stage_s23", "stage_s23",
+                                                                           "stage_s4")]
     return float(sum(ks)) if all(k is not None for k in ks) else None
 
 
@@ -221,8 +226,8 @@ def cpu_worker(args):
                       "value": nx * nz * nv * len(times) / total, "ms_per_step": 1e3 * total / len(times)}))
 
 
-def run_cpu(size, nn, steps, warmup, budget):
-    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+def run_cpu(size, nn, steps, warmup, budget, threads=None):
+    cores = threads or (len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count())
     env = dict(os.environ, OMP_NUM_THREADS=str(cores), OMP_PROC_BIND="close")
     cmd = [sys.executable, os.path.abspath(__file__), "--cpu-worker", "--cpu-size", str(size), "--cpu-nn", str(nn),
            "--cpu-steps", str(steps), "--cpu-warmup", str(warmup), "--cpu-budget", str(budget)]
@@ -232,25 +237,44 @@ def run_cpu(size, nn, steps, warmup, budget):
     return res
 
 
-def cpu_baseline_obj(res):
-    return {"value": res["value"], "unit": METRIC, "cores": res["cores"], "kind": res["kind"],
-            "sample": "%dx%d cells x %d velocities, FP64, 6th-difference KO, %d RK4 steps after 1 warm-up, "
-                      "OMP threads=%d (%s)" % (res["nx"], res["nz"], res["nv"], res["steps"], res["cores"],
-                                               "reference CPU build oracle/_ref" if res["kind"] == "reference"
-                                               else "C restatement oracle/")}
+def cpu_baseline_obj(res, one=None):
+    o = {"value": res["value"], "unit": METRIC, "cores": res["cores"], "kind": res["kind"],
+         "sample": "%dx%d cells x %d velocities, FP64, 6th-difference KO, %d RK4 steps after 1 warm-up, "
+                   "OMP threads=%d (%s)" % (res["nx"], res["nz"], res["nv"], res["steps"], res["cores"],
+                                            "reference CPU build oracle/_ref" if res["kind"] == "reference"
+                                            else "C restatement oracle/")}
+    if one is not None:
+        o["one_thread"] = {"value": one["value"], "unit": METRIC, "cores": 1, "steps": one["steps"],
+                           "ms_per_step": one["ms_per_step"]}
+    return o
+
+
+def one_thread_cpu(args):
+    """The same CPU sample on one thread (1 warm-up, at least 2 timed steps)."""
+    try:
+        return run_cpu(args.cpu_sample, args.nn, 3, 1, budget=args.cpu_seconds_1t, threads=1)
+    except Exception:
+        return None
 
 
 def bench_reference(args, world, rank):
-    w = workload(args.size, args.nn, args.precision)
+    w = workload(args.cpu_sample, args.nn, 0)
     nv = 10 * args.nn * args.nn + 2
     if rank != 0:
         return 0
     res = run_cpu(args.cpu_sample, args.nn, args.steps, max(1, args.warmup), budget=1e9)
+    one = one_thread_cpu(args)
+    cfg = config_of(w, nv, "n/a (CPU)")
+    cfg["workload"] = ("RK4 step of the reference's CPU build on a %dx%d cells x %d velocities sample of the "
+                       "%dx%d x %d workload (the full size needs about 283 GB of host memory in the reference's "
+                       "layout), FP64, 6th-difference KO, dx 0.1" % (res["nx"], res["nz"], res["nv"], args.size,
+                                                                       args.size, nv))
+    cfg["dx"] = 0.1
     line = {"metric": METRIC, "value": res["value"], "unit": METRIC, "impl": "reference", "n_gpus": world,
             "steps": res["steps"], "warmup": args.warmup, "ms_per_step": res["ms_per_step"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (seeded eps per cell)", "config": config_of(w, nv, "n/a (CPU)"),
-            "cpu_baseline": cpu_baseline_obj(res),
+            "data": "synthetic (seeded eps per cell)", "config": cfg,
+            "cpu_baseline": cpu_baseline_obj(res, one),
             "e2e": {"value": res["value"], "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
@@ -304,25 +328,31 @@ def bench_ours(args, world, rank, local):
     value = replica_value(cells, args.steps, ms, world)
     diag = s.analysis()
 
-    # dominant kernel: the S2/S3 stage kernel (two of four stages)
-    k_ms, k_n = prof["stage_s23"]
+    # dominant kernel: the stage kind with the largest share of the live step
+    # time (S2/S3 run as two launches of one kernel)
     peak, peak_kind = measured_peaks()
-    alg_bytes = STAGE_S23_PASSES * 8 * esize * cells
-    moved_bytes = STAGE_S23_MOVED_PASSES * 8 * esize * cells
+    dom = max(STAGE_PASSES, key=lambda k: prof[k][0])
+    k_ms, k_n = prof[dom]
+    alg_bytes = STAGE_PASSES[dom] * 8 * esize * cells
     launch_s = k_ms / k_n / 1e3 if k_n else None
     achieved = alg_bytes / launch_s / 1e9 if k_n else None
     step_gbs = BYTES_PER_CELL_STEP[dtype] * cells / (ms_per_step / 1e3) / 1e9
     step_moved_gbs = MOVED_BYTES_PER_CELL_STEP[dtype] * cells / (ms_per_step / 1e3) / 1e9
     total_prof = sum(v[0] for v in prof.values()) or 1.0
+    stages = {}
+    for k in STAGE_PASSES:
+        ms_k, n_k = prof[k]
+        if n_k:
+            b = STAGE_PASSES[k] * 8 * esize * cells
+            stages[STAGE_NAMES[k]] = {"passes": STAGE_PASSES[k], "mean_launch_ms": ms_k / n_k,
+                                      "gbs": b / (ms_k / n_k / 1e3) / 1e9, "frac": b / (ms_k / n_k / 1e3) / 1e9 / peak}
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak if achieved else None,
-                "traffic": traffic_per_launch("stage_s23_%s_%d_%d" % (dtype, nx, nv)),
+                "traffic": traffic_per_launch("%s_%s_%d_%d" % (dom, dtype, nx, nv)),
                 "step_traffic": step_traffic(dtype, nx, nv),
-                "kernel": "stage S2/S3 (%s)" % ("x-march" if prof["moment_finalize"][1] else "direct"),
+                "kernel": "stage %s (%s)" % (STAGE_NAMES[dom], "x-march" if prof["moment_finalize"][1] else "direct"),
                 "algorithmic_bytes_per_launch": alg_bytes,
-                "moved_bytes_per_launch": moved_bytes,
-                "moved_gbs": moved_bytes / launch_s / 1e9 if k_n else None,
-                "moved_frac": moved_bytes / launch_s / 1e9 / peak if k_n else None,
+                "per_stage": stages,
                 "mean_launch_ms": k_ms / k_n if k_n else None,
                 "peak_source": "%s (MEASURED_PEAKS.json hbm_gbs)" % peak_kind if peak_kind == "measured"
                 else "fallback 6.65 TB/s",
@@ -364,7 +394,8 @@ def bench_ours(args, world, rank, local):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
-            cpu = cpu_baseline_obj(run_cpu(args.cpu_sample, args.nn, 20, 1, budget=args.cpu_seconds))
+            cpu = cpu_baseline_obj(run_cpu(args.cpu_sample, args.nn, 20, 1, budget=args.cpu_seconds),
+                                   None if args.no_cpu_1t else one_thread_cpu(args))
         except Exception as ex:  # report, do not fail the GPU number
             cpu = {"value": None, "error": str(ex)[:200]}
 
@@ -525,6 +556,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-sample", type=int, default=128)
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    ap.add_argument("--cpu-seconds-1t", type=float, default=12.0, help="time budget of the one-thread CPU figure")
+    ap.add_argument("--no-cpu-1t", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the FP32, batch and serving sections")
     ap.add_argument("--batch-steps", type=int, default=20)
     ap.add_argument("--serve-requests", type=int, default=64)

@@ -229,14 +229,17 @@ int nuosc_get_profile(nuosc_handle *h, double *ms, long long *launches, int nkin
  * states laid out like the library's registers, [8 fields][nx][nz][nv_stride]
  * of double (NUOSC_FP64) or float (NUOSC_FP32), padding velocities zero, and
  * the quadrature arrays (nv_stride doubles each, zero in the padding).  The
- * call computes out = L(in), the calRHS of the reference, on `stream` and
- * allocates nothing: the per-cell velocity moments it needs go to a
- * file-scope device array of NUOSC_NOALLOC_MAX_CELLS * 12 doubles (6 MiB),
- * which every GPU that loads the library holds until the process exits.
- *   - grids with nx*nz > NUOSC_NOALLOC_MAX_CELLS are rejected (NUOSC_ERR_INVALID);
- *   - the first call on a device looks up the array's device address
- *     (cudaGetSymbolAddress) with that device current; make that first call
- *     before any stream capture begins;
+ * call computes out = L(in), the same right-hand side nuosc_calrhs computes
+ * on a handle's registers, on `stream` and allocates nothing: the per-cell
+ * velocity moments it needs go to a file-scope device array of
+ * NUOSC_NOALLOC_MAX_CELLS * 12 doubles (6 MiB), which every GPU that loads
+ * the library holds until the process exits.
+ *   - grids with nx*nz > NUOSC_NOALLOC_MAX_CELLS, dx or dz <= 0 and
+ *     non-finite coefficients are rejected (NUOSC_ERR_INVALID);
+ *   - the first call in a CUDA context (the device's primary context, or a
+ *     caller's own) looks up the array's device address in that context
+ *     (cudaGetSymbolAddress) with its device current, and caches it per
+ *     context; make that first call before any stream capture begins;
  *   - all calls share the one array and it keeps the last call's moments;
  *     each call rewrites every entry it reads, so nothing needs clearing, but
  *     calls that overlap on the GPU (e.g. on two streams at once) race on it.

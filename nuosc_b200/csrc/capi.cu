@@ -9,12 +9,16 @@
 //   S3: k3 = L(Yb) ; A = A + dt/3 k3 ; Ya = U + dt   k3
 //   S4: k4 = L(Ya) ; U = A + dt/6 k4
 // which is U + dt/6 (k1 + 2k2 + 2k3 + k4), the reference's update, with
-// 16 state passes per step instead of the reference's 4 calRHS + 6 vectorize.
-// On the TMA path S1 stores only Ya, and S2 forms A1 = U + dt/6 k1 as
-// U + (Ya - U)/3 from the U it reads and its stencil input Ya:
-//   S1: Ya = U + dt/2 k1                                     2 passes
-//   S2: A = U + (Ya - U)/3 + dt/3 k2 ; Yb = U + dt/2 k2     4
-// 14 state passes per step.
+// 16 state passes per step instead of the reference's 4 calRHS + 6 vectorize
+// (the direct and cp.async paths).  The TMA path keeps no accumulator: each
+// dt*k_s of the first three stages is the difference of a stage input and U,
+// so the last stage rebuilds the sum from them (registers U = v_stat,
+// Y2 = v_pre, Y3 = v_cor, Y4 = v_rhs):
+//   S1: k1 = L(U)  ; Y2 = U + dt/2 k1                        2 passes
+//   S2: k2 = L(Y2) ; Y3 = U + dt/2 k2                        3
+//   S3: k3 = L(Y3) ; Y4 = U + dt   k3                        3
+//   S4: k4 = L(Y4) ; U = U + [(Y2-U) + 2(Y3-U) + (Y4-U)]/3 + dt/6 k4   5
+// 13 state passes per step.
 #include "../../include/nuosc_b200.h"
 #include "internal.cuh"
 
@@ -257,8 +261,9 @@ int prof_kind(int mode) {
     case MODE_S1: return 0;
     case MODE_S1Y: return 0;
     case MODE_S23: return 1;
-    case MODE_S2: return 1;
+    case MODE_SY: return 1;
     case MODE_S4: return 2;
+    case MODE_S4F: return 2;
     default: return 3;
     }
 }
@@ -296,11 +301,12 @@ int run_stage_direct(nuosc_handle *h, int mode, int in, int u, int acc_src, int 
 // one RK4 stage in the x-march path (moments of the stage output fused)
 template <typename T>
 int run_stage_xmarch(nuosc_handle *h, bool tma, const XTile &tile, int mode, int in, int u, int acc_src, int acc_dst,
-                     int y_dst, double cA, double cY) {
+                     int y_dst, double cA, double cY, int w = -1) {
     StageArgs<T> a{};
     a.in = (const T *)h->reg[in];
     a.u = u >= 0 ? (const T *)h->reg[u] : nullptr;
     a.acc_src = acc_src >= 0 ? (const T *)h->reg[acc_src] : nullptr;
+    a.w = w >= 0 ? (const T *)h->reg[w] : nullptr;
     a.acc_dst = acc_dst >= 0 ? (T *)h->reg[acc_dst] : nullptr;
     a.y_dst = y_dst >= 0 ? (T *)h->reg[y_dst] : nullptr;
     a.mom_in = h->d_mom;
@@ -374,15 +380,16 @@ int step_impl(nuosc_handle *h, int nsteps) {
     }
     for (int n = 0; n < nsteps; ++n) {
         int rc;
-        if (xm) {
-            if ((rc = run_stage_xmarch<T>(h, tma, tile, tma ? MODE_S1Y : MODE_S1, 0, -1, -1, tma ? -1 : 1, 2, dt / 6.0,
-                                          0.5 * dt)))
-                return rc;
-            if (tma) {  // 14-pass sequence: S1 stores only Ya, S2 forms A1 from U and Ya
-                if ((rc = run_stage_xmarch<T>(h, tma, tile, MODE_S2, 2, 0, -1, 1, 3, dt / 3.0, 0.5 * dt))) return rc;
-            } else {
-                if ((rc = run_stage_xmarch<T>(h, tma, tile, MODE_S23, 2, 0, 1, 1, 3, dt / 3.0, 0.5 * dt))) return rc;
-            }
+        if (tma) {
+            // 13-pass sequence (registers 0 U, 2 Y2, 3 Y3, 1 Y4): no accumulator;
+            // the last stage recovers dt k1..dt k3 from Y2, Y3, Y4 and U
+            if ((rc = run_stage_xmarch<T>(h, tma, tile, MODE_S1Y, 0, -1, -1, -1, 2, 0.0, 0.5 * dt))) return rc;
+            if ((rc = run_stage_xmarch<T>(h, tma, tile, MODE_SY, 2, 0, -1, -1, 3, 0.0, 0.5 * dt))) return rc;
+            if ((rc = run_stage_xmarch<T>(h, tma, tile, MODE_SY, 3, 0, -1, -1, 1, 0.0, dt))) return rc;
+            if ((rc = run_stage_xmarch<T>(h, tma, tile, MODE_S4F, 1, 0, 2, 0, -1, dt / 6.0, 0.0, 3))) return rc;
+        } else if (xm) {
+            if ((rc = run_stage_xmarch<T>(h, tma, tile, MODE_S1, 0, -1, -1, 1, 2, dt / 6.0, 0.5 * dt))) return rc;
+            if ((rc = run_stage_xmarch<T>(h, tma, tile, MODE_S23, 2, 0, 1, 1, 3, dt / 3.0, 0.5 * dt))) return rc;
             if ((rc = run_stage_xmarch<T>(h, tma, tile, MODE_S23, 3, 0, 1, 1, 2, dt / 3.0, dt))) return rc;
             if ((rc = run_stage_xmarch<T>(h, tma, tile, MODE_S4, 2, -1, 1, 0, -1, dt / 6.0, 0.0))) return rc;
         } else {
@@ -1070,16 +1077,17 @@ struct nuosc_batch {
 
 namespace {
 
-// RK4 stage k of step_impl's x-march sequence: (mode, in, u, acc_src, acc_dst,
-// y_dst) with cA = dt / da and cY = fy * dt, the same expressions as step_impl
+// RK4 stage k of step_impl's 13-pass TMA sequence: (mode, in, u, acc_src, w,
+// acc_dst, y_dst) with cA = dt / da (da 0: cA = 0) and cY = fy * dt, the same
+// expressions as step_impl
 struct StageSpec {
-    int mode, in, u, acc_src, acc_dst, y_dst;
+    int mode, in, u, acc_src, w, acc_dst, y_dst;
     double da, fy;
 };
-constexpr StageSpec kStages[4] = {{MODE_S1Y, 0, -1, -1, -1, 2, 6.0, 0.5},
-                                  {MODE_S2, 2, 0, -1, 1, 3, 3.0, 0.5},
-                                  {MODE_S23, 3, 0, 1, 1, 2, 3.0, 1.0},
-                                  {MODE_S4, 2, -1, 1, 0, -1, 6.0, 0.0}};
+constexpr StageSpec kStages[4] = {{MODE_S1Y, 0, -1, -1, -1, -1, 2, 0.0, 0.5},
+                                  {MODE_SY, 2, 0, -1, -1, -1, 3, 0.0, 0.5},
+                                  {MODE_SY, 3, 0, -1, -1, -1, 1, 0.0, 1.0},
+                                  {MODE_S4F, 1, 0, 2, 3, 0, -1, 6.0, 0.0}};
 
 std::vector<double> batch_signature(const nuosc_batch *b) {
     std::vector<double> s;
@@ -1163,6 +1171,7 @@ int batch_build(nuosc_batch *b) {
             a.in = (const T *)h->reg[sp.in];
             a.u = sp.u >= 0 ? (const T *)h->reg[sp.u] : nullptr;
             a.acc_src = sp.acc_src >= 0 ? (const T *)h->reg[sp.acc_src] : nullptr;
+            a.w = sp.w >= 0 ? (const T *)h->reg[sp.w] : nullptr;
             a.acc_dst = sp.acc_dst >= 0 ? (T *)h->reg[sp.acc_dst] : nullptr;
             a.y_dst = sp.y_dst >= 0 ? (T *)h->reg[sp.y_dst] : nullptr;
             a.mom_in = h->d_mom;
@@ -1170,7 +1179,7 @@ int batch_build(nuosc_batch *b) {
             a.q = h->quad();
             a.g = h->g;
             a.c = h->coeffs();
-            a.cA = h->dt / sp.da;
+            a.cA = sp.da > 0.0 ? h->dt / sp.da : 0.0;
             a.cY = sp.fy == 1.0 ? h->dt : sp.fy * h->dt;
             a.status = h->d_status;
             ti = xtma_batch_fill<T>(&host[((size_t)k * n + i) * b->item_bytes], a, b->ko6, b->tz, lxs[i]);

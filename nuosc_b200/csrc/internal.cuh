@@ -44,17 +44,23 @@ struct Quad {
 //   MODE_S1  : acc_dst = in + cA*k ;          y_dst = in + cY*k
 //   MODE_S23 : acc_dst = acc_src + cA*k ;     y_dst = u  + cY*k
 //   MODE_S4  : acc_dst = acc_src + cA*k
-// and the 14-pass sequence of the TMA path, which never stores A1:
+// (the classic 16-pass sequence of the direct and cp.async paths), and the
+// 13-pass sequence of the TMA path, which keeps no accumulator register:
 //   MODE_S1Y : y_dst = in + cY*k                       (Y2 = U + dt/2 k1)
-//   MODE_S2  : acc_dst = (u + (in - u)/3) + cA*k ;    y_dst = u + cY*k
-// In S2, in = Y2 = U + dt/2 k1, so u + (in - u)/3 = U + dt/6 k1 = A1.
-enum StageMode { MODE_RHS = 0, MODE_S1 = 1, MODE_S23 = 2, MODE_S4 = 3, MODE_S2 = 4, MODE_S1Y = 5 };
+//   MODE_SY  : y_dst = u + cY*k                        (Y3 = U + dt/2 k2, Y4 = U + dt k3)
+//   MODE_S4F : acc_dst = u + ((acc_src - u) + 2 (w - u) + (in - u))/3 + cA*k
+// In S4F, in = Y4, acc_src = Y2, w = Y3 and cA = dt/6, so the update is
+// U + dt/6 (k1 + 2 k2 + 2 k3 + k4) with each dt*k_s recovered as a
+// difference Y_s+1 - U of nearby values (exact by Sterbenz where they lie
+// within a factor 2).
+enum StageMode { MODE_RHS = 0, MODE_S1 = 1, MODE_S23 = 2, MODE_S4 = 3, MODE_S1Y = 5, MODE_SY = 6, MODE_S4F = 7 };
 
 template <typename T>
 struct StageArgs {
     const T *in;
     const T *u;
     const T *acc_src;
+    const T *w;            // MODE_S4F: the third pointwise input (Y3)
     T *acc_dst;
     T *y_dst;
     const double *mom_in;  // [ncell][12] moments of `in`

@@ -16,10 +16,14 @@
 #include "../../include/nuosc_b200.h"
 #include "internal.cuh"
 
+#include <cuda.h>
+
 #include <cmath>
 #include <cstdio>
 #include <mutex>
 #include <string>
+#include <utility>
+#include <vector>
 
 namespace nuosc {
 namespace {
@@ -27,11 +31,43 @@ namespace {
 // 12 moments per cell for at most NUOSC_NOALLOC_MAX_CELLS cells
 static __device__ __align__(256) double g_noalloc_moments[(size_t)NUOSC_NOALLOC_MAX_CELLS * NMOM];
 
-constexpr int kMaxDevices = 64;
+// The array's device address belongs to a CUDA context: the primary context
+// of a device gets a new one after cudaDeviceReset, and a host framework that
+// makes its own context on the same device gets its own copy of the array.
+// So the address is looked up once per context (keyed by the context's
+// process-unique id, cuCtxGetId) and cached.
+using CtxGetCurrentFn = CUresult (*)(CUcontext *);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long *);
+constexpr size_t kMaxContexts = 64;
 std::mutex g_mu;
-double *g_scratch[kMaxDevices] = {nullptr};
+std::vector<std::pair<unsigned long long, double *>> g_scratch;  // (context id, array address)
 
 int fail(int code, const char *msg) { return set_last_error(code, msg); }
+
+template <typename F>
+F driver_fn(const char *name) {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint(name, &p, cudaEnableDefault, &q) != cudaSuccess || q != cudaDriverEntryPointSuccess)
+        return nullptr;
+    return (F)p;
+}
+
+// id of the calling thread's current context; the runtime's primary context
+// of the current device is made current first when none is
+bool current_context_id(unsigned long long *id) {
+    static const CtxGetCurrentFn get_current = driver_fn<CtxGetCurrentFn>("cuCtxGetCurrent");
+    static const CtxGetIdFn get_id = driver_fn<CtxGetIdFn>("cuCtxGetId");
+    if (!get_current || !get_id) return false;
+    CUcontext ctx = nullptr;
+    if (get_current(&ctx) != CUDA_SUCCESS) return false;
+    if (!ctx) {
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess || cudaSetDevice(dev) != cudaSuccess) return false;
+        if (get_current(&ctx) != CUDA_SUCCESS || !ctx) return false;
+    }
+    return get_id(ctx, id) == CUDA_SUCCESS;
+}
 
 }  // namespace
 }  // namespace nuosc
@@ -42,6 +78,9 @@ extern "C" int nuosc_calrhs_noalloc(const nuosc_rhs_desc *d, const void *in, voi
     if (!d || !in || !out) return fail(NUOSC_ERR_INVALID, "calrhs_noalloc: null argument");
     if (d->nx < 4 || d->nz < 4 || d->nv < 1 || d->nv_stride < d->nv)
         return fail(NUOSC_ERR_INVALID, "calrhs_noalloc: bad geometry");
+    if (!(d->dx > 0.0) || !(d->dz > 0.0) || !std::isfinite(d->dx) || !std::isfinite(d->dz) || !std::isfinite(d->ko) ||
+        !std::isfinite(d->mu) || !std::isfinite(d->pmo))
+        return fail(NUOSC_ERR_INVALID, "calrhs_noalloc: bad spacing or coefficient (dx, dz > 0; ko, mu, pmo finite)");
     if ((long long)d->nx * d->nz > NUOSC_NOALLOC_MAX_CELLS)
         return fail(NUOSC_ERR_INVALID,
                     "calrhs_noalloc: nx*nz exceeds NUOSC_NOALLOC_MAX_CELLS (65536) cells of device scratch");
@@ -50,20 +89,23 @@ extern "C" int nuosc_calrhs_noalloc(const nuosc_rhs_desc *d, const void *in, voi
     if (d->ko_order != 6 && d->ko_order != 4) return fail(NUOSC_ERR_INVALID, "calrhs_noalloc: ko_order must be 6 or 4");
     if (!d->vx || !d->vy || !d->vz || !d->vw) return fail(NUOSC_ERR_INVALID, "calrhs_noalloc: null quadrature");
 
-    // device address of the scratch array: looked up once per device, with that device current
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices)
-        return fail(NUOSC_ERR_CUDA, "calrhs_noalloc: no current CUDA device");
+    // device address of the scratch array in the current context: looked up
+    // on the first call in that context (with its device current) and cached
+    unsigned long long ctx = 0;
+    if (!current_context_id(&ctx)) return fail(NUOSC_ERR_CUDA, "calrhs_noalloc: no current CUDA context");
     double *scratch = nullptr;
     {
         std::lock_guard<std::mutex> lock(g_mu);
-        if (!g_scratch[dev]) {
+        for (const auto &e : g_scratch)
+            if (e.first == ctx) scratch = e.second;
+        if (!scratch) {
             void *p = nullptr;
             const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_moments);
             if (e != cudaSuccess) return fail(NUOSC_ERR_CUDA, "calrhs_noalloc: cudaGetSymbolAddress failed");
-            g_scratch[dev] = (double *)p;
+            if (g_scratch.size() >= kMaxContexts) g_scratch.clear();  // entries of contexts that are gone
+            g_scratch.emplace_back(ctx, (double *)p);
+            scratch = (double *)p;
         }
-        scratch = g_scratch[dev];
     }
 
     Geom g;

@@ -70,20 +70,16 @@ __device__ __forceinline__ void tail_point(const StageArgs<T> &a, const long lon
         for (int f = 0; f < 4; ++f) {
             const long long idx = o + f * g.fs;
             if (MODE == MODE_S1Y) {
-                outm[f] = c4[f] + cY * kv[f];
+                outm[f] = c4[f] + cY * kv[f];  // Y2
                 a.y_dst[idx] = outm[f];
-            } else if (MODE == MODE_S23) {
-                a.acc_dst[idx] = a.acc_src[idx] + cA * kv[f];
-                outm[f] = a.u[idx] + cY * kv[f];
-                a.y_dst[idx] = outm[f];
-            } else if (MODE == MODE_S2) {
-                const T u = a.u[idx];
-                const T a1 = u + (c4[f] - u) * T(1.0 / 3.0);  // A1 = U + dt/6 k1 from Y2 = U + dt/2 k1
-                a.acc_dst[idx] = a1 + cA * kv[f];
-                outm[f] = u + cY * kv[f];
+            } else if (MODE == MODE_SY) {
+                outm[f] = a.u[idx] + cY * kv[f];  // Y3, Y4
                 a.y_dst[idx] = outm[f];
             } else {
-                outm[f] = a.acc_src[idx] + cA * kv[f];
+                // U + [(Y2 - U) + 2 (Y3 - U) + (Y4 - U)]/3 + dt/6 k4, as the TMA kernel
+                const T u = a.u[idx];
+                const T p = fma(T(2), a.w[idx] - u, a.acc_src[idx] - u);
+                outm[f] = u + fma(p + (c4[f] - u), T(1.0 / 3.0), cA * kv[f]);
                 a.acc_dst[idx] = outm[f];
             }
         }
@@ -150,9 +146,8 @@ cudaError_t launch_tail_ko(const StageArgs<T> &a, int mode, int v0, int twp, int
     const unsigned blocks = (unsigned)((threads + TAIL_BLOCK - 1) / TAIL_BLOCK);
     switch (mode) {
     case MODE_S1Y: k_stage_tail<T, KO6, MODE_S1Y><<<blocks, TAIL_BLOCK, 0, s>>>(a, v0, twp, nvb); break;
-    case MODE_S23: k_stage_tail<T, KO6, MODE_S23><<<blocks, TAIL_BLOCK, 0, s>>>(a, v0, twp, nvb); break;
-    case MODE_S2: k_stage_tail<T, KO6, MODE_S2><<<blocks, TAIL_BLOCK, 0, s>>>(a, v0, twp, nvb); break;
-    case MODE_S4: k_stage_tail<T, KO6, MODE_S4><<<blocks, TAIL_BLOCK, 0, s>>>(a, v0, twp, nvb); break;
+    case MODE_SY: k_stage_tail<T, KO6, MODE_SY><<<blocks, TAIL_BLOCK, 0, s>>>(a, v0, twp, nvb); break;
+    case MODE_S4F: k_stage_tail<T, KO6, MODE_S4F><<<blocks, TAIL_BLOCK, 0, s>>>(a, v0, twp, nvb); break;
     default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
@@ -164,9 +159,8 @@ cudaError_t launch_tail_batch_ko(const TailItem<T> *items, const long long *star
     const unsigned blocks = (unsigned)((total + TAIL_BLOCK - 1) / TAIL_BLOCK);
     switch (mode) {
     case MODE_S1Y: k_stage_tail_batch<T, KO6, MODE_S1Y><<<blocks, TAIL_BLOCK, 0, s>>>(items, starts, n, total); break;
-    case MODE_S23: k_stage_tail_batch<T, KO6, MODE_S23><<<blocks, TAIL_BLOCK, 0, s>>>(items, starts, n, total); break;
-    case MODE_S2: k_stage_tail_batch<T, KO6, MODE_S2><<<blocks, TAIL_BLOCK, 0, s>>>(items, starts, n, total); break;
-    case MODE_S4: k_stage_tail_batch<T, KO6, MODE_S4><<<blocks, TAIL_BLOCK, 0, s>>>(items, starts, n, total); break;
+    case MODE_SY: k_stage_tail_batch<T, KO6, MODE_SY><<<blocks, TAIL_BLOCK, 0, s>>>(items, starts, n, total); break;
+    case MODE_S4F: k_stage_tail_batch<T, KO6, MODE_S4F><<<blocks, TAIL_BLOCK, 0, s>>>(items, starts, n, total); break;
     default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();

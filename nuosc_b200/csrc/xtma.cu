@@ -15,8 +15,8 @@
 //     march: a warp waits only on full barriers and releases a slot after its
 //     last use by arriving on the slot's "empty" mbarrier; the issuing lane
 //     waits on "empty" before refilling a slot;
-//   * the pointwise inputs of the epilogue (U in S2, U and A in S3, A in S4;
-//     none in S1) are plain coalesced loads issued at the top of each plane,
+//   * the pointwise inputs of the epilogue (U in S2 and S3, U, Y2 and Y3 in
+//     S4; none in S1) are plain coalesced loads issued at the top of each plane,
 //     before the waits and the stencil; the issuing lane prefetches their TZ
 //     rows into L2 two planes ahead with a tensor prefetch
 //     (cp.async.bulk.prefetch.tensor), so the loads find them in L2;
@@ -66,7 +66,8 @@ struct __align__(64) TmaMaps {
     CUtensorMap tz;   // TZ rows (middle piece of a box wrapped at both ends)
     CUtensorMap r;    // R rows (wrapped halo)
     CUtensorMap pu;   // TZ rows of the stage's U register (L2 prefetch of the pointwise input)
-    CUtensorMap pa;   // TZ rows of the stage's accumulator input A (L2 prefetch)
+    CUtensorMap pa;   // TZ rows of the final stage's Y2 input (acc_src; L2 prefetch)
+    CUtensorMap pw;   // TZ rows of the final stage's Y3 input (w; L2 prefetch)
 };
 
 __device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
@@ -219,19 +220,19 @@ constexpr int tma_ctas_per_sm() {
 }
 
 // Ring geometry of one march.  Boxes are issued D planes ahead of their
-// front use: 3 with 16-row tiles (one CTA per SM, 9 slots of 24 KB at R = 3),
+// front use: 3 with 16-row tiles (one CTA per SM, 8 slots of 24 KB at R = 3),
 // 2 with 8-row tiles (two CTAs per SM share the 228 KB).  The pointwise
-// inputs of the epilogue (U in S2/S3, A in S3/S4) stay plain per-thread loads,
-// but thread 0 prefetches their TZ rows of plane x + PFD into L2 with one
-// tensor prefetch each, so those loads hit L2: measured 3 % faster per step
-// than without (PFD 1 and 3 equal within noise, 6 slower), and faster than
-// staging A or U through shared memory, which costs ring depth.
+// inputs of the epilogue (U in S2/S3/S4, Y2 and Y3 in S4) stay plain
+// per-thread loads, but thread 0 prefetches their TZ rows of plane x + PFD
+// into L2 with one tensor prefetch each, so those loads hit L2: measured 3 %
+// faster per step than without (PFD 1 and 3 equal within noise, 6 slower),
+// and faster than staging them through shared memory, which costs ring depth.
 template <typename T, int R, int MODE, int TZ>
 struct MarchCfg {
     static constexpr int D = TZ == 16 ? 3 : 2;  // boxes issued ahead of their first use
     static constexpr int PFD = 2;                 // L2 prefetch distance of the pointwise inputs, planes
-    static constexpr bool PU = MODE == MODE_S23 || MODE == MODE_S2;  // reads U pointwise
-    static constexpr bool PA = MODE == MODE_S23 || MODE == MODE_S4;  // reads A pointwise
+    static constexpr bool PU = MODE == MODE_SY || MODE == MODE_S4F;  // reads U pointwise
+    static constexpr bool PA = MODE == MODE_S4F;                     // reads Y2 (acc_src) and Y3 (w) pointwise
     static constexpr int NS = R + D + 2;  // a box lives from its front use to its centre use, plus slack
     static constexpr size_t ring = (size_t)NS * Slot<T, TZ, R>::bytes;
     static constexpr size_t smem = ring + 2 * NS * 8;  // box ring | mbarriers
@@ -322,7 +323,10 @@ __device__ __forceinline__ bool xtma_march(const TmaMaps *const &mp, const Stage
         if ((CF::PU || CF::PA) && i < nplanes) {
             const TmaMaps &maps = *rd<SA>(mp);
             if (CF::PU) tma_prefetch_4d(&maps.pu, vb * VB, 4 * half, z0, xs + i);
-            if (CF::PA) tma_prefetch_4d(&maps.pa, vb * VB, 4 * half, z0, xs + i);
+            if (CF::PA) {
+                tma_prefetch_4d(&maps.pa, vb * VB, 4 * half, z0, xs + i);
+                tma_prefetch_4d(&maps.pw, vb * VB, 4 * half, z0, xs + i);
+            }
         }
     };
 
@@ -408,6 +412,8 @@ __device__ __forceinline__ bool xtma_march(const TmaMaps *const &mp, const Stage
         }
         const int x = xs + i;
         const long long oc = hoff + (long long)x * P + own;
+        // uin: U; ain (S4F): (Y2 - U) + 2 (Y3 - U), formed at once so that
+        // only two values per field stay live across the stencil
         T uin[4][NP], ain[4][NP];
         {
             // pointwise epilogue inputs first (they are not in the ring; L2 hits
@@ -415,13 +421,20 @@ __device__ __forceinline__ bool xtma_march(const TmaMaps *const &mp, const Stage
             constexpr bool LU = CF::PU, LA = CF::PA;
             const T *up = LU ? rd<SA>(a.u) + oc : nullptr;
             const T *ap = LA ? rd<SA>(a.acc_src) + oc : nullptr;
+            const T *wp = LA ? rd<SA>(a.w) + oc : nullptr;
 #pragma unroll
             for (int f = 0; f < 4; ++f) {
 #pragma unroll
                 for (int p = 0; p < NP; ++p) uin[f][p] = ain[f][p] = T(0);
                 if (vact) {
                     if (LU) ldv<T, NP>(up + f * fs, uin[f]);
-                    if (LA) ldv<T, NP>(ap + f * fs, ain[f]);
+                    if (LA) {
+                        T y2[NP], y3[NP];
+                        ldv<T, NP>(ap + f * fs, y2);
+                        ldv<T, NP>(wp + f * fs, y3);
+#pragma unroll
+                        for (int p = 0; p < NP; ++p) ain[f][p] = fma(T(2), y3[p] - uin[f][p], y2[p] - uin[f][p]);
+                    }
                 }
             }
         }
@@ -495,33 +508,20 @@ __device__ __forceinline__ bool xtma_march(const TmaMaps *const &mp, const Stage
             for (int f = 0; f < 4; ++f) {
                 if (MODE == MODE_S1Y) {
                     outm[f][p] = cen[f] + cY * kk[f];  // Y2
-                } else if (MODE == MODE_S23) {
-                    ain[f][p] = ain[f][p] + cA * kk[f];
-                    outm[f][p] = uin[f][p] + cY * kk[f];
-                } else if (MODE == MODE_S2) {
-                    const T u = uin[f][p];
-                    const T a1 = u + (cen[f] - u) * T(1.0 / 3.0);  // A1 = U + dt/6 k1 from Y2 = U + dt/2 k1
-                    ain[f][p] = a1 + cA * kk[f];
-                    outm[f][p] = u + cY * kk[f];
+                } else if (MODE == MODE_SY) {
+                    outm[f][p] = uin[f][p] + cY * kk[f];  // Y3, Y4
                 } else {
-                    outm[f][p] = ain[f][p] + cA * kk[f];
+                    // U + [(Y2 - U) + 2 (Y3 - U) + (Y4 - U)]/3 + dt/6 k4: the small
+                    // increments are summed first, U is added last
+                    const T u = uin[f][p];
+                    outm[f][p] = u + fma(ain[f][p] + (cen[f] - u), T(1.0 / 3.0), cA * kk[f]);
                 }
             }
         }
         if (vact) {
-            T *dp = MODE != MODE_S1Y ? rd<SA>(a.acc_dst) + oc : nullptr;
-            T *yp = MODE != MODE_S4 ? rd<SA>(a.y_dst) + oc : nullptr;
+            T *dp = (MODE == MODE_S4F ? rd<SA>(a.acc_dst) : rd<SA>(a.y_dst)) + oc;
 #pragma unroll
-            for (int f = 0; f < 4; ++f) {
-                if (MODE == MODE_S1Y) {
-                    stv<T, NP>(yp + f * fs, outm[f]);
-                } else if (MODE == MODE_S23 || MODE == MODE_S2) {
-                    stv<T, NP>(dp + f * fs, ain[f]);
-                    stv<T, NP>(yp + f * fs, outm[f]);
-                } else {
-                    stv<T, NP>(dp + f * fs, outm[f]);
-                }
-            }
+            for (int f = 0; f < 4; ++f) stv<T, NP>(dp + f * fs, outm[f]);
         }
         // velocity-moment partials of the written state (nuosc_class.cpp:69-71).
         // FP64: products and the warp's reduce-scatter in double.  FP32 (two
@@ -671,7 +671,10 @@ __global__ void __launch_bounds__(32 * TZ, tma_ctas_per_sm<T, TZ>())
                 tensormap_acquire(&e.maps.tz);
                 tensormap_acquire(&e.maps.r);
                 if (MarchCfg<T, R, MODE, TZ>::PU) tensormap_acquire(&e.maps.pu);
-                if (MarchCfg<T, R, MODE, TZ>::PA) tensormap_acquire(&e.maps.pa);
+                if (MarchCfg<T, R, MODE, TZ>::PA) {
+                    tensormap_acquire(&e.maps.pa);
+                    tensormap_acquire(&e.maps.pw);
+                }
             }
         }
         __syncthreads();
@@ -758,9 +761,11 @@ template <typename T>
 bool make_maps(TmaMaps *m, const StageArgs<T> &a, int tz, int r) {
     memset((void *)&m->pu, 0, sizeof m->pu);
     memset((void *)&m->pa, 0, sizeof m->pa);
+    memset((void *)&m->pw, 0, sizeof m->pw);
     return make_map<T>(&m->zr, a.in, a.g, tz + 2 * r) && make_map<T>(&m->tzr, a.in, a.g, tz + r) &&
            make_map<T>(&m->tz, a.in, a.g, tz) && make_map<T>(&m->r, a.in, a.g, r) &&
-           (!a.u || make_map<T>(&m->pu, a.u, a.g, tz)) && (!a.acc_src || make_map<T>(&m->pa, a.acc_src, a.g, tz));
+           (!a.u || make_map<T>(&m->pu, a.u, a.g, tz)) && (!a.acc_src || make_map<T>(&m->pa, a.acc_src, a.g, tz)) &&
+           (!a.w || make_map<T>(&m->pw, a.w, a.g, tz));
 }
 
 template <typename T, int R, int MODE, int TZ, bool VAC>
@@ -788,9 +793,8 @@ template <typename T, int R, int TZ, bool VAC>
 cudaError_t launch_tm(const StageArgs<T> &a, int mode, XTile t, cudaStream_t s) {
     switch (mode) {
     case MODE_S1Y: return launch_t<T, R, MODE_S1Y, TZ, VAC>(a, t, s);
-    case MODE_S23: return launch_t<T, R, MODE_S23, TZ, VAC>(a, t, s);
-    case MODE_S2: return launch_t<T, R, MODE_S2, TZ, VAC>(a, t, s);
-    case MODE_S4: return launch_t<T, R, MODE_S4, TZ, VAC>(a, t, s);
+    case MODE_SY: return launch_t<T, R, MODE_SY, TZ, VAC>(a, t, s);
+    case MODE_S4F: return launch_t<T, R, MODE_S4F, TZ, VAC>(a, t, s);
     default: return cudaErrorInvalidValue;
     }
 }
@@ -832,10 +836,9 @@ auto batch_dispatch(int mode, bool ko6, int tz, bool vac, Args... args) {
 #define NUOSC_BATCH_V(R, M, Z) (vac ? F<T, R, M, Z, true>::run(args...) : F<T, R, M, Z, false>::run(args...))
 #define NUOSC_BATCH_TZ(R, M) (tz == 16 ? NUOSC_BATCH_V(R, M, 16) : NUOSC_BATCH_V(R, M, 8))
 #define NUOSC_BATCH_MODE(R)                                                                                   \
-    (mode == MODE_S1Y   ? NUOSC_BATCH_TZ(R, MODE_S1Y)                                                         \
-     : mode == MODE_S2  ? NUOSC_BATCH_TZ(R, MODE_S2)                                                          \
-     : mode == MODE_S23 ? NUOSC_BATCH_TZ(R, MODE_S23)                                                         \
-                        : NUOSC_BATCH_TZ(R, MODE_S4))
+    (mode == MODE_S1Y ? NUOSC_BATCH_TZ(R, MODE_S1Y)                                                           \
+     : mode == MODE_SY ? NUOSC_BATCH_TZ(R, MODE_SY)                                                           \
+                       : NUOSC_BATCH_TZ(R, MODE_S4F))
     return ko6 ? NUOSC_BATCH_MODE(3) : NUOSC_BATCH_MODE(2);
 #undef NUOSC_BATCH_MODE
 #undef NUOSC_BATCH_TZ
@@ -886,8 +889,7 @@ long long xtma_batch_fill(void *item, const StageArgs<T> &a, bool ko6, int tz, i
 
 template <typename T>
 int xtma_batch_grid(int mode, bool ko6, int tz, bool vac, int device) {
-    if ((tz != 8 && tz != 16) || (mode != MODE_S1Y && mode != MODE_S2 && mode != MODE_S23 && mode != MODE_S4))
-        return -1;
+    if ((tz != 8 && tz != 16) || (mode != MODE_S1Y && mode != MODE_SY && mode != MODE_S4F)) return -1;
     return batch_dispatch<T, BatchGrid>(mode, ko6, tz, vac, device);
 }
 
@@ -895,8 +897,7 @@ template <typename T>
 cudaError_t launch_stage_xtma_batch(const void *items, const long long *starts, int n, long long ntiles,
                                     unsigned long long *counter, int mode, bool ko6, int tz, bool vac, int grid,
                                     cudaStream_t s) {
-    if ((tz != 8 && tz != 16) || (mode != MODE_S1Y && mode != MODE_S2 && mode != MODE_S23 && mode != MODE_S4) ||
-        n < 1 || grid < 1)
+    if ((tz != 8 && tz != 16) || (mode != MODE_S1Y && mode != MODE_SY && mode != MODE_S4F) || n < 1 || grid < 1)
         return cudaErrorInvalidValue;
     return batch_dispatch<T, BatchLaunch>(mode, ko6, tz, vac, items, starts, n, ntiles, counter, grid, s);
 }

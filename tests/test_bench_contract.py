@@ -56,9 +56,28 @@ def test_step_traffic_from_profiles():
     with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
         t = json.load(f)
     for dt in ("f64", "f32"):
-        want = sum(t["stage_%s_%s_1024_642" % (k, dt)] for k in ("s1", "s23", "s23", "s4"))
+        keys = ["stage_%s_%s_1024_642" % (k, dt) for k in ("s1", "s23", "s23", "s4")]
+        if not all(k in t for k in keys):
+            assert bench.step_traffic(dt, 1024, 642) is None
+            continue
+        want = sum(t[k] for k in keys)
         assert bench.step_traffic(dt, 1024, 642) == want
-        # within 10 % of the bytes the 14-pass step moves (896 / 448 B per cell-step)
+        # within 10 % of the bytes the 13-pass step moves (832 / 416 B per cell-step)
         moved = bench.MOVED_BYTES_PER_CELL_STEP[dt] * 1024 * 1024 * 642
         assert 1.0 <= want / moved < 1.1
     assert bench.step_traffic("f64", 512, 642) is None
+
+
+def test_reference_arm_names_its_sample():
+    """The reference arm's config names the sample it timed, not the full grid."""
+    env = dict(os.environ)
+    for k in ("WORLD_SIZE", "RANK", "LOCAL_RANK"):
+        env.pop(k, None)
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "2",
+                          "--warmup", "1", "--cpu-sample", "16", "--nn", "2", "--cpu-seconds-1t", "2"], env=env,
+                         stdout=subprocess.PIPE, stderr=subprocess.PIPE, check=True, timeout=600)
+    d = json.loads([l for l in out.stdout.decode().splitlines() if l.startswith("{")][0])
+    assert d["config"]["nx"] == 16 and d["config"]["nv"] == 42
+    assert "16x16 cells x 42 velocities sample" in d["config"]["workload"]
+    one = d["cpu_baseline"]["one_thread"]
+    assert one["cores"] == 1 and one["value"] > 0

@@ -365,3 +365,78 @@ def test_launch_count(nb):
     n0 = s.kernel_launches
     s.step_rk4(3)
     assert s.kernel_launches - n0 >= 3 * 4
+
+
+def _tma_solve(nb, p, ko_order, seed, steps, tile=None, **phys):
+    """Runs `steps` RK4 steps on the TMA x-march kernel, which must accept the
+    geometry (no silent fallback to another kernel)."""
+    s = make(nb, p, ko_order, kernel=nb.KERNEL_XTMA)
+    if tile is not None:
+        s.set_tile(*tile)
+    s.fillInitValue(1, seed=seed, **phys)
+    s.step_rk4(steps)
+    return s
+
+
+def _oracle_solve(p, ko_order, seed, steps, **phys):
+    x0, x1, dx, cfl, ko, mu, pmo, nn = p
+    o = po.Oracle(nn=int(nn), x0=x0, x1=x1, z0=x0, z1=x1, dx=dx, dz=dx, cfl=cfl, ko=ko, ko_order=ko_order, mu=mu,
+                  pmo=pmo)
+    o.fill_init(ipt=1, seed=seed, **phys)
+    o.step(steps)
+    return o
+
+
+HARD = dict(alpha=1.2, eps0=1e-3, sigma=1.0, lnue=0.6, lnueb=0.4)
+
+
+@pytest.mark.parametrize("pmo", [0.0, 0.3])
+def test_tma_fp64_642_velocities_against_oracle(nb, pmo):
+    """The production kernel configuration on a small grid: FP64, 642
+    velocities (nn = 8: 20 full 32-velocity blocks on the TMA kernel, 640-641
+    on the tail kernel), 16-row tiles with the tile table's 128-plane x
+    segments, 6th-difference KO; 32x32 cells, 10 steps, every field within
+    1e-12 of the oracle, with and without the vacuum term."""
+    p = box_params(32, 8, mu=1.0, pmo=pmo)
+    s = _tma_solve(nb, p, 6, 21, 10, **HARD)
+    assert s.get_tile()[0] == 16
+    o = _oracle_solve(p, 6, 21, 10, **HARD)
+    a, b = s.get_state(), o.get_state(0)
+    for f in range(8):
+        assert po.relerr(a[f], b[f]) < FP64_TOL, f
+    assert_diag_close(diag_vec(s.analysis()), o.analysis())
+    s.close()
+
+
+@pytest.mark.parametrize("tile", [(16, 32), (8, 7)])
+def test_tma_ko4_against_oracle(nb, tile):
+    """The TMA kernel with the 4th-difference KO (2 ghost cells, R = 2 queue)
+    on 32x32 cells x 162 velocities (the tail kernel runs 160-161), 16- and
+    8-row tiles, 10 steps against the oracle."""
+    p = box_params(32, 4, mu=1.3, pmo=0.2)
+    s = _tma_solve(nb, p, 4, 22, 10, tile=tile, **HARD)
+    assert s.get_tile() == tile
+    o = _oracle_solve(p, 4, 22, 10, **HARD)
+    a, b = s.get_state(), o.get_state(0)
+    for f in range(8):
+        assert po.relerr(a[f], b[f]) < FP64_TOL, f
+    s.close()
+
+
+def test_tma_ko4_ten_steps_match_reference_on_32_cells(nb):
+    """KO4 on the TMA kernel against the reference build's own 10-step state
+    (where the reference build is present; the oracle, pinned to it by the CPU
+    tests, otherwise)."""
+    p = box_params(32, 2)
+    s = _tma_solve(nb, p, 4, 9, 10, **PHYS)
+    a = s.get_state()
+    if po.ref_available(4):
+        r = po.RefSim(nn=2, x0=p[0], x1=p[1], z0=p[0], z1=p[1], dx=0.1, dz=0.1, cfl=0.4, ko=0.1, ko_order=4)
+        r.fill_init(ipt=1, seed=9, **PHYS)
+        r.step(10)
+        b = r.get_state(0)
+    else:
+        b = _oracle_solve(p, 4, 9, 10, **PHYS).get_state(0)
+    for f in range(8):
+        assert po.relerr(a[f], b[f]) < FP64_TOL, f
+    s.close()

@@ -99,3 +99,17 @@ def test_calrhs_noalloc_rejects_oversized_grid(gpu):
     rc = fn(C.byref(desc), C.c_void_p(16), C.c_void_p(16), None)
     assert rc == nb._lib.ERR_INVALID
     assert b"65536" in lib.nuosc_last_error()
+
+
+def test_calrhs_noalloc_rejects_bad_spacing(gpu):
+    import nuosc_b200 as nb
+    lib = nb.lib()
+    fn = lib.nuosc_calrhs_noalloc
+    fn.argtypes = [C.POINTER(RhsDesc), C.c_void_p, C.c_void_p, C.c_void_p]
+    fn.restype = C.c_int
+    for dx, mu in ((0.0, 1.0), (-0.1, 1.0), (float("nan"), 1.0), (0.1, float("inf"))):
+        desc = RhsDesc(nx=16, nz=16, nv=42, nv_stride=42, precision=0, ko_order=6, dx=dx, dz=0.1, ko=0.1,
+                       mu=mu, pmo=0.0, vx=1, vy=1, vz=1, vw=1)
+        rc = fn(C.byref(desc), C.c_void_p(16), C.c_void_p(16), None)
+        assert rc == nb._lib.ERR_INVALID, (dx, mu)
+        assert b"spacing" in lib.nuosc_last_error()
