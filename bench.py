@@ -18,8 +18,8 @@ e2e      the same metric through the public C ABI with host buffers: upload
          analysis() (diagnostics read back), download the final state.
 roofline the dominant stage kernel (largest share of the live step time)
          timed with CUDA events on the solver's stream: the state passes that
-         stage reads and writes in the 13-pass step (S1 2, S2 and S3 3 each,
-         S4 5) x 8 fields x 8 B per cell-velocity / mean launch time, against
+         stage reads and writes in the 13-pass step (S1 2, S2 4, S3 3, S4 4)
+         x 8 fields x 8 B per cell-velocity / mean launch time, against
          the measured HBM copy bandwidth in MEASURED_PEAKS.json.  Step figures
          use the classic RK4 sequence's 1024 B per cell-step (step_frac,
          frac_vs_8tbs) and the 832 B this implementation moves (step_moved_*);
@@ -55,10 +55,10 @@ METRIC = "cell-steps/s"
 # sizeof(real) per cell-step, the fixed work figure the roofline counts.
 BYTES_PER_CELL_STEP = {"f64": 1024, "f32": 512}
 # State passes (8 fields each) per stage launch in the 13-pass step of the TMA
-# path: S1 reads U, writes Y2; S2 (S3) reads Y2 (Y3) and U, writes Y3 (Y4); S4
-# reads Y4, U, Y2, Y3 and writes U.  The profile kind "stage_s23" holds S2 and S3.
-STAGE_PASSES = {"stage_s1": 2, "stage_s23": 3, "stage_s4": 5}
-STAGE_NAMES = {"stage_s1": "S1", "stage_s23": "S2/S3", "stage_s4": "S4"}
+# path: S1 reads U, writes Y2; S2 reads Y2 and U, writes Y3 and B; S3 reads Y3
+# and U, writes Y4; S4 reads Y4, U and B, writes U.
+STAGE_PASSES = {"stage_s1": 2, "stage_s2": 4, "stage_s3": 3, "stage_s4": 4}
+STAGE_NAMES = {"stage_s1": "S1", "stage_s2": "S2", "stage_s3": "S3", "stage_s4": "S4"}
 MOVED_BYTES_PER_CELL_STEP = {"f64": 13 * 64, "f32": 13 * 32}
 
 
@@ -154,8 +154,7 @@ def traffic_per_launch(kernel_key):
 def step_traffic(dtype, nx, nv):
     """ncu DRAM bytes of one RK4 step's four stage launches (S1, S2, S3, S4;
     tails and finalize excluded) from the committed per-launch figures, or None."""
-    ks = [traffic_per_launch("%s_%s_%d_%d" % (k, dtype, nx, nv)) for k in ("stage_s1", "stage_s23", "stage_s23",
-                                                                           "stage_s4")]
+    ks = [traffic_per_launch("%s_%s_%d_%d" % (k, dtype, nx, nv)) for k in STAGE_PASSES]
     return float(sum(ks)) if all(k is not None for k in ks) else None
 
 
@@ -328,8 +327,7 @@ def bench_ours(args, world, rank, local):
     value = replica_value(cells, args.steps, ms, world)
     diag = s.analysis()
 
-    # dominant kernel: the stage kind with the largest share of the live step
-    # time (S2/S3 run as two launches of one kernel)
+    # dominant kernel: the stage with the largest share of the live step time
     peak, peak_kind = measured_peaks()
     dom = max(STAGE_PASSES, key=lambda k: prof[k][0])
     k_ms, k_n = prof[dom]
@@ -506,9 +504,8 @@ def bench_serving(args, local, single):
     at a time on the plain FP64 path)."""
     from nuosc_b200 import serve
 
-    def ref_rate(reqs):
-        cs64 = sum(r.cell_steps for r in reqs if r.precision == 0)
-        cs32 = sum(r.cell_steps for r in reqs if r.precision == 1)
+    def ref_rate(rep):  # the large solves' rate for the served FP64/FP32 cell-steps mix
+        cs64, cs32 = rep["cell_steps_fp64"], rep["cell_steps_fp32"]
         return (cs64 + cs32) / (cs64 / single["f64"] + cs32 / single["f32"])
 
     steps = (args.serve_min_steps, args.serve_max_steps)
@@ -525,7 +522,7 @@ def bench_serving(args, local, single):
 
     return {"requests": len(reqs), "steps_range": list(steps), "budget_gb": 150,
             "saturated": {"cell_steps_per_s": rs["cell_steps_per_s"],
-                          "vs_single_large_solve": rs["cell_steps_per_s"] / ref_rate(sat),
+                          "vs_single_large_solve": rs["cell_steps_per_s"] / ref_rate(rs),
                           "makespan_s": rs["makespan_s"], "peak_resident": rs["peak_resident"],
                           "latency_p50_s": rs["latency_p50_s"], "latency_p99_s": rs["latency_p99_s"],
                           **loop_stats(rs)},
@@ -533,12 +530,15 @@ def bench_serving(args, local, single):
                         "cell_steps_per_busy_s": rp["cell_steps_per_busy_s"],
                         "latency_p50_s": rp["latency_p50_s"], "latency_p99_s": rp["latency_p99_s"],
                         "makespan_s": rp["makespan_s"], "peak_resident": rp["peak_resident"], **loop_stats(rp),
-                        "one_at_a_time_fp64": {k: one[k] for k in ("cell_steps_per_s", "latency_p50_s",
-                                                                   "latency_p99_s", "makespan_s")}},
-            "diverged": rp["diverged"],
+                        "one_at_a_time_fp64_modelled": {k: one[k] for k in ("cell_steps_per_s", "latency_p50_s",
+                                                                            "latency_p99_s", "makespan_s")}},
+            "failed": {"saturated": rs["failed"], "poisson": rp["failed"],
+                       "poisson_failed_cell_steps_run": rp["failed_cell_steps_run"]},
             "note": "single-large-solve reference = the 1024x1024x642 FP64/FP32 solves timed above, weighted by "
                     "the requests' FP64/FP32 cell-steps; one-at-a-time latencies from measured per-shape FP64 step "
-                    "times; requests whose state blew up keep stepping (same cost) and are counted in 'diverged'; "
+                    "times (modelled: FIFO over measured per-shape step times, no host costs); a request whose "
+                    "streamed analysis reports a blown-up state is retired as failed and counted in 'failed', not "
+                    "in cell_steps_per_s or the latencies; "
                     "the 512-request run is in profiles/serving_512_requests.md"}
 
 

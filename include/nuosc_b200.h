@@ -130,6 +130,19 @@ int nuosc_set_kernel(nuosc_handle *h, int kind);
  * library, keyed on velocity count and precision).  No reference counterpart. */
 int nuosc_set_tile(nuosc_handle *h, int tz, int lx);
 int nuosc_get_tile(const nuosc_handle *h, int *tz, int *lx);
+/* How the FP32 TMA kernel sums the velocity-moment partials of a 64-velocity
+ * block: 1 in FP64 (products of the float state with double weights, double
+ * sums; the default, and always so for FP64 state), 0 in float.  The tile
+ * table's sixth column holds the autotuner's choice per (nv, precision).
+ * No reference counterpart (the reference sums in FP64, nuosc_class.cpp:62-82). */
+int nuosc_set_moment_sum(nuosc_handle *h, int msum);
+int nuosc_get_moment_sum(const nuosc_handle *h, int *msum);
+/* Summation error of the handle's fused cell moments (the ones the last
+ * stage's kernel accumulated for v_stat) against an FP64 recomputation from
+ * the same stored state: max |fused - FP64| / max |FP64| over all cells and
+ * the 12 moments.  The autotuner's accuracy test of the moment summation.
+ * Synchronises; needs a step run since the state was last set. */
+int nuosc_moment_error(nuosc_handle *h, double *err);
 
 /* grid geometry (CartGrid members) and the velocity quadrature (CartGrid::vx,vy,vz,vw) */
 int nuosc_get_geometry(const nuosc_handle *h, nuosc_geometry *out);
@@ -211,12 +224,27 @@ int nuosc_release_cached_memory(int device);
  * *ms (may be NULL); the device stays usable afterwards. */
 int nuosc_selftest_wait_timeout(int device, unsigned spins, double *ms);
 
+/* Self-test of the TMA stage kernels' own timeout path (no reference
+ * counterpart).  While extra_bytes > 0 (a multiple of 16, at most 65536),
+ * every TMA stage launch of this handle -- solo, or as a batch member --
+ * declares extra_bytes more than its copies deliver for one box of the
+ * handle's first tile (first z rows, velocity block, x segment and flavour
+ * half).  All copies land; that box's full barrier never completes, so every
+ * warp's bounded wait on it runs out (about 1 s), the tile stops, records
+ * NUOSC_ERR_TIMEOUT in the handle's status word, waits (bounded) for the
+ * copies it issued and returns; nothing faults.  nuosc_synchronize /
+ * nuosc_batch_synchronize then return NUOSC_ERR_TIMEOUT and the handle's
+ * state is undefined until it is set again.  0 switches the test off. */
+int nuosc_selftest_overdeclare_tx(nuosc_handle *h, unsigned extra_bytes);
+
 /* Per-kernel timing with CUDA events on the handle's stream (no counterpart
  * in the reference, which prints wall time per step, nuosc.cpp:222-235).
- * Kinds: 0 stage S1, 1 stage S2/S3, 2 stage S4, 3 calRHS, 4 moments,
- * 5 moment finalize.  nuosc_get_profile synchronises, fills ms[k] (total
- * milliseconds) and launches[k] for k < nkinds, and resets the counters. */
-#define NUOSC_PROF_KINDS 6
+ * Kinds: 0 stage S1, 1 stage S2 (and S3 on the direct and cp.async paths),
+ * 2 stage S4, 3 calRHS, 4 moments, 5 moment finalize, 6 stage S3 of the TMA
+ * path.  A stage's time includes its tail-kernel launch.  nuosc_get_profile
+ * synchronises, fills ms[k] (total milliseconds) and launches[k] for
+ * k < nkinds, and resets the counters. */
+#define NUOSC_PROF_KINDS 7
 int nuosc_set_profiling(nuosc_handle *h, int on);
 int nuosc_get_profile(nuosc_handle *h, double *ms, long long *launches, int nkinds);
 

@@ -137,6 +137,22 @@ class NuOsc:
         check(lib().nuosc_get_tile(self._h, C.byref(tz), C.byref(lx)))
         return tz.value, lx.value
 
+    def set_moment_sum(self, msum):
+        """FP32 TMA kernel: 1 sums the velocity-moment partials in FP64, 0 in float."""
+        check(lib().nuosc_set_moment_sum(self._h, int(msum)))
+
+    def get_moment_sum(self):
+        m = C.c_int()
+        check(lib().nuosc_get_moment_sum(self._h, C.byref(m)))
+        return m.value
+
+    def moment_error(self):
+        """Relative summation error of the fused cell moments of v_stat against an
+        FP64 recomputation from the stored state."""
+        e = C.c_double()
+        check(lib().nuosc_moment_error(self._h, C.byref(e)))
+        return e.value
+
     def _geometry(self):
         g = _lib.Geometry()
         check(lib().nuosc_get_geometry(self._h, C.byref(g)))

@@ -100,6 +100,9 @@ _SIGS = {
     "nuosc_check_snapshot": [_P, _I],
     "nuosc_gather": [_P, _I, _IP, _I, _IP, _I, _DP],
     "nuosc_synchronize": [_P],
+    "nuosc_set_moment_sum": [_P, _I],
+    "nuosc_get_moment_sum": [_P, _IP],
+    "nuosc_moment_error": [_P, _DP],
     "nuosc_set_profiling": [_P, _I],
     "nuosc_get_profile": [_P, _DP, C.POINTER(C.c_longlong), _I],
     "nuosc_batch_create": [C.POINTER(_P), _I, C.POINTER(_P)],
@@ -111,8 +114,9 @@ _SIGS = {
     "nuosc_batch_record_diag": [_P, C.POINTER(BatchRecord), C.POINTER(Diag)],
     "nuosc_release_cached_memory": [_I],
     "nuosc_selftest_wait_timeout": [_I, C.c_uint, C.POINTER(C.c_double)],
+    "nuosc_selftest_overdeclare_tx": [_P, C.c_uint],
 }
-PROF_KINDS = ["stage_s1", "stage_s23", "stage_s4", "calrhs", "moments", "moment_finalize"]
+PROF_KINDS = ["stage_s1", "stage_s2", "stage_s4", "calrhs", "moments", "moment_finalize", "stage_s3"]
 
 _lib = None
 

@@ -10,14 +10,14 @@
 //   S4: k4 = L(Ya) ; U = A + dt/6 k4
 // which is U + dt/6 (k1 + 2k2 + 2k3 + k4), the reference's update, with
 // 16 state passes per step instead of the reference's 4 calRHS + 6 vectorize
-// (the direct and cp.async paths).  The TMA path keeps no accumulator: each
-// dt*k_s of the first three stages is the difference of a stage input and U,
-// so the last stage rebuilds the sum from them (registers U = v_stat,
-// Y2 = v_pre, Y3 = v_cor, Y4 = v_rhs):
-//   S1: k1 = L(U)  ; Y2 = U + dt/2 k1                        2 passes
-//   S2: k2 = L(Y2) ; Y3 = U + dt/2 k2                        3
-//   S3: k3 = L(Y3) ; Y4 = U + dt   k3                        3
-//   S4: k4 = L(Y4) ; U = U + [(Y2-U) + 2(Y3-U) + (Y4-U)]/3 + dt/6 k4   5
+// (the direct and cp.async paths).  The TMA path recovers dt/2 k1 = Y2 - U
+// and dt k3 = Y4 - U from the stage inputs it reads anyway, so only one
+// partial sum B is stored (registers U = v_stat, Y2 and Y4 = v_pre, Y3 =
+// v_cor, B = v_rhs):
+//   S1: k1 = L(U)  ; Y2 = U + dt/2 k1                           2 passes
+//   S2: k2 = L(Y2) ; Y3 = U + dt/2 k2 ; B = (Y2 - U) + dt k2    4
+//   S3: k3 = L(Y3) ; Y4 = U + dt k3                             3
+//   S4: k4 = L(Y4) ; U = U + [B + (Y4 - U)]/3 + dt/6 k4         4
 // 13 state passes per step.
 #include "../../include/nuosc_b200.h"
 #include "internal.cuh"
@@ -98,6 +98,7 @@ struct nuosc_handle {
     XTile tile{16, 64, 32};
     long long launches = 0;
     bool mom_valid = false;  // d_mom holds the moments of v_stat
+    unsigned fault_tx = 0;   // self-test of the TMA kernels' bounded waits (nuosc_selftest_overdeclare_tx)
     long long steps_done = 0;  // RK4 steps since the initial data
     nuosc_batch *batch = nullptr;  // the live batch this handle belongs to
 
@@ -261,9 +262,10 @@ int prof_kind(int mode) {
     case MODE_S1: return 0;
     case MODE_S1Y: return 0;
     case MODE_S23: return 1;
-    case MODE_SY: return 1;
+    case MODE_SY: return 6;
+    case MODE_S2B: return 1;
     case MODE_S4: return 2;
-    case MODE_S4F: return 2;
+    case MODE_S4B: return 2;
     default: return 3;
     }
 }
@@ -301,12 +303,11 @@ int run_stage_direct(nuosc_handle *h, int mode, int in, int u, int acc_src, int 
 // one RK4 stage in the x-march path (moments of the stage output fused)
 template <typename T>
 int run_stage_xmarch(nuosc_handle *h, bool tma, const XTile &tile, int mode, int in, int u, int acc_src, int acc_dst,
-                     int y_dst, double cA, double cY, int w = -1) {
+                     int y_dst, double cA, double cY) {
     StageArgs<T> a{};
     a.in = (const T *)h->reg[in];
     a.u = u >= 0 ? (const T *)h->reg[u] : nullptr;
     a.acc_src = acc_src >= 0 ? (const T *)h->reg[acc_src] : nullptr;
-    a.w = w >= 0 ? (const T *)h->reg[w] : nullptr;
     a.acc_dst = acc_dst >= 0 ? (T *)h->reg[acc_dst] : nullptr;
     a.y_dst = y_dst >= 0 ? (T *)h->reg[y_dst] : nullptr;
     a.mom_in = h->d_mom;
@@ -317,6 +318,7 @@ int run_stage_xmarch(nuosc_handle *h, bool tma, const XTile &tile, int mode, int
     a.cA = cA;
     a.cY = cY;
     a.status = h->d_status;
+    a.fault_tx = tma ? h->fault_tx : 0u;
     if (!h->mom_valid) {
         const int ps = h->prof_begin(4);
         CUDA_TRY(launch_moments<T>((const T *)h->reg[in], h->d_mom, a.q, h->g, h->stream));
@@ -381,12 +383,11 @@ int step_impl(nuosc_handle *h, int nsteps) {
     for (int n = 0; n < nsteps; ++n) {
         int rc;
         if (tma) {
-            // 13-pass sequence (registers 0 U, 2 Y2, 3 Y3, 1 Y4): no accumulator;
-            // the last stage recovers dt k1..dt k3 from Y2, Y3, Y4 and U
+            // 13-pass sequence (registers 0 U, 2 Y2 then Y4, 3 Y3, 1 B)
             if ((rc = run_stage_xmarch<T>(h, tma, tile, MODE_S1Y, 0, -1, -1, -1, 2, 0.0, 0.5 * dt))) return rc;
-            if ((rc = run_stage_xmarch<T>(h, tma, tile, MODE_SY, 2, 0, -1, -1, 3, 0.0, 0.5 * dt))) return rc;
-            if ((rc = run_stage_xmarch<T>(h, tma, tile, MODE_SY, 3, 0, -1, -1, 1, 0.0, dt))) return rc;
-            if ((rc = run_stage_xmarch<T>(h, tma, tile, MODE_S4F, 1, 0, 2, 0, -1, dt / 6.0, 0.0, 3))) return rc;
+            if ((rc = run_stage_xmarch<T>(h, tma, tile, MODE_S2B, 2, 0, -1, 1, 3, dt, 0.5 * dt))) return rc;
+            if ((rc = run_stage_xmarch<T>(h, tma, tile, MODE_SY, 3, 0, -1, -1, 2, 0.0, dt))) return rc;
+            if ((rc = run_stage_xmarch<T>(h, tma, tile, MODE_S4B, 2, 0, 1, 0, -1, dt / 6.0, 0.0))) return rc;
         } else if (xm) {
             if ((rc = run_stage_xmarch<T>(h, tma, tile, MODE_S1, 0, -1, -1, 1, 2, dt / 6.0, 0.5 * dt))) return rc;
             if ((rc = run_stage_xmarch<T>(h, tma, tile, MODE_S23, 2, 0, 1, 1, 3, dt / 3.0, 0.5 * dt))) return rc;
@@ -779,6 +780,44 @@ int nuosc_get_tile(const nuosc_handle *h, int *tz, int *lx) {
     return NUOSC_OK;
 }
 
+int nuosc_set_moment_sum(nuosc_handle *h, int msum) {
+    if (!h) return fail(NUOSC_ERR_INVALID, "null handle");
+    if (msum != 0 && msum != 1) return fail(NUOSC_ERR_INVALID, "moment summation %d (0 float in-block, 1 FP64)", msum);
+    h->tile.msum = msum;
+    return NUOSC_OK;
+}
+
+int nuosc_get_moment_sum(const nuosc_handle *h, int *msum) {
+    if (!h || !msum) return fail(NUOSC_ERR_INVALID, "null argument");
+    *msum = h->precision == NUOSC_FP64 ? 1 : h->tile.msum;
+    return NUOSC_OK;
+}
+
+int nuosc_moment_error(nuosc_handle *h, double *err) {
+    HANDLE_CHECK(h);
+    if (!err) return fail(NUOSC_ERR_INVALID, "null argument");
+    if (!h->mom_valid) return fail(NUOSC_ERR_INVALID, "moment_error: no moments of v_stat held (run a step first)");
+    const size_t n = (size_t)h->g.ncell * NMOM;
+    double *tmp = nullptr;
+    CUDA_TRY(dev_alloc((void **)&tmp, n * sizeof(double), h->device, h->stream));
+    cudaError_t e = h->precision == NUOSC_FP64
+                        ? launch_moments<double>((const double *)h->reg[0], tmp, h->quad(), h->g, h->stream)
+                        : launch_moments<float>((const float *)h->reg[0], tmp, h->quad(), h->g, h->stream);
+    std::vector<double> a(n), b(n);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(a.data(), h->d_mom, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(b.data(), tmp, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    dev_free(tmp, h->stream);
+    CUDA_TRY(e);
+    double d = 0.0, m = 0.0;
+    for (size_t i = 0; i < n; ++i) {
+        d = std::max(d, std::fabs(a[i] - b[i]));
+        m = std::max(m, std::fabs(b[i]));
+    }
+    *err = m > 0.0 ? d / m : d;
+    return NUOSC_OK;
+}
+
 int nuosc_set_time(nuosc_handle *h, double t) {
     if (!h) return fail(NUOSC_ERR_INVALID, "null handle");
     h->phy_time = t;
@@ -1053,6 +1092,7 @@ struct nuosc_batch {
     bool ko6 = true;
     int tz = 16;
     bool vac = false;               // some member has a vacuum term (pmo != 0)
+    bool m64 = true;                // moment partials summed in FP64 (the members' tile msum; FP64 always)
     std::vector<nuosc_handle *> m;  // service order: largest first
     std::vector<nuosc_handle *> user;  // the caller's order (record member indices)
     std::vector<int> user_index;       // user index of m[i]
@@ -1077,17 +1117,17 @@ struct nuosc_batch {
 
 namespace {
 
-// RK4 stage k of step_impl's 13-pass TMA sequence: (mode, in, u, acc_src, w,
+// RK4 stage k of step_impl's 13-pass TMA sequence: (mode, in, u, acc_src,
 // acc_dst, y_dst) with cA = dt / da (da 0: cA = 0) and cY = fy * dt, the same
 // expressions as step_impl
 struct StageSpec {
-    int mode, in, u, acc_src, w, acc_dst, y_dst;
+    int mode, in, u, acc_src, acc_dst, y_dst;
     double da, fy;
 };
-constexpr StageSpec kStages[4] = {{MODE_S1Y, 0, -1, -1, -1, -1, 2, 0.0, 0.5},
-                                  {MODE_SY, 2, 0, -1, -1, -1, 3, 0.0, 0.5},
-                                  {MODE_SY, 3, 0, -1, -1, -1, 1, 0.0, 1.0},
-                                  {MODE_S4F, 1, 0, 2, 3, 0, -1, 6.0, 0.0}};
+constexpr StageSpec kStages[4] = {{MODE_S1Y, 0, -1, -1, -1, 2, 0.0, 0.5},
+                                  {MODE_S2B, 2, 0, -1, 1, 3, 1.0, 0.5},
+                                  {MODE_SY, 3, 0, -1, -1, 2, 0.0, 1.0},
+                                  {MODE_S4B, 2, 0, 1, 0, -1, 6.0, 0.0}};
 
 std::vector<double> batch_signature(const nuosc_batch *b) {
     std::vector<double> s;
@@ -1096,6 +1136,8 @@ std::vector<double> batch_signature(const nuosc_batch *b) {
         s.push_back(h->pmo);
         s.push_back(h->dt);
         s.push_back(h->tile.lx);
+        s.push_back(h->tile.msum);
+        s.push_back(h->fault_tx);
         s.push_back(h->renorm ? 1.0 : 0.0);
         s.push_back((double)(uintptr_t)h->d_part);
     }
@@ -1113,6 +1155,12 @@ void batch_release_graph(nuosc_batch *b) {
 template <typename T>
 int batch_build(nuosc_batch *b) {
     const int n = (int)b->m.size();
+    // one persistent kernel runs every member: they must sum their moment
+    // partials the same way as their own solo launches do
+    b->m64 = sizeof(T) == 8 || b->m[0]->tile.msum != 0;
+    for (const nuosc_handle *h : b->m)
+        if (sizeof(T) == 4 && (h->tile.msum != 0) != b->m64)
+            return fail(NUOSC_ERR_UNSUPPORTED, "batch members must share the moment summation (tile msum)");
     CUDA_TRY(cudaStreamSynchronize(b->stream));  // no replay still reads the tables
     batch_release_graph(b);
     for (nuosc_handle *h : b->m) {
@@ -1171,7 +1219,6 @@ int batch_build(nuosc_batch *b) {
             a.in = (const T *)h->reg[sp.in];
             a.u = sp.u >= 0 ? (const T *)h->reg[sp.u] : nullptr;
             a.acc_src = sp.acc_src >= 0 ? (const T *)h->reg[sp.acc_src] : nullptr;
-            a.w = sp.w >= 0 ? (const T *)h->reg[sp.w] : nullptr;
             a.acc_dst = sp.acc_dst >= 0 ? (T *)h->reg[sp.acc_dst] : nullptr;
             a.y_dst = sp.y_dst >= 0 ? (T *)h->reg[sp.y_dst] : nullptr;
             a.mom_in = h->d_mom;
@@ -1182,6 +1229,7 @@ int batch_build(nuosc_batch *b) {
             a.cA = sp.da > 0.0 ? h->dt / sp.da : 0.0;
             a.cY = sp.fy == 1.0 ? h->dt : sp.fy * h->dt;
             a.status = h->d_status;
+            a.fault_tx = h->fault_tx;
             ti = xtma_batch_fill<T>(&host[((size_t)k * n + i) * b->item_bytes], a, b->ko6, b->tz, lxs[i]);
             if (v0 < h->g.nvs)
                 tails[k].push_back(TailItem<T>{a, v0, tail_lanes(h->g.nvs - v0), xtma_num_vblocks<T>(h->g), 0});
@@ -1228,7 +1276,7 @@ int batch_build(nuosc_batch *b) {
     b->vac = false;
     for (const nuosc_handle *h : b->m) b->vac = b->vac || h->pmo != 0.0;
     for (int k = 0; k < 4; ++k) {
-        b->grid[k] = xtma_batch_grid<T>(kStages[k].mode, b->ko6, b->tz, b->vac, b->device);
+        b->grid[k] = xtma_batch_grid<T>(kStages[k].mode, b->ko6, b->tz, b->vac, b->m64, b->device);
         if (b->grid[k] < 1) return fail(NUOSC_ERR_CUDA, "batch: cannot size the persistent stage grid");
     }
 
@@ -1238,7 +1286,7 @@ int batch_build(nuosc_batch *b) {
     cudaError_t e = cudaMemsetAsync(b->d_counter, 0, 4 * sizeof(unsigned long long), b->stream);
     for (int k = 0; k < 4 && e == cudaSuccess; ++k) {
         e = launch_stage_xtma_batch<T>(b->d_buf + (size_t)k * n * b->item_bytes, b->d_starts, n, tiles,
-                                       b->d_counter + k, kStages[k].mode, b->ko6, b->tz, b->vac, b->grid[k],
+                                       b->d_counter + k, kStages[k].mode, b->ko6, b->tz, b->vac, b->m64, b->grid[k],
                                        b->stream);
         if (e == cudaSuccess && b->ntail) {
             const size_t tb = 4 * (size_t)b->ntail * sizeof(TailItem<T>);
@@ -1476,6 +1524,14 @@ int nuosc_selftest_wait_timeout(int device, unsigned spins, double *ms) {
     if (ms) *ms = el;
     if (st != NUOSC_TIMEOUT_CODE) return fail(NUOSC_ERR_INVALID, "selftest: the wait did not expire (status %d)", st);
     return fail(NUOSC_ERR_TIMEOUT, "selftest: the bounded wait expired after %u polls (%.3f ms)", spins, el);
+}
+
+int nuosc_selftest_overdeclare_tx(nuosc_handle *h, unsigned extra_bytes) {
+    if (!h) return fail(NUOSC_ERR_INVALID, "null handle");
+    if (extra_bytes % 16 || extra_bytes > 65536)
+        return fail(NUOSC_ERR_INVALID, "overdeclare_tx: %u bytes (a multiple of 16, at most 65536)", extra_bytes);
+    h->fault_tx = extra_bytes;
+    return NUOSC_OK;
 }
 
 int nuosc_release_cached_memory(int device) {

@@ -45,22 +45,25 @@ struct Quad {
 //   MODE_S23 : acc_dst = acc_src + cA*k ;     y_dst = u  + cY*k
 //   MODE_S4  : acc_dst = acc_src + cA*k
 // (the classic 16-pass sequence of the direct and cp.async paths), and the
-// 13-pass sequence of the TMA path, which keeps no accumulator register:
+// 13-pass sequence of the TMA path:
 //   MODE_S1Y : y_dst = in + cY*k                       (Y2 = U + dt/2 k1)
-//   MODE_SY  : y_dst = u + cY*k                        (Y3 = U + dt/2 k2, Y4 = U + dt k3)
-//   MODE_S4F : acc_dst = u + ((acc_src - u) + 2 (w - u) + (in - u))/3 + cA*k
-// In S4F, in = Y4, acc_src = Y2, w = Y3 and cA = dt/6, so the update is
-// U + dt/6 (k1 + 2 k2 + 2 k3 + k4) with each dt*k_s recovered as a
-// difference Y_s+1 - U of nearby values (exact by Sterbenz where they lie
-// within a factor 2).
-enum StageMode { MODE_RHS = 0, MODE_S1 = 1, MODE_S23 = 2, MODE_S4 = 3, MODE_S1Y = 5, MODE_SY = 6, MODE_S4F = 7 };
+//   MODE_S2B : y_dst = u + cY*k ; acc_dst = (in - u) + cA*k
+//                                   (Y3 = U + dt/2 k2, B = dt/2 k1 + dt k2)
+//   MODE_SY  : y_dst = u + cY*k                        (Y4 = U + dt k3)
+//   MODE_S4B : acc_dst = u + (acc_src + (in - u))/3 + cA*k
+// In S4B, in = Y4, acc_src = B and cA = dt/6, so the update is
+// U + dt/6 (k1 + 2 k2 + 2 k3 + k4); dt/2 k1 = Y2 - U and dt k3 = Y4 - U are
+// recovered as differences of nearby values (exact by Sterbenz where they
+// lie within a factor 2).
+enum StageMode {
+    MODE_RHS = 0, MODE_S1 = 1, MODE_S23 = 2, MODE_S4 = 3, MODE_S1Y = 5, MODE_SY = 6, MODE_S4B = 7, MODE_S2B = 8
+};
 
 template <typename T>
 struct StageArgs {
     const T *in;
     const T *u;
     const T *acc_src;
-    const T *w;            // MODE_S4F: the third pointwise input (Y3)
     T *acc_dst;
     T *y_dst;
     const double *mom_in;  // [ncell][12] moments of `in`
@@ -70,6 +73,10 @@ struct StageArgs {
     Coeffs c;
     double cA, cY;
     int *status;           // device status word (bounded waits)
+    // test of the TMA kernels' bounded waits (0 in normal use): the first
+    // front box of the instance's first tile declares this many bytes more
+    // than its copies deliver, so every wait on it runs out
+    unsigned fault_tx;
 };
 
 // ---------------------------------------------------------------- launches
@@ -84,6 +91,7 @@ struct XTile {
     int lx;        // x planes marched per CTA
     int vb;        // velocities per CTA (32)
     int kind = 0;  // preferred x-march kernel from the tile table: 2 cp.async, 3 TMA, 0 either
+    int msum = 1;  // FP32 TMA march: moment partials summed in FP64 (1) or in float within a block (0)
 };
 template <typename T>
 bool xmarch_supported(const Geom &g, bool ko6, XTile t);
@@ -111,16 +119,17 @@ size_t xtma_batch_item_bytes();
 template <typename T>
 long long xtma_batch_fill(void *item, const StageArgs<T> &a, bool ko6, int tz, int lx);
 // CTAs of a persistent launch on `device` (also sets the kernel's dynamic
-// shared-memory limit); -1 on failure.  vac: some instance has pmo != 0.
+// shared-memory limit); -1 on failure.  vac: some instance has pmo != 0;
+// m64: FP32 moment partials summed in FP64 (XTile::msum; FP64 always is).
 template <typename T>
-int xtma_batch_grid(int mode, bool ko6, int tz, bool vac, int device);
+int xtma_batch_grid(int mode, bool ko6, int tz, bool vac, bool m64, int device);
 // starts[i] = tiles of instances 0..i-1 (instances ordered as the caller
 // wants them served); grid = xtma_batch_grid(...); *counter must be 0 at the
 // launch (the work-list cursor)
 template <typename T>
 cudaError_t launch_stage_xtma_batch(const void *items, const long long *starts, int n, long long ntiles,
-                                    unsigned long long *counter, int mode, bool ko6, int tz, bool vac, int grid,
-                                    cudaStream_t s);
+                                    unsigned long long *counter, int mode, bool ko6, int tz, bool vac, bool m64,
+                                    int grid, cudaStream_t s);
 // Tail of the TMA x-march stage (tail.cu): when the last velocity block of
 // the TMA kernel would hold at most a quarter block of real velocities, the
 // velocities from xtma_tail_v0 on are computed by a one-thread-per-(cell,

@@ -73,13 +73,17 @@ __device__ __forceinline__ void tail_point(const StageArgs<T> &a, const long lon
                 outm[f] = c4[f] + cY * kv[f];  // Y2
                 a.y_dst[idx] = outm[f];
             } else if (MODE == MODE_SY) {
-                outm[f] = a.u[idx] + cY * kv[f];  // Y3, Y4
+                outm[f] = a.u[idx] + cY * kv[f];  // Y4
+                a.y_dst[idx] = outm[f];
+            } else if (MODE == MODE_S2B) {
+                const T u = a.u[idx];
+                a.acc_dst[idx] = (c4[f] - u) + cA * kv[f];  // B = dt/2 k1 + dt k2
+                outm[f] = u + cY * kv[f];                   // Y3
                 a.y_dst[idx] = outm[f];
             } else {
-                // U + [(Y2 - U) + 2 (Y3 - U) + (Y4 - U)]/3 + dt/6 k4, as the TMA kernel
+                // U + [B + (Y4 - U)]/3 + dt/6 k4, as the TMA kernel
                 const T u = a.u[idx];
-                const T p = fma(T(2), a.w[idx] - u, a.acc_src[idx] - u);
-                outm[f] = u + fma(p + (c4[f] - u), T(1.0 / 3.0), cA * kv[f]);
+                outm[f] = u + fma(a.acc_src[idx] + (c4[f] - u), T(1.0 / 3.0), cA * kv[f]);
                 a.acc_dst[idx] = outm[f];
             }
         }
@@ -146,8 +150,9 @@ cudaError_t launch_tail_ko(const StageArgs<T> &a, int mode, int v0, int twp, int
     const unsigned blocks = (unsigned)((threads + TAIL_BLOCK - 1) / TAIL_BLOCK);
     switch (mode) {
     case MODE_S1Y: k_stage_tail<T, KO6, MODE_S1Y><<<blocks, TAIL_BLOCK, 0, s>>>(a, v0, twp, nvb); break;
+    case MODE_S2B: k_stage_tail<T, KO6, MODE_S2B><<<blocks, TAIL_BLOCK, 0, s>>>(a, v0, twp, nvb); break;
     case MODE_SY: k_stage_tail<T, KO6, MODE_SY><<<blocks, TAIL_BLOCK, 0, s>>>(a, v0, twp, nvb); break;
-    case MODE_S4F: k_stage_tail<T, KO6, MODE_S4F><<<blocks, TAIL_BLOCK, 0, s>>>(a, v0, twp, nvb); break;
+    case MODE_S4B: k_stage_tail<T, KO6, MODE_S4B><<<blocks, TAIL_BLOCK, 0, s>>>(a, v0, twp, nvb); break;
     default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
@@ -159,8 +164,9 @@ cudaError_t launch_tail_batch_ko(const TailItem<T> *items, const long long *star
     const unsigned blocks = (unsigned)((total + TAIL_BLOCK - 1) / TAIL_BLOCK);
     switch (mode) {
     case MODE_S1Y: k_stage_tail_batch<T, KO6, MODE_S1Y><<<blocks, TAIL_BLOCK, 0, s>>>(items, starts, n, total); break;
+    case MODE_S2B: k_stage_tail_batch<T, KO6, MODE_S2B><<<blocks, TAIL_BLOCK, 0, s>>>(items, starts, n, total); break;
     case MODE_SY: k_stage_tail_batch<T, KO6, MODE_SY><<<blocks, TAIL_BLOCK, 0, s>>>(items, starts, n, total); break;
-    case MODE_S4F: k_stage_tail_batch<T, KO6, MODE_S4F><<<blocks, TAIL_BLOCK, 0, s>>>(items, starts, n, total); break;
+    case MODE_S4B: k_stage_tail_batch<T, KO6, MODE_S4B><<<blocks, TAIL_BLOCK, 0, s>>>(items, starts, n, total); break;
     default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();

@@ -436,7 +436,7 @@ template cudaError_t launch_stage_xmarch<float>(const StageArgs<float> &, int, b
 // NUOSC_TILES), written by the autotuner nuosc_b200/autotune.py; kernel 2 is
 // the cp.async x-march, 3 the TMA one.  Shapes not listed use 16 x 128.
 XTile autotune_lookup(int nv, int precision) {
-    static std::vector<std::array<int, 5>> table;
+    static std::vector<std::array<int, 6>> table;
     static std::once_flag once;
     std::call_once(once, [] {
         std::string path;
@@ -454,16 +454,17 @@ XTile autotune_lookup(int nv, int precision) {
         if (!f) return;
         char line[256];
         while (fgets(line, sizeof line, f)) {
-            std::array<int, 5> e{0, 0, 0, 0, 0};
-            if (line[0] != '#' && sscanf(line, "%d %d %d %d %d", &e[0], &e[1], &e[2], &e[3], &e[4]) >= 4)
+            // nv precision tz lx [kernel [msum]]; msum defaults to FP64 sums
+            std::array<int, 6> e{0, 0, 0, 0, 0, 1};
+            if (line[0] != '#' && sscanf(line, "%d %d %d %d %d %d", &e[0], &e[1], &e[2], &e[3], &e[4], &e[5]) >= 4)
                 table.push_back(e);
         }
         fclose(f);
     });
     for (const auto &e : table)
         if (e[0] == nv && e[1] == precision && (e[2] == 4 || e[2] == 8 || e[2] == 16) && e[3] >= 1)
-            return XTile{e[2], e[3], VB, e[4]};
-    return XTile{16, 128, VB, 0};
+            return XTile{e[2], e[3], VB, e[4], e[5] != 0};
+    return XTile{16, 128, VB, 0, 1};
 }
 
 }  // namespace nuosc

@@ -15,8 +15,8 @@
 //     march: a warp waits only on full barriers and releases a slot after its
 //     last use by arriving on the slot's "empty" mbarrier; the issuing lane
 //     waits on "empty" before refilling a slot;
-//   * the pointwise inputs of the epilogue (U in S2 and S3, U, Y2 and Y3 in
-//     S4; none in S1) are plain coalesced loads issued at the top of each plane,
+//   * the pointwise inputs of the epilogue (U in S2 and S3, U and B in S4;
+//     none in S1) are plain coalesced loads issued at the top of each plane,
 //     before the waits and the stencil; the issuing lane prefetches their TZ
 //     rows into L2 two planes ahead with a tensor prefetch
 //     (cp.async.bulk.prefetch.tensor), so the loads find them in L2;
@@ -66,8 +66,7 @@ struct __align__(64) TmaMaps {
     CUtensorMap tz;   // TZ rows (middle piece of a box wrapped at both ends)
     CUtensorMap r;    // R rows (wrapped halo)
     CUtensorMap pu;   // TZ rows of the stage's U register (L2 prefetch of the pointwise input)
-    CUtensorMap pa;   // TZ rows of the final stage's Y2 input (acc_src; L2 prefetch)
-    CUtensorMap pw;   // TZ rows of the final stage's Y3 input (w; L2 prefetch)
+    CUtensorMap pa;   // TZ rows of the final stage's B input (acc_src; L2 prefetch)
 };
 
 __device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
@@ -151,27 +150,47 @@ struct Slot {
     static constexpr unsigned tx = sizeof(T) * ZR * 4 * VB + 8 * TZ * NMOM;  // bytes landing per plane
 };
 
-// One axis of the stencil over s[0..2R] (centre s[R]):
-//   ko  = KO difference with unit strength, the centre term included:
-//         6th: s[0]+s[6] - 6 (s[1]+s[5]) + 15 (s[2]+s[4]) - 20 s[3]
-//         4th: s[0]+s[4] - 4 (s[1]+s[3]) + 6 s[2]
-//   adv = s[C-2] - s[C+2] - 8 (s[C-1] - s[C+1]), the 4th-order central
-//         difference of the advection term before its factor -v/(12 dx).
-// The stencil value is eps_z ko_z + eps_x ko_x + fz adv_z + fx adv_x, so
-// only two uniform coefficients (eps_x, eps_z) enter per field; the integer
-// weights are compile-time constants.
-template <typename T, int R>
-__device__ __forceinline__ void axis_parts(const T (&s)[2 * R + 1], T &ko, T &adv) {
-    constexpr int C = R;
-    const T d2 = s[C - 2] - s[C + 2], d1 = s[C - 1] - s[C + 1];
-    adv = fma(T(-8), d1, d2);
-    if constexpr (R == 3) {
-        const T t3 = s[0] + s[6], t2 = s[1] + s[5], t1 = s[2] + s[4];
-        ko = fma(T(-20), s[3], fma(T(15), t1, fma(T(-6), t2, t3)));
+// The stencil of one field at one point, eps_z KO_z + eps_x KO_x + fz ADV_z
+// + fx ADV_x with
+//   KO  (unit strength) 6th: s[0]+s[6] - 6 (s[1]+s[5]) + 15 (s[2]+s[4]) - 20 s[3]
+//                       4th: s[0]+s[4] - 4 (s[1]+s[3]) + 6 s[2]
+//   ADV = s[C-2] - s[C+2] - 8 (s[C-1] - s[C+1]) (the 4th-order central
+//         difference before its factor f = -v/(12 dx)),
+// is evaluated as one weighted sum per axis: the four neighbours at offsets
+// -2, -1, +1, +2 carry per-velocity weights (KO and ADV coefficients folded
+// together, StencilW), the pair at +-3 (6th difference only) the uniform
+// eps, and the centre, shared by both axes, -20 (eps_z + eps_x) or
+// 6 (eps_z + eps_x).  That is 14 (6th) or 10 (4th) FP64 operations per field
+// instead of 22 (18) for the separate KO and ADV sums.
+//   6th: w = {-6 eps + f, 15 eps - 8 f, 15 eps + 8 f, -6 eps - f}
+//   4th: w = {eps + f, -4 eps - 8 f, -4 eps + 8 f, eps - f}
+template <int R>
+__host__ __device__ __forceinline__ void stencil_weights(double eps, double f, double (&w)[4]) {
+    if (R == 3) {
+        w[0] = -6 * eps + f;
+        w[1] = 15 * eps - 8 * f;
+        w[2] = 15 * eps + 8 * f;
+        w[3] = -6 * eps - f;
     } else {
-        const T t2 = s[0] + s[4], t1 = s[1] + s[3];
-        ko = fma(T(6), s[2], fma(T(-4), t1, t2));
+        w[0] = eps + f;
+        w[1] = -4 * eps - 8 * f;
+        w[2] = -4 * eps + 8 * f;
+        w[3] = eps - f;
     }
+}
+
+// one axis's off-centre terms: s[C-2..C+2] without the centre with weights
+// w[0..3], plus eps (s[0] + s[6]) in the 6th difference
+template <typename T, int R>
+__device__ __forceinline__ T axis_sum(const T (&s)[2 * R + 1], const T (&w)[4], T eps) {
+    constexpr int C = R;
+    T acc;
+    if constexpr (R == 3) acc = eps * (s[0] + s[6]);
+    else acc = T(0);
+    acc = fma(w[0], s[C - 2], acc);
+    acc = fma(w[1], s[C - 1], acc);
+    acc = fma(w[2], s[C + 1], acc);
+    return fma(w[3], s[C + 2], acc);
 }
 
 template <typename T, bool VAC>
@@ -201,16 +220,21 @@ __device__ __forceinline__ void rs_step(M (&m)[16]) {
     for (int i = 0; i < N / 2; ++i) m[i] += __shfl_xor_sync(0xffffffffu, m[i + N / 2], O);
 }
 
-// statically allocated per-CTA scratch of the march: the abort flag and, with
-// two velocities per thread (FP32), the per-velocity constants
-template <typename T>
+// statically allocated per-CTA scratch of the march: the abort flag, the
+// per-velocity stencil weights and, with two velocities per thread (FP32),
+// the per-velocity constants of the commutator and the moments (the moment
+// weights in double when the FP32 march sums its moment partials in FP64, M64)
+template <typename T, bool M64>
 struct MarchShared {
     static constexpr bool kShared = vpt<T>() == 2;
     static constexpr int VB = vblock<T>();
-    // [component][p * 32 + lane] and [4 p + j][lane]: consecutive lanes read
-    // consecutive words (a lane-major layout would put 16 lanes on one bank)
+    static constexpr int NP = vpt<T>();
+    // [component][p * 32 + lane], [4 p + j][lane] and [j][NP lane + p]:
+    // consecutive lanes read consecutive words (a lane-major layout would put
+    // 16 lanes on one bank); a lane's NP stencil weights are one vector load
     double vq[kShared ? 3 : 1][kShared ? VB : 2];          // vx, vy, vz
-    float wp[kShared ? vpt<T>() * 4 : 1][kShared ? 32 : 2];  // lane-permuted weights, rounded to float
+    std::conditional_t<M64, double, float> wp[kShared ? vpt<T>() * 4 : 1][kShared ? 32 : 2];  // lane-permuted
+    T sw[8][32 * NP];                                       // stencil weights: z axis j = 0..3, x axis 4..7
     int abort;
 };
 
@@ -222,7 +246,7 @@ constexpr int tma_ctas_per_sm() {
 // Ring geometry of one march.  Boxes are issued D planes ahead of their
 // front use: 3 with 16-row tiles (one CTA per SM, 8 slots of 24 KB at R = 3),
 // 2 with 8-row tiles (two CTAs per SM share the 228 KB).  The pointwise
-// inputs of the epilogue (U in S2/S3/S4, Y2 and Y3 in S4) stay plain
+// inputs of the epilogue (U in S2/S3/S4, B in S4) stay plain
 // per-thread loads, but thread 0 prefetches their TZ rows of plane x + PFD
 // into L2 with one tensor prefetch each, so those loads hit L2: measured 3 %
 // faster per step than without (PFD 1 and 3 equal within noise, 6 slower),
@@ -231,8 +255,8 @@ template <typename T, int R, int MODE, int TZ>
 struct MarchCfg {
     static constexpr int D = TZ == 16 ? 3 : 2;  // boxes issued ahead of their first use
     static constexpr int PFD = 2;                 // L2 prefetch distance of the pointwise inputs, planes
-    static constexpr bool PU = MODE == MODE_SY || MODE == MODE_S4F;  // reads U pointwise
-    static constexpr bool PA = MODE == MODE_S4F;                     // reads Y2 (acc_src) and Y3 (w) pointwise
+    static constexpr bool PU = MODE == MODE_SY || MODE == MODE_S2B || MODE == MODE_S4B;  // reads U pointwise
+    static constexpr bool PA = MODE == MODE_S4B;                                       // reads B pointwise
     static constexpr int NS = R + D + 2;  // a box lives from its front use to its centre use, plus slack
     static constexpr size_t ring = (size_t)NS * Slot<T, TZ, R>::bytes;
     static constexpr size_t smem = ring + 2 * NS * 8;  // box ring | mbarriers
@@ -256,10 +280,10 @@ __device__ __forceinline__ P rd(const P &x) {
 // (cell, velocity) does not depend on which.  VAC compiles the vacuum term in
 // (it then runs where a.c.pmo != 0).  Returns true when a bounded wait
 // expired (the status word is set and the tile is incomplete).
-template <typename T, int R, int MODE, int TZ, bool VAC, bool SA>
+template <typename T, int R, int MODE, int TZ, bool VAC, bool SA, bool M64>
 __device__ __forceinline__ bool xtma_march(const TmaMaps *const &mp, const StageArgs<T> &a, const int z0, const int vb,
                                            const int nvb, const int xs, const int xe, const int half,
-                                           unsigned char *smem, MarchShared<T> &sh) {
+                                           unsigned char *smem, MarchShared<T, M64> &sh) {
     using S = Slot<T, TZ, R>;
     using CF = MarchCfg<T, R, MODE, TZ>;
     constexpr int NP = vpt<T>();       // velocities per thread
@@ -294,12 +318,19 @@ __device__ __forceinline__ bool xtma_march(const TmaMaps *const &mp, const Stage
     __syncthreads();
 
     // lane 0 of warp 0: load box j (plane xs + j, periodic) into slot j % NS
+    // (phase j / NS of its full barrier).  `issued` = last box issued + 1.
+    // fault_tx (the self-test of the bounded waits) over-declares the bytes of
+    // box R of the instance's first tile: all its copies land, its phase never
+    // completes.
+    int issued = 0;
+    const unsigned fault_tx =
+        (tid == 0 && z0 == 0 && vb == 0 && xs == 0 && half == 0) ? rd<SA>(a.fault_tx) : 0u;
     auto issue = [&](int j) -> bool {
         const int s = j % NS;
         if (j >= NS && !mbar_wait(smem_u32(&bars[NS + s]), (unsigned)((j / NS - 1) & 1))) return false;
         const unsigned full = smem_u32(&bars[s]);
         unsigned char *sp = smem + s * S::bytes;
-        mbar_expect_tx(full, S::tx);
+        mbar_expect_tx(full, S::tx + (j == R ? fault_tx : 0u));
         const int x = (xs + j) % rd<SA>(a.g.nx);
         const int nz = rd<SA>(a.g.nz);
         const TmaMaps &maps = *rd<SA>(mp);
@@ -315,6 +346,7 @@ __device__ __forceinline__ bool xtma_march(const TmaMaps *const &mp, const Stage
             dst += len;
         }
         bulk_load(smem_u32(sp + S::mb), rd<SA>(a.mom_in) + ((long long)x * nz + z0) * NMOM, 8u * TZ * NMOM, full);
+        issued = j + 1;
         return true;
     };
 
@@ -323,10 +355,7 @@ __device__ __forceinline__ bool xtma_march(const TmaMaps *const &mp, const Stage
         if ((CF::PU || CF::PA) && i < nplanes) {
             const TmaMaps &maps = *rd<SA>(mp);
             if (CF::PU) tma_prefetch_4d(&maps.pu, vb * VB, 4 * half, z0, xs + i);
-            if (CF::PA) {
-                tma_prefetch_4d(&maps.pa, vb * VB, 4 * half, z0, xs + i);
-                tma_prefetch_4d(&maps.pw, vb * VB, 4 * half, z0, xs + i);
-            }
+            if (CF::PA) tma_prefetch_4d(&maps.pa, vb * VB, 4 * half, z0, xs + i);
         }
     };
 
@@ -337,18 +366,25 @@ __device__ __forceinline__ bool xtma_march(const TmaMaps *const &mp, const Stage
     // in shared memory and are read per plane, which keeps the register queue
     // clear of spills.
     const int perm = (lane >> 1) & 15;
-    constexpr bool kShared = MarchShared<T>::kShared;
+    constexpr bool kShared = MarchShared<T, M64>::kShared;
     auto &s_vq = sh.vq;
     auto &s_wp = sh.wp;
     double vxd[NP], vyd[NP], vzd[NP], wperm[NP][4];
-    T fx[NP], fz[NP];
 #pragma unroll
     for (int p = 0; p < NP; ++p) {
         vxd[p] = a.q.vx[vc + p];
         vyd[p] = a.q.vy[vc + p];
         vzd[p] = a.q.vz[vc + p];
-        fx[p] = T(vxd[p] * a.c.fxs);
-        fz[p] = T(vzd[p] * a.c.fzs);
+        if (r == 0) {
+            double wz[4], wx[4];
+            stencil_weights<R>(a.c.kz, vzd[p] * a.c.fzs, wz);
+            stencil_weights<R>(a.c.kx, vxd[p] * a.c.fxs, wx);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                sh.sw[j][NP * lane + p] = T(wz[j]);
+                sh.sw[4 + j][NP * lane + p] = T(wx[j]);
+            }
+        }
         const double wd = vact ? a.q.vw[vc + p] : 0.0;
         const double v4w[4] = {wd, vxd[p] * wd, vyd[p] * wd, vzd[p] * wd};
 #pragma unroll
@@ -365,16 +401,17 @@ __device__ __forceinline__ bool xtma_march(const TmaMaps *const &mp, const Stage
                 s_vq[1][p * 32 + lane] = vyd[p];
                 s_vq[2][p * 32 + lane] = vzd[p];
 #pragma unroll
-                for (int j = 0; j < 4; ++j) s_wp[4 * p + j][lane] = (float)wperm[p][j];
+                for (int j = 0; j < 4; ++j) s_wp[4 * p + j][lane] = (std::conditional_t<M64, double, float>)wperm[p][j];
             }
         }
-        __syncthreads();
     }
+    __syncthreads();  // the per-velocity constants in shared memory are complete
     // uniform coefficients: hoisted (kernel parameters in the single-instance
     // kernel; FP32 values in registers), except for the FP64 batched kernel,
     // which re-reads them from shared memory at each use
     constexpr bool RR = SA && sizeof(T) == 8;
     const T kz = RR ? T(0) : T(a.c.kz), kx = RR ? T(0) : T(a.c.kx), mu = RR ? T(0) : T(a.c.mu);
+    const T kc = T((R == 3 ? -20.0 : 6.0) * (a.c.kz + a.c.kx));  // centre weight of both axes
     const T cA0 = RR ? T(0) : T(a.cA), cY0 = RR ? T(0) : T(a.cY);
     auto K = [&](const double &x, T hoisted) -> T {
         if constexpr (RR) return T(rd<true>(x));
@@ -412,29 +449,20 @@ __device__ __forceinline__ bool xtma_march(const TmaMaps *const &mp, const Stage
         }
         const int x = xs + i;
         const long long oc = hoff + (long long)x * P + own;
-        // uin: U; ain (S4F): (Y2 - U) + 2 (Y3 - U), formed at once so that
-        // only two values per field stay live across the stencil
-        T uin[4][NP], ain[4][NP];
+        T uin[4][NP], ain[4][NP];  // U, B
         {
             // pointwise epilogue inputs first (they are not in the ring; L2 hits
             // after the tensor prefetch PFD planes earlier)
             constexpr bool LU = CF::PU, LA = CF::PA;
             const T *up = LU ? rd<SA>(a.u) + oc : nullptr;
             const T *ap = LA ? rd<SA>(a.acc_src) + oc : nullptr;
-            const T *wp = LA ? rd<SA>(a.w) + oc : nullptr;
 #pragma unroll
             for (int f = 0; f < 4; ++f) {
 #pragma unroll
                 for (int p = 0; p < NP; ++p) uin[f][p] = ain[f][p] = T(0);
                 if (vact) {
                     if (LU) ldv<T, NP>(up + f * fs, uin[f]);
-                    if (LA) {
-                        T y2[NP], y3[NP];
-                        ldv<T, NP>(ap + f * fs, y2);
-                        ldv<T, NP>(wp + f * fs, y3);
-#pragma unroll
-                        for (int p = 0; p < NP; ++p) ain[f][p] = fma(T(2), y3[p] - uin[f][p], y2[p] - uin[f][p]);
-                    }
+                    if (LA) ldv<T, NP>(ap + f * fs, ain[f]);
                 }
             }
         }
@@ -457,26 +485,33 @@ __device__ __forceinline__ bool xtma_march(const TmaMaps *const &mp, const Stage
 
         T sten[4][NP];
         const T kzp = K(a.c.kz, kz), kxp = K(a.c.kx, kx);
+        T swz[4][NP], swx[4][NP];  // this lane's stencil weights (shared memory, re-read per plane)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            ldv<T, NP>(&sh.sw[j][NP * lane], swz[j]);
+            ldv<T, NP>(&sh.sw[4 + j][NP * lane], swx[j]);
+        }
 #pragma unroll
         for (int f = 0; f < 4; ++f) {
             T zs[W][NP];
 #pragma unroll
-            for (int k = 0; k < W; ++k) ldv<T, NP>(&zb[((r + k) * 4 + f) * VB + NP * lane], zs[k]);
+            for (int k = 0; k < W; ++k)  // the centre row is the x-queue's centre: not re-read
+                if (k != R) ldv<T, NP>(&zb[((r + k) * 4 + f) * VB + NP * lane], zs[k]);
 #pragma unroll
             for (int p = 0; p < NP; ++p) {
-                T zsp[W], xsp[W];
+                T zsp[W], xsp[W], wzp[4], wxp[4];
 #pragma unroll
                 for (int k = 0; k < W; ++k) {
-                    zsp[k] = zs[k][p];
+                    zsp[k] = k == R ? q[f][R][p] : zs[k][p];
                     xsp[k] = q[f][k][p];
                 }
-                T koz, advz, kox, advx;
-                axis_parts<T, R>(zsp, koz, advz);
-                axis_parts<T, R>(xsp, kox, advx);
-                T acc = kzp * koz;
-                acc = fma(kxp, kox, acc);
-                acc = fma(fz[p], advz, acc);
-                sten[f][p] = fma(fx[p], advx, acc);
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    wzp[j] = swz[j][p];
+                    wxp[j] = swx[j][p];
+                }
+                const T sz = axis_sum<T, R>(zsp, wzp, kzp), sx = axis_sum<T, R>(xsp, wxp, kxp);
+                sten[f][p] = fma(kc, q[f][R][p], sz + sx);
             }
         }
         double m[NMOM];
@@ -509,30 +544,40 @@ __device__ __forceinline__ bool xtma_march(const TmaMaps *const &mp, const Stage
                 if (MODE == MODE_S1Y) {
                     outm[f][p] = cen[f] + cY * kk[f];  // Y2
                 } else if (MODE == MODE_SY) {
-                    outm[f][p] = uin[f][p] + cY * kk[f];  // Y3, Y4
+                    outm[f][p] = uin[f][p] + cY * kk[f];  // Y4
+                } else if (MODE == MODE_S2B) {
+                    const T u = uin[f][p];
+                    ain[f][p] = (cen[f] - u) + cA * kk[f];  // B = dt/2 k1 + dt k2
+                    outm[f][p] = u + cY * kk[f];            // Y3
                 } else {
-                    // U + [(Y2 - U) + 2 (Y3 - U) + (Y4 - U)]/3 + dt/6 k4: the small
-                    // increments are summed first, U is added last
+                    // U + [B + (Y4 - U)]/3 + dt/6 k4: the increments are summed
+                    // first, U is added last
                     const T u = uin[f][p];
                     outm[f][p] = u + fma(ain[f][p] + (cen[f] - u), T(1.0 / 3.0), cA * kk[f]);
                 }
             }
         }
         if (vact) {
-            T *dp = (MODE == MODE_S4F ? rd<SA>(a.acc_dst) : rd<SA>(a.y_dst)) + oc;
+            T *dp = (MODE == MODE_S4B ? rd<SA>(a.acc_dst) : rd<SA>(a.y_dst)) + oc;
 #pragma unroll
             for (int f = 0; f < 4; ++f) stv<T, NP>(dp + f * fs, outm[f]);
+            if (MODE == MODE_S2B) {
+                T *bp = rd<SA>(a.acc_dst) + oc;
+#pragma unroll
+                for (int f = 0; f < 4; ++f) stv<T, NP>(bp + f * fs, ain[f]);
+            }
         }
         // velocity-moment partials of the written state (nuosc_class.cpp:69-71).
-        // FP64: products and the warp's reduce-scatter in double.  FP32 (two
-        // velocities per thread): in float -- the float state's products with
+        // M64 (every FP64 march; the FP32 march when the tile table says so):
+        // products and the warp's reduce-scatter in double -- the float state
+        // converts exactly and each product with a double weight is a double
+        // product, so the sums carry no error beyond the state's own rounding.
+        // FP32 march without M64: in float -- the float state's products with
         // float-rounded weights, summed over the block's 64 velocities --, the
-        // block's partial stored as double and the blocks and both halves summed
-        // in FP64 by the finalize; half of the FP32 step's FP64 instructions and
-        // 64-bit shuffles go, which measured 7 % off the FP32 step with no
-        // visible change in the FP32-vs-FP64 error series.
+        // block's partial stored as double; the blocks and both halves are
+        // summed in FP64 by the finalize either way.
         {
-            using M = std::conditional_t<kShared, float, double>;
+            using M = std::conditional_t<M64, double, float>;
             M mp[16];
 #pragma unroll
             for (int k = 0; k < 16; ++k) mp[k] = M(0);
@@ -575,13 +620,14 @@ __device__ __forceinline__ bool xtma_march(const TmaMaps *const &mp, const Stage
     const bool aborted = s_abort != 0;
     if (tid == 0) {
         if (aborted) {
-            // a wait expired: report it, then drain (bounded) every slot that may
-            // still receive a copy before the CTA's shared memory is reused or released
+            // a wait expired: report it, then wait (bounded) for the copies of
+            // the last NS boxes issued -- the only ones that may still be in
+            // flight: box j - NS of a slot was consumed (so had landed) before
+            // box j was issued into it -- before the CTA's shared memory is
+            // reused or released
             atomicExch(a.status, NUOSC_TIMEOUT_CODE);
-            for (int s = 0; s < NS; ++s) {
-                mbar_wait(smem_u32(&bars[s]), 0);
-                mbar_wait(smem_u32(&bars[s]), 1);
-            }
+            for (int j = issued > NS ? issued - NS : 0; j < issued; ++j)
+                if (j >= R || j < nplanes) mbar_wait(smem_u32(&bars[j % NS]), (unsigned)((j / NS) & 1));
         }
         for (int s = 0; s < 2 * NS; ++s) mbar_inval(smem_u32(&bars[s]));
     }
@@ -591,15 +637,15 @@ __device__ __forceinline__ bool xtma_march(const TmaMaps *const &mp, const Stage
 // grid (velocity blocks run by this kernel, z tiles, 2 x x-segments); nvb:
 // velocity blocks of the moment partials (one more when a tail kernel runs
 // the last block)
-template <typename T, int R, int MODE, int TZ, bool VAC>
+template <typename T, int R, int MODE, int TZ, bool VAC, bool M64>
 __global__ void __launch_bounds__(32 * TZ, tma_ctas_per_sm<T, TZ>())
     k_xtma(const __grid_constant__ TmaMaps maps, const StageArgs<T> a, int LX, int nvb) {
     extern __shared__ __align__(1024) unsigned char smem[];
-    __shared__ MarchShared<T> sh;
+    __shared__ MarchShared<T, M64> sh;
     const int xs = (blockIdx.z >> 1) * LX;
     if (xs >= a.g.nx) return;
     const TmaMaps *mp = &maps;
-    xtma_march<T, R, MODE, TZ, VAC, false>(mp, a, blockIdx.y * TZ, blockIdx.x, nvb, xs, min(xs + LX, a.g.nx),
+    xtma_march<T, R, MODE, TZ, VAC, false, M64>(mp, a, blockIdx.y * TZ, blockIdx.x, nvb, xs, min(xs + LX, a.g.nx),
                                            blockIdx.z & 1, smem, sh);
 }
 
@@ -627,14 +673,14 @@ struct __align__(64) BatchItem {
 // them out of the register file that the march's x-queue fills.  VAC compiles
 // the vacuum term in (for batches with any pmo != 0); it is then switched per
 // instance at run time.
-template <typename T, int R, int MODE, int TZ, bool VAC>
+template <typename T, int R, int MODE, int TZ, bool VAC, bool M64>
 __global__ void __launch_bounds__(32 * TZ, tma_ctas_per_sm<T, TZ>())
     k_xtma_batch(const BatchItem<T> *items, const long long *__restrict__ starts, int ninst, long long nitems,
                  unsigned long long *counter) {
     constexpr int NW = (int)(sizeof(StageArgs<T>) / 8);
     static_assert(sizeof(StageArgs<T>) % 8 == 0 && NW <= 32 * TZ, "StageArgs copy: one 8-byte word per thread");
     extern __shared__ __align__(1024) unsigned char smem[];
-    __shared__ MarchShared<T> sh;
+    __shared__ MarchShared<T, M64> sh;
     __shared__ __align__(16) StageArgs<T> s_a;
     __shared__ const TmaMaps *s_mp;
     __shared__ int s_t[6];  // instance, z0, vb, xs, xe, half
@@ -671,10 +717,7 @@ __global__ void __launch_bounds__(32 * TZ, tma_ctas_per_sm<T, TZ>())
                 tensormap_acquire(&e.maps.tz);
                 tensormap_acquire(&e.maps.r);
                 if (MarchCfg<T, R, MODE, TZ>::PU) tensormap_acquire(&e.maps.pu);
-                if (MarchCfg<T, R, MODE, TZ>::PA) {
-                    tensormap_acquire(&e.maps.pa);
-                    tensormap_acquire(&e.maps.pw);
-                }
+                if (MarchCfg<T, R, MODE, TZ>::PA) tensormap_acquire(&e.maps.pa);
             }
         }
         __syncthreads();
@@ -686,7 +729,7 @@ __global__ void __launch_bounds__(32 * TZ, tma_ctas_per_sm<T, TZ>())
         const int nvb = items[lo].nvb;
         const int z0 = s_t[1], vb = s_t[2], xs = s_t[3], xe = s_t[4], half = s_t[5];
         __syncthreads();  // s_a is complete
-        if (xtma_march<T, R, MODE, TZ, VAC, true>(s_mp, s_a, z0, vb, nvb, xs, xe, half, smem, sh)) break;
+        if (xtma_march<T, R, MODE, TZ, VAC, true, M64>(s_mp, s_a, z0, vb, nvb, xs, xe, half, smem, sh)) break;
     }
 }
 
@@ -713,6 +756,8 @@ cudaError_t launch_wait_selftest(int *status, unsigned spins, cudaStream_t s) {
 
 // ------------------------------------------------------------------ host side
 namespace {
+
+bool tma_mode(int mode) { return mode == MODE_S1Y || mode == MODE_S2B || mode == MODE_SY || mode == MODE_S4B; }
 
 using EncodeFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
                               const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
@@ -761,22 +806,20 @@ template <typename T>
 bool make_maps(TmaMaps *m, const StageArgs<T> &a, int tz, int r) {
     memset((void *)&m->pu, 0, sizeof m->pu);
     memset((void *)&m->pa, 0, sizeof m->pa);
-    memset((void *)&m->pw, 0, sizeof m->pw);
     return make_map<T>(&m->zr, a.in, a.g, tz + 2 * r) && make_map<T>(&m->tzr, a.in, a.g, tz + r) &&
            make_map<T>(&m->tz, a.in, a.g, tz) && make_map<T>(&m->r, a.in, a.g, r) &&
-           (!a.u || make_map<T>(&m->pu, a.u, a.g, tz)) && (!a.acc_src || make_map<T>(&m->pa, a.acc_src, a.g, tz)) &&
-           (!a.w || make_map<T>(&m->pw, a.w, a.g, tz));
+           (!a.u || make_map<T>(&m->pu, a.u, a.g, tz)) && (!a.acc_src || make_map<T>(&m->pa, a.acc_src, a.g, tz));
 }
 
-template <typename T, int R, int MODE, int TZ, bool VAC>
+template <typename T, int R, int MODE, int TZ, bool VAC, bool M64>
 cudaError_t launch_t(const StageArgs<T> &a, XTile t, cudaStream_t s) {
     using CF = MarchCfg<T, R, MODE, TZ>;
-    static_assert(tma_ctas_per_sm<T, TZ>() * (CF::smem + sizeof(MarchShared<T>) + 64 + 1024) <= 228 * 1024,
+    static_assert(tma_ctas_per_sm<T, TZ>() * (CF::smem + sizeof(MarchShared<T, M64>) + 64 + 1024) <= 228 * 1024,
                   "ring exceeds shared memory");
     TmaMaps maps;
     if (!make_maps<T>(&maps, a, TZ, R)) return cudaErrorInvalidValue;
     const size_t smem = CF::smem;
-    cudaError_t e = cudaFuncSetAttribute(k_xtma<T, R, MODE, TZ, VAC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t e = cudaFuncSetAttribute(k_xtma<T, R, MODE, TZ, VAC, M64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e != cudaSuccess) return e;
     const int nseg = (a.g.nx + t.lx - 1) / t.lx;
@@ -785,23 +828,33 @@ cudaError_t launch_t(const StageArgs<T> &a, XTile t, cudaStream_t s) {
     // velocity blocks fastest: the CTAs resident at once read whole velocity
     // rows of a few z rows (DRAM page locality) rather than one block of many rows
     dim3 grid(nvbm, a.g.nz / TZ, nseg * 2);
-    k_xtma<T, R, MODE, TZ, VAC><<<grid, 32 * TZ, smem, s>>>(maps, a, t.lx, nvb);
+    k_xtma<T, R, MODE, TZ, VAC, M64><<<grid, 32 * TZ, smem, s>>>(maps, a, t.lx, nvb);
     return cudaGetLastError();
 }
 
-template <typename T, int R, int TZ, bool VAC>
+template <typename T, int R, int TZ, bool VAC, bool M64>
 cudaError_t launch_tm(const StageArgs<T> &a, int mode, XTile t, cudaStream_t s) {
     switch (mode) {
-    case MODE_S1Y: return launch_t<T, R, MODE_S1Y, TZ, VAC>(a, t, s);
-    case MODE_SY: return launch_t<T, R, MODE_SY, TZ, VAC>(a, t, s);
-    case MODE_S4F: return launch_t<T, R, MODE_S4F, TZ, VAC>(a, t, s);
+    case MODE_S1Y: return launch_t<T, R, MODE_S1Y, TZ, VAC, M64>(a, t, s);
+    case MODE_S2B: return launch_t<T, R, MODE_S2B, TZ, VAC, M64>(a, t, s);
+    case MODE_SY: return launch_t<T, R, MODE_SY, TZ, VAC, M64>(a, t, s);
+    case MODE_S4B: return launch_t<T, R, MODE_S4B, TZ, VAC, M64>(a, t, s);
     default: return cudaErrorInvalidValue;
     }
 }
 
-template <typename T, int R, int TZ>
+template <typename T, int R, int TZ, bool M64>
 cudaError_t launch_tv(const StageArgs<T> &a, int mode, XTile t, cudaStream_t s) {
-    return a.c.pmo != 0.0 ? launch_tm<T, R, TZ, true>(a, mode, t, s) : launch_tm<T, R, TZ, false>(a, mode, t, s);
+    return a.c.pmo != 0.0 ? launch_tm<T, R, TZ, true, M64>(a, mode, t, s)
+                          : launch_tm<T, R, TZ, false, M64>(a, mode, t, s);
+}
+
+// moment partials summed in FP64 (always for FP64 state; for FP32 state per
+// the tile's msum) or in float within a velocity block
+template <typename T, int R, int TZ>
+cudaError_t launch_tms(const StageArgs<T> &a, int mode, XTile t, cudaStream_t s) {
+    if constexpr (sizeof(T) == 8) return launch_tv<T, R, TZ, true>(a, mode, t, s);
+    else return t.msum ? launch_tv<T, R, TZ, true>(a, mode, t, s) : launch_tv<T, R, TZ, false>(a, mode, t, s);
 }
 
 // ---- batched launch: one persistent grid per stage over many instances
@@ -810,10 +863,10 @@ constexpr size_t batch_smem() {
     return MarchCfg<T, R, MODE, TZ>::smem;
 }
 
-template <typename T, int R, int MODE, int TZ, bool VAC>
+template <typename T, int R, int MODE, int TZ, bool VAC, bool M64>
 int batch_grid_t(int device) {
     const size_t smem = batch_smem<T, R, MODE, TZ>();
-    auto kern = k_xtma_batch<T, R, MODE, TZ, VAC>;
+    auto kern = k_xtma_batch<T, R, MODE, TZ, VAC, M64>;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return -1;
     int per_sm = 0, sms = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * TZ, smem) != cudaSuccess ||
@@ -822,38 +875,40 @@ int batch_grid_t(int device) {
     return per_sm * sms;
 }
 
-template <typename T, int R, int MODE, int TZ, bool VAC>
+template <typename T, int R, int MODE, int TZ, bool VAC, bool M64>
 cudaError_t batch_launch_t(const void *items, const long long *starts, int n, long long ntiles,
                            unsigned long long *counter, int grid, cudaStream_t s) {
-    k_xtma_batch<T, R, MODE, TZ, VAC><<<grid, 32 * TZ, batch_smem<T, R, MODE, TZ>(), s>>>(
+    k_xtma_batch<T, R, MODE, TZ, VAC, M64><<<grid, 32 * TZ, batch_smem<T, R, MODE, TZ>(), s>>>(
         (const BatchItem<T> *)items, starts, n, ntiles, counter);
     return cudaGetLastError();
 }
 
 // dispatch of (mode, ko6, tz, vac) onto the template instances of F
-template <typename T, template <typename, int, int, int, bool> class F, typename... Args>
+template <typename T, bool M64, template <typename, int, int, int, bool, bool> class F, typename... Args>
 auto batch_dispatch(int mode, bool ko6, int tz, bool vac, Args... args) {
-#define NUOSC_BATCH_V(R, M, Z) (vac ? F<T, R, M, Z, true>::run(args...) : F<T, R, M, Z, false>::run(args...))
+#define NUOSC_BATCH_V(R, M, Z) \
+    (vac ? F<T, R, M, Z, true, M64>::run(args...) : F<T, R, M, Z, false, M64>::run(args...))
 #define NUOSC_BATCH_TZ(R, M) (tz == 16 ? NUOSC_BATCH_V(R, M, 16) : NUOSC_BATCH_V(R, M, 8))
 #define NUOSC_BATCH_MODE(R)                                                                                   \
-    (mode == MODE_S1Y ? NUOSC_BATCH_TZ(R, MODE_S1Y)                                                           \
-     : mode == MODE_SY ? NUOSC_BATCH_TZ(R, MODE_SY)                                                           \
-                       : NUOSC_BATCH_TZ(R, MODE_S4F))
+    (mode == MODE_S1Y   ? NUOSC_BATCH_TZ(R, MODE_S1Y)                                                         \
+     : mode == MODE_S2B ? NUOSC_BATCH_TZ(R, MODE_S2B)                                                         \
+     : mode == MODE_SY  ? NUOSC_BATCH_TZ(R, MODE_SY)                                                          \
+                        : NUOSC_BATCH_TZ(R, MODE_S4B))
     return ko6 ? NUOSC_BATCH_MODE(3) : NUOSC_BATCH_MODE(2);
 #undef NUOSC_BATCH_MODE
 #undef NUOSC_BATCH_TZ
 #undef NUOSC_BATCH_V
 }
 
-template <typename T, int R, int MODE, int TZ, bool VAC>
+template <typename T, int R, int MODE, int TZ, bool VAC, bool M64>
 struct BatchGrid {
-    static int run(int device) { return batch_grid_t<T, R, MODE, TZ, VAC>(device); }
+    static int run(int device) { return batch_grid_t<T, R, MODE, TZ, VAC, M64>(device); }
 };
-template <typename T, int R, int MODE, int TZ, bool VAC>
+template <typename T, int R, int MODE, int TZ, bool VAC, bool M64>
 struct BatchLaunch {
     static cudaError_t run(const void *items, const long long *starts, int n, long long ntiles,
                            unsigned long long *counter, int grid, cudaStream_t s) {
-        return batch_launch_t<T, R, MODE, TZ, VAC>(items, starts, n, ntiles, counter, grid, s);
+        return batch_launch_t<T, R, MODE, TZ, VAC, M64>(items, starts, n, ntiles, counter, grid, s);
     }
 };
 
@@ -888,18 +943,27 @@ long long xtma_batch_fill(void *item, const StageArgs<T> &a, bool ko6, int tz, i
 }
 
 template <typename T>
-int xtma_batch_grid(int mode, bool ko6, int tz, bool vac, int device) {
-    if ((tz != 8 && tz != 16) || (mode != MODE_S1Y && mode != MODE_SY && mode != MODE_S4F)) return -1;
-    return batch_dispatch<T, BatchGrid>(mode, ko6, tz, vac, device);
+int xtma_batch_grid(int mode, bool ko6, int tz, bool vac, bool m64, int device) {
+    if ((tz != 8 && tz != 16) || !tma_mode(mode)) return -1;
+    if constexpr (sizeof(T) == 8) return batch_dispatch<T, true, BatchGrid>(mode, ko6, tz, vac, device);
+    else
+        return m64 ? batch_dispatch<T, true, BatchGrid>(mode, ko6, tz, vac, device)
+                   : batch_dispatch<T, false, BatchGrid>(mode, ko6, tz, vac, device);
 }
 
 template <typename T>
 cudaError_t launch_stage_xtma_batch(const void *items, const long long *starts, int n, long long ntiles,
-                                    unsigned long long *counter, int mode, bool ko6, int tz, bool vac, int grid,
-                                    cudaStream_t s) {
-    if ((tz != 8 && tz != 16) || (mode != MODE_S1Y && mode != MODE_SY && mode != MODE_S4F) || n < 1 || grid < 1)
+                                    unsigned long long *counter, int mode, bool ko6, int tz, bool vac, bool m64,
+                                    int grid, cudaStream_t s) {
+    if ((tz != 8 && tz != 16) || !tma_mode(mode) || n < 1 || grid < 1)
         return cudaErrorInvalidValue;
-    return batch_dispatch<T, BatchLaunch>(mode, ko6, tz, vac, items, starts, n, ntiles, counter, grid, s);
+    if constexpr (sizeof(T) == 8)
+        return batch_dispatch<T, true, BatchLaunch>(mode, ko6, tz, vac, items, starts, n, ntiles, counter, grid, s);
+    else
+        return m64 ? batch_dispatch<T, true, BatchLaunch>(mode, ko6, tz, vac, items, starts, n, ntiles, counter, grid,
+                                                          s)
+                   : batch_dispatch<T, false, BatchLaunch>(mode, ko6, tz, vac, items, starts, n, ntiles, counter,
+                                                           grid, s);
 }
 
 template <typename T>
@@ -916,8 +980,8 @@ int xtma_tail_v0(const Geom &g) {
 template <typename T>
 cudaError_t launch_stage_xtma(const StageArgs<T> &a, int mode, bool ko6, XTile t, cudaStream_t s) {
     if (!a.mom_part || a.g.nz % t.tz) return cudaErrorInvalidValue;
-    if (t.tz == 16) return ko6 ? launch_tv<T, 3, 16>(a, mode, t, s) : launch_tv<T, 2, 16>(a, mode, t, s);
-    return ko6 ? launch_tv<T, 3, 8>(a, mode, t, s) : launch_tv<T, 2, 8>(a, mode, t, s);
+    if (t.tz == 16) return ko6 ? launch_tms<T, 3, 16>(a, mode, t, s) : launch_tms<T, 2, 16>(a, mode, t, s);
+    return ko6 ? launch_tms<T, 3, 8>(a, mode, t, s) : launch_tms<T, 2, 8>(a, mode, t, s);
 }
 
 template bool xtma_supported<double>(const Geom &, XTile);
@@ -932,11 +996,13 @@ template size_t xtma_batch_item_bytes<double>();
 template size_t xtma_batch_item_bytes<float>();
 template long long xtma_batch_fill<double>(void *, const StageArgs<double> &, bool, int, int);
 template long long xtma_batch_fill<float>(void *, const StageArgs<float> &, bool, int, int);
-template int xtma_batch_grid<double>(int, bool, int, bool, int);
-template int xtma_batch_grid<float>(int, bool, int, bool, int);
+template int xtma_batch_grid<double>(int, bool, int, bool, bool, int);
+template int xtma_batch_grid<float>(int, bool, int, bool, bool, int);
 template cudaError_t launch_stage_xtma_batch<double>(const void *, const long long *, int, long long,
-                                                     unsigned long long *, int, bool, int, bool, int, cudaStream_t);
+                                                     unsigned long long *, int, bool, int, bool, bool, int,
+                                                     cudaStream_t);
 template cudaError_t launch_stage_xtma_batch<float>(const void *, const long long *, int, long long,
-                                                    unsigned long long *, int, bool, int, bool, int, cudaStream_t);
+                                                    unsigned long long *, int, bool, int, bool, bool, int,
+                                                    cudaStream_t);
 
 }  // namespace nuosc

@@ -21,6 +21,11 @@ parameters, a step count and a precision) arrive over time; the server
   * streams the analysis record (Pee, max||P|-1|, ...) of every solve every
     100 of its steps -- queued on the device between the batch's steps, no
     host synchronisation -- and at its last step;
+  * retires a solve as failed when a streamed record reports a blown-up state
+    (a non-finite value or max||P|-1| >= 10, the reference's assert in
+    nuosc_ana.cpp:131): it leaves its batch at the end of the quantum in
+    which the record arrives, and neither its steps nor its latency count
+    as served work;
   * reports per-request time-to-completion (p50/p99) and the aggregate
     cell-steps/s (nx*nz*nv per RK4 step).
 
@@ -83,6 +88,8 @@ class Record:
     diags: list = field(default_factory=list)  # (step, analysis dict or None)
     diverged_at: int = -1  # first streamed step whose analysis reported a blown-up state
     rejected: bool = False
+    failed: bool = False  # retired before its last step because its state blew up
+    steps_run: int = 0
 
     @property
     def latency(self):
@@ -235,16 +242,19 @@ class Server:
                 for rid in ran:
                     a = active[rid]
                     a[1] += q
+                    recs[rid].steps_run = a[1]
                     stats["steps_run"] += q
-                    if a[1] == recs[rid].req.steps:
+                    if a[1] == recs[rid].req.steps or recs[rid].diverged_at >= 0:
                         done.append(rid)
                 for rid in done:
                     s = active[rid][0]
                     req = recs[rid].req
-                    if req.steps % self.every:  # (multiples of `every` were streamed already)
-                        stream(rid, req.steps, _analysis(s)[0])
+                    if recs[rid].diverged_at < 0 and req.steps % self.every:
+                        stream(rid, req.steps, _analysis(s)[0])  # (multiples of `every` were streamed already)
+                    # a blown-up state (retired early, or at its last step) is a failed solve
+                    recs[rid].failed = recs[rid].diverged_at >= 0
                     recs[rid].completed = now()
-                    if self.on_complete:
+                    if self.on_complete and not recs[rid].failed:
                         self.on_complete(rid, s)
                 tc = time.perf_counter()
                 if done:
@@ -340,17 +350,25 @@ class Server:
 
     @staticmethod
     def _report(reqs, recs, makespan, busy, stats):
-        served = [recs[r.rid] for r in reqs if not recs[r.rid].rejected]
+        """Served = completed every requested step with a finite state; failed
+        solves (retired on a blown-up record) count neither their cell-steps nor
+        their latency, and their steps run are reported apart."""
+        served = [recs[r.rid] for r in reqs if not recs[r.rid].rejected and not recs[r.rid].failed]
+        failed = [recs[r.rid] for r in reqs if recs[r.rid].failed]
         lat = np.array([r.latency for r in served]) if served else np.zeros(1)
         cs = float(sum(r.req.cell_steps for r in served))
         first = min(r.arrival for r in reqs) if reqs else 0.0
         return {
             "requests": len(reqs), "served": len(served), "rejected": sum(r.rejected for r in recs.values()),
+            "failed": len(failed),
+            "failed_cell_steps_run": float(sum(r.req.nx * r.req.nz * r.req.nv * r.steps_run for r in failed)),
             "fp32": sum(r.req.precision == 1 for r in served), "fp64": sum(r.req.precision == 0 for r in served),
+            "cell_steps_fp64": float(sum(r.req.cell_steps for r in served if r.req.precision == 0)),
+            "cell_steps_fp32": float(sum(r.req.cell_steps for r in served if r.req.precision == 1)),
             "cell_steps": cs, "makespan_s": makespan, "busy_s": busy,
             "cell_steps_per_s": cs / max(1e-9, makespan - first), "cell_steps_per_busy_s": cs / max(1e-9, busy),
             "latency_p50_s": float(np.percentile(lat, 50)), "latency_p99_s": float(np.percentile(lat, 99)),
-            "latency_max_s": float(lat.max()), "diverged": sum(r.diverged_at >= 0 for r in served), **stats,
+            "latency_max_s": float(lat.max()), **stats,
         }
 
 

@@ -50,13 +50,13 @@ def test_reference_arm_under_torchrun_two_ranks():
 
 def test_step_traffic_from_profiles():
     """The roofline's per-step DRAM bytes are the four stage launches' ncu
-    figures (S2/S3 counted twice); sizes without a capture give None."""
+    figures; sizes without a capture give None."""
     sys.path.insert(0, ROOT)
     import bench
     with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
         t = json.load(f)
     for dt in ("f64", "f32"):
-        keys = ["stage_%s_%s_1024_642" % (k, dt) for k in ("s1", "s23", "s23", "s4")]
+        keys = ["stage_%s_%s_1024_642" % (k, dt) for k in ("s1", "s2", "s3", "s4")]
         if not all(k in t for k in keys):
             assert bench.step_traffic(dt, 1024, 642) is None
             continue

@@ -440,3 +440,29 @@ def test_tma_ko4_ten_steps_match_reference_on_32_cells(nb):
     for f in range(8):
         assert po.relerr(a[f], b[f]) < FP64_TOL, f
     s.close()
+
+
+def test_fp32_moment_summation_variants(nb):
+    """FP32 TMA kernel on 32x32 cells x 642 velocities: summing the
+    velocity-moment partials in FP64 (msum 1, the default) leaves the fused
+    cell moments within 1e-12 of an FP64 recomputation from the stored FP32
+    state; float partials (msum 0) do not reach that (about 1e-7).  Both stay
+    within FP32 rounding of the FP64 oracle, and the batch of a member keeps
+    its solo bits."""
+    p = box_params(32, 8, pmo=0.0)
+    o = _oracle_solve(p, 6, 31, 10, **HARD)
+    ref = o.get_state(0)
+    errs = {}
+    for msum in (1, 0):
+        s = make(nb, p, 6, precision=nb.FP32, kernel=nb.KERNEL_XTMA)
+        assert s.get_moment_sum() == 1
+        s.set_moment_sum(msum)
+        s.fillInitValue(1, seed=31, **HARD)
+        s.step_rk4(10)
+        errs[msum] = s.moment_error()
+        st = s.get_state()
+        for f in range(8):
+            assert po.relerr(st[f], ref[f]) < FP32_TOL, (msum, f)
+        s.close()
+    assert errs[1] < 1e-12, errs
+    assert errs[0] > errs[1]

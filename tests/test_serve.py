@@ -199,3 +199,60 @@ def test_served_results_equal_solo(gpu):
         assert diags[r.rid] == want
         assert np.array_equal(finals[r.rid], s.get_state().view(np.uint64))
         s.close()
+
+
+class BlowUpSolver(FakeSolver):
+    """A fake solve whose state blows up at step `bad` (its analysis then
+    reports a numeric error, as NuOsc.analysis does for a non-finite state or
+    max||P|-1| >= 10)."""
+    bad = {}
+
+    def analysis(self):
+        b = BlowUpSolver.bad.get(self.req.rid)
+        if b is not None and self.steps >= b:
+            import nuosc_b200 as nb
+            raise nb.NuoscError(nb._lib.ERR_NUMERIC, "blown up")
+        return super().analysis()
+
+
+class BlowUpBatch(FakeBatch):
+    def step_stream(self, n, every):
+        recs = []
+        for _ in range(n):
+            for m, s in enumerate(self.solvers):
+                s.step_rk4(1)
+                if s.steps % every == 0:
+                    d, _ = serve._analysis(s)
+                    recs.append((m, s.steps, d))
+        return recs
+
+
+def test_blown_up_solves_are_retired_as_failed():
+    """A solve whose streamed record reports a blown-up state leaves the GPU
+    at the end of that quantum: it runs no more steps, is reported as failed,
+    and its cell-steps and latency are not counted as served work."""
+    reqs = serve.draw_requests(6, rate=0.0, seed=4, steps=(900, 1000), sizes=(32,), nns=(2,))
+    BlowUpSolver.bad = {reqs[1].rid: 250, reqs[4].rid: 100}
+    made = {}
+
+    def factory(req, device):
+        made[req.rid] = BlowUpSolver(req)
+        return made[req.rid]
+
+    srv = serve.Server(budget_bytes=1e12, stream_every=100, solver_factory=factory, batch_factory=BlowUpBatch,
+                       quantum_s=1e-9)  # one step per quantum
+    rep = srv.run(reqs)
+    assert rep["failed"] == 2 and rep["served"] == 4
+    for r in reqs:
+        s = made[r.rid]
+        assert s.closed
+        if r.rid == reqs[1].rid:
+            assert s.steps == 300  # the record at step 300 is the first blown-up one
+        elif r.rid == reqs[4].rid:
+            assert s.steps == 100
+        else:
+            assert s.steps == r.steps
+    ok = [r for r in reqs if r.rid not in BlowUpSolver.bad]
+    assert rep["cell_steps"] == sum(r.cell_steps for r in ok)
+    assert rep["failed_cell_steps_run"] == (300 + 100) * 32 * 32 * 42
+    assert not FakeBatch.live
