@@ -105,6 +105,10 @@ typedef struct nuosc_geometry {
 typedef struct nuosc_diag {
     double phy_time, maxdP, surv, survb, avgP, avgPb, aM0, Lex, ELNe;
     long long nonfinite; /* count of non-finite state values seen by the reduction */
+    /* the advection test's integrals (printed by the reference when built
+     * with ADV_TEST, nuosc_ana.cpp:58-61,121): I1 = sum w ee / nor,
+     * I2 = sum w ee^2 / nor, nor = sum w G0 over all cells */
+    double I1, I2;
 } nuosc_diag;
 
 /* gen_v2d_icosahedron (CartGrid.cpp:46-61, icosahedron.h:36-171): the velocity
@@ -193,6 +197,18 @@ int nuosc_add_snapshot_at_v(nuosc_handle *h, const int *fields, int nfields, con
 int nuosc_add_snapshot_at_xv(nuosc_handle *h, const int *fields, int nfields, const char *fntpl, int every,
                              const int *xidx, int n_xidx, const int *vidx, int n_vidx);
 int nuosc_check_snapshot(nuosc_handle *h, int t);
+
+/* Checkpoint and restart of a solve (no counterpart in the reference, which
+ * only writes slices).  save writes v_stat (raw, in the handle's precision),
+ * the spectra G0/G0b, time, step count, n_nue0, mu, pmo, renorm and the cell
+ * moments held for v_stat; load restores them into a handle created with
+ * the same grid, velocity count, precision, ghost width, dt and ko (else
+ * NUOSC_ERR_INVALID).  A run stopped after step n, saved, loaded into a new
+ * handle and continued is bit-identical to the uninterrupted run.  Both
+ * synchronise the handle's stream and stage the state through 256 MB of
+ * page-locked host memory. */
+int nuosc_save_checkpoint(nuosc_handle *h, const char *path);
+int nuosc_load_checkpoint(nuosc_handle *h, const char *path);
 /* gather one snapshot block (sx * nz * sv doubles, (i,j,v) order) into host memory */
 int nuosc_gather(nuosc_handle *h, int field, const int *xidx, int n_xidx, const int *vidx, int n_vidx,
                  double *host);

@@ -94,6 +94,10 @@ class NuOsc {
                        double lnuebx, uint64_t seed = 0) {
         check(nuosc_fill_init(h_, ipt, alpha, eps0, sigma, lnue, lnueb, lnuex, lnuebx, seed));
     }
+    // the advection tests (nuosc_init.cpp:162-236), ipt 10 / 20 / 30 of nuosc_fill_init
+    void fillInitAdvtest(double eps0, double sigma) { check(nuosc_fill_init(h_, 10, 0, eps0, sigma, 1, 1, 0, 0, 0)); }
+    void fillInitSquare(double eps0, double sigma) { check(nuosc_fill_init(h_, 20, 0, eps0, sigma, 1, 1, 0, 0, 0)); }
+    void fillInitTriangle(double eps0, double sigma) { check(nuosc_fill_init(h_, 30, 0, eps0, sigma, 1, 1, 0, 0, 0)); }
 
     // the hot path
     void updatePeriodicBoundary(int reg = NUOSC_REG_STAT) { check(nuosc_update_periodic_boundary(h_, reg)); }
@@ -107,15 +111,21 @@ class NuOsc {
     // analysis(): returns the record; like the reference it prints the
     // "T= ..." line when print is set and appends to the analysis file when
     // one is open (nuosc_ana.cpp:119-129)
-    nuosc_diag analysis(bool print = false) {
+    // With adv_test the printed line is the advection test's (the reference
+    // built with ADV_TEST, nuosc_ana.cpp:120-121): the integrals I1, I2.
+    nuosc_diag analysis(bool print = false, bool adv_test = false) {
         nuosc_diag d{};
         check(nuosc_analysis(h_, &d));
-        if (print)
+        if (print && adv_test)
+            printf("T= %15f  I1= %5.4e I2= %5.4e\n", d.phy_time, d.I1, d.I2);
+        else if (print)
             printf("T= %15f  |dP|max= %5.4e surb= %5.4e %5.4e conP= %5.4e %5.4e |M0|= %5.4e ELNe= %g Lex= %g\n",
                    d.phy_time, d.maxdP, d.surv, d.survb, d.avgP, d.avgPb, d.aM0, d.ELNe, d.Lex);
         return d;
     }
     void open_analysis_file(const char *path = "analysis.dat") { check(nuosc_open_analysis_file(h_, path)); }
+    void save_checkpoint(const char *path) { check(nuosc_save_checkpoint(h_, path)); }
+    void load_checkpoint(const char *path) { check(nuosc_load_checkpoint(h_, path)); }
 
     // snapshots (nuosc_snapshot.cpp:13-122); fields are NUOSC_* ids
     void addSnapShotAtV(const std::vector<int> &fields, const char *fntpl, int dumpstep,

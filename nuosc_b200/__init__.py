@@ -17,6 +17,7 @@ them call the C ABI of include/nuosc_b200.h; the state lives in HBM.
 """
 import ctypes as C
 import math
+import os
 
 import numpy as np
 
@@ -199,11 +200,34 @@ class NuOsc:
 
     # ------------------------------------------------------------ init / state
     def fillInitValue(self, ipt, alpha, eps0, sigma, lnue, lnueb, lnuex=0.0, lnuebx=0.0, seed=0):
-        """nuosc_init.cpp:17-137 (generic branch); ipt=1 draws eps0*U(-1,1) per (x,z) from `seed`.
-        lnuex/lnuebx <= 0 (or inf) mean unbounded, the reference default."""
+        """nuosc_init.cpp:17-137: ipt 0..3 the generic branch (ipt=1 draws eps0*U(-1,1)
+        per (x,z) from `seed`), ipt 4 the "NOC" Fourier-phase branch (phases
+        from `seed`, every x), ipt 10/20/30 the advection tests (Advtest,
+        Square, Triangle; eps0 and sigma only).  lnuex/lnuebx <= 0 (or inf)
+        mean unbounded, the reference default."""
         lnuex = 0.0 if (lnuex is None or math.isinf(lnuex) or lnuex >= 1e300) else lnuex
         lnuebx = 0.0 if (lnuebx is None or math.isinf(lnuebx) or lnuebx >= 1e300) else lnuebx
         check(lib().nuosc_fill_init(self._h, int(ipt), alpha, eps0, sigma, lnue, lnueb, lnuex, lnuebx, int(seed)))
+
+    def save_checkpoint(self, path):
+        """Write the solve (state, spectra, time, moments) to `path`."""
+        check(lib().nuosc_save_checkpoint(self._h, os.fsencode(path)))
+
+    def load_checkpoint(self, path):
+        """Restore a solve saved by save_checkpoint into this handle (same grid)."""
+        check(lib().nuosc_load_checkpoint(self._h, os.fsencode(path)))
+
+    def fillInitAdvtest(self, eps0, sigma):
+        """NuOsc::fillInitAdvtest (nuosc_init.cpp:162-186): G0 = G0b = 1, ee a z profile."""
+        self.fillInitValue(10, 0.0, eps0, sigma, 1.0, 1.0)
+
+    def fillInitSquare(self, eps0, sigma):
+        """NuOsc::fillInitSquare (nuosc_init.cpp:188-211)."""
+        self.fillInitValue(20, 0.0, eps0, sigma, 1.0, 1.0)
+
+    def fillInitTriangle(self, eps0, sigma):
+        """NuOsc::fillInitTriangle (nuosc_init.cpp:213-236)."""
+        self.fillInitValue(30, 0.0, eps0, sigma, 1.0, 1.0)
 
     def get_field(self, field, reg=REG_STAT, layout=LAYOUT_COMPACT):
         g = self.grid

@@ -44,7 +44,7 @@ class Geometry(C.Structure):
 class Diag(C.Structure):
     _fields_ = [(n, C.c_double) for n in
                 ("phy_time", "maxdP", "surv", "survb", "avgP", "avgPb", "aM0", "Lex", "ELNe")] + \
-               [("nonfinite", C.c_longlong)]
+               [("nonfinite", C.c_longlong), ("I1", C.c_double), ("I2", C.c_double)]
 
     def as_dict(self):
         return {n: getattr(self, n) for n, _ in self._fields_}
@@ -100,6 +100,8 @@ _SIGS = {
     "nuosc_check_snapshot": [_P, _I],
     "nuosc_gather": [_P, _I, _IP, _I, _IP, _I, _DP],
     "nuosc_synchronize": [_P],
+    "nuosc_save_checkpoint": [_P, C.c_char_p],
+    "nuosc_load_checkpoint": [_P, C.c_char_p],
     "nuosc_set_moment_sum": [_P, _I],
     "nuosc_get_moment_sum": [_P, _IP],
     "nuosc_moment_error": [_P, _DP],

@@ -455,6 +455,49 @@ void compute_spectra(nuosc_handle *h, double alpha, double lnue, double lnueb, d
     }
 }
 
+// ipt = 4 spectra (nuosc_init.cpp:8-13, 49-50): G0 = g(vz, lnue), G0b = alpha
+// g(vz, lnueb) with g normalised analytically over vz in [-1, 1] (erf), not by
+// the quadrature sum of the generic branch
+void noc_spectra(nuosc_handle *h, double alpha, double lnue, double lnueb) {
+    auto g = [](double v, double sigma) {
+        const double v0 = 1.0;
+        const double N = sigma * std::sqrt(0.5 * M_PI) *
+                         (std::erf((1.0 + v0) / sigma / std::sqrt(2.0)) + std::erf((1.0 - v0) / sigma / std::sqrt(2.0)));
+        return std::exp(-(v - v0) * (v - v0) / (2.0 * sigma * sigma)) / N;
+    };
+    const int nv = h->g.nv;
+    h->G0.resize(nv);
+    h->G0b.resize(nv);
+    for (int v = 0; v < nv; ++v) {
+        h->G0[v] = g(h->vz[v], lnue);
+        h->G0b[v] = alpha * g(h->vz[v], lnueb);
+    }
+}
+
+// ipt = 4 perturbation in z (nuosc_init.cpp:28-46): amax = nz/20 Fourier modes
+// k = -amax .. amax-1 (k != 0) of amplitude 1e-7/|k| with phases phi[k + amax];
+// out[j] = sum cos(2 pi k Z_j / (z0 - z1) + phi), out[nz + j] the same with sin.
+// The reference draws the phases with rand(); here phi[m] = 2 pi U(seed, m),
+// U the seeded counter hash that ipt = 1 uses per cell, with the second key -1.
+std::vector<double> noc_profile(int nz, double z0, double z1, double dz, uint64_t seed) {
+    const int amax = nz / 2 / 10;
+    std::vector<double> phi(2 * amax + 1), out(2 * (size_t)nz, 0.0);
+    for (int m = 0; m <= 2 * amax; ++m) phi[m] = 2.0 * M_PI * seeded_uniform(seed, m, -1);
+    const double pi2oL = 2.0 * M_PI / (z0 - z1);
+    for (int j = 0; j < nz; ++j) {
+        const double Zj = z0 + (j + 0.5) * dz;
+        double tr = 0.0, ti = 0.0;
+        for (int k = -amax; k < amax; ++k) {
+            if (k == 0) continue;
+            tr += 1.e-7 / std::abs(k) * std::cos(pi2oL * k * Zj + phi[k + amax]);
+            ti += 1.e-7 / std::abs(k) * std::sin(pi2oL * k * Zj + phi[k + amax]);
+        }
+        out[j] = tr;
+        out[nz + j] = ti;
+    }
+    return out;
+}
+
 int upload_spectra(nuosc_handle *h) {
     const int s = h->g.nvs;
     CUDA_TRY(cudaMemsetAsync(h->d_quad + 4 * s, 0, 2 * s * sizeof(double), h->stream));
@@ -597,6 +640,8 @@ void diag_from_sums(const nuosc_handle *h, const double *q, double phy_time, nuo
     d.Lex = q[7] * h->ds_L;
     d.ELNe = std::fabs(h->n_nue0[0] * (1.0 - d.surv) - h->n_nue0[1] * (1.0 - d.survb)) / (h->n_nue0[0] + h->n_nue0[1]);
     d.nonfinite = (long long)q[10];
+    d.I1 = q[1] / q[8];
+    d.I2 = q[11] / q[8];
     *o = d;
 }
 
@@ -867,16 +912,36 @@ int nuosc_set_spectra(nuosc_handle *h, const double *G0, const double *G0b, doub
 int nuosc_fill_init(nuosc_handle *h, int ipt, double alpha, double eps0, double sigma, double lnue, double lnueb,
                     double lnuex, double lnuebx, uint64_t seed) {
     HANDLE_CHECK(h);
-    if (ipt < 0 || ipt > 3)
-        return fail(NUOSC_ERR_UNSUPPORTED, "ipt=%d: supported initial data are ipt 0..3", ipt);
-    compute_spectra(h, alpha, lnue, lnueb, lnuex, lnuebx);
+    if (!((ipt >= 0 && ipt <= 4) || ipt == 10 || ipt == 20 || ipt == 30))
+        return fail(NUOSC_ERR_UNSUPPORTED, "ipt=%d: supported initial data are ipt 0..4, 10, 20, 30", ipt);
+    if (ipt >= 10 && !(sigma > 0.0)) return fail(NUOSC_ERR_INVALID, "ipt=%d needs sigma > 0", ipt);
+    std::vector<double> zprof;
+    if (ipt == 4) {
+        noc_spectra(h, alpha, lnue, lnueb);
+        zprof = noc_profile(h->g.nz, h->z0, h->z1, h->dz, seed);
+    } else if (ipt >= 10) {  // advection tests: G0 = G0b = 1 (nuosc_init.cpp:168-169)
+        h->G0.assign(h->g.nv, 1.0);
+        h->G0b.assign(h->g.nv, 1.0);
+    } else {
+        compute_spectra(h, alpha, lnue, lnueb, lnuex, lnuebx);
+    }
     if (int rc = upload_spectra(h)) return rc;
-    if (h->precision == NUOSC_FP64)
-        CUDA_TRY(launch_init<double>((double *)h->reg[0], h->dG0(), h->dG0b(), h->g, ipt, eps0, sigma, h->z0, h->dz,
-                                     seed, h->stream));
-    else
-        CUDA_TRY(launch_init<float>((float *)h->reg[0], h->dG0(), h->dG0b(), h->g, ipt, eps0, sigma, h->z0, h->dz,
-                                    seed, h->stream));
+    double *dprof = nullptr;
+    if (!zprof.empty()) {
+        CUDA_TRY(dev_alloc((void **)&dprof, zprof.size() * sizeof(double), h->device, h->stream));
+        CUDA_TRY(cudaMemcpyAsync(dprof, zprof.data(), zprof.size() * sizeof(double), cudaMemcpyHostToDevice,
+                                 h->stream));
+    }
+    cudaError_t e = h->precision == NUOSC_FP64
+                        ? launch_init<double>((double *)h->reg[0], h->dG0(), h->dG0b(), h->g, ipt, eps0, sigma, h->z0,
+                                              h->dz, seed, dprof, h->stream)
+                        : launch_init<float>((float *)h->reg[0], h->dG0(), h->dG0b(), h->g, ipt, eps0, sigma, h->z0,
+                                             h->dz, seed, dprof, h->stream);
+    if (dprof) {
+        cudaStreamSynchronize(h->stream);  // zprof is host memory of this frame
+        dev_free(dprof, h->stream);
+    }
+    CUDA_TRY(e);
     h->mom_valid = false;
     h->phy_time = 0.0;
     h->steps_done = 0;
@@ -1014,6 +1079,115 @@ int nuosc_add_snapshot_at_xv(nuosc_handle *h, const int *fields, int nfields, co
     s.vidx.assign(vidx, vidx + n_vidx);
     if (int rc = write_meta(h, s, true)) return rc;
     h->snapshots.push_back(s);
+    return NUOSC_OK;
+}
+
+// ---------------------------------------------------------------- checkpoints
+// File layout (native byte order): "NUOSCCK1" | CkHeader | G0[nv] G0b[nv] |
+// v_stat: 8 fields x nx x nz x nv_stride elements of the state type, padding
+// velocities included | the 12 FP64 cell moments held for v_stat (ncell x
+// 12), when mom_valid.  Restoring the moments with the state makes a resumed
+// run bit-identical to an uninterrupted one: the next stage reads exactly the
+// moments the previous stage's kernel accumulated.
+namespace {
+struct CkHeader {
+    int32_t version, precision, nx, nz, nv, nvs, ghost, renorm, mom_valid, pad;
+    int64_t steps_done;
+    double x0, x1, z0, z1, dx, dz, dt, ko, mu, pmo, phy_time, n0, n1;
+};
+const char kCkMagic[8] = {'N', 'U', 'O', 'S', 'C', 'C', 'K', '1'};
+constexpr size_t kCkChunk = 256u << 20;  // bytes per staged device <-> host copy
+
+int ck_copy(nuosc_handle *h, FILE *f, char *dev, size_t bytes, bool save, char *stage) {
+    for (size_t off = 0; off < bytes; off += kCkChunk) {
+        const size_t n = std::min(kCkChunk, bytes - off);
+        if (save) {
+            CUDA_TRY(cudaMemcpyAsync(stage, dev + off, n, cudaMemcpyDeviceToHost, h->stream));
+            CUDA_TRY(cudaStreamSynchronize(h->stream));
+            if (fwrite(stage, 1, n, f) != n) return fail(NUOSC_ERR_INVALID, "checkpoint: write failed");
+        } else {
+            if (fread(stage, 1, n, f) != n) return fail(NUOSC_ERR_INVALID, "checkpoint: file is truncated");
+            CUDA_TRY(cudaMemcpyAsync(dev + off, stage, n, cudaMemcpyHostToDevice, h->stream));
+            CUDA_TRY(cudaStreamSynchronize(h->stream));
+        }
+    }
+    return 0;
+}
+
+int ck_transfer(nuosc_handle *h, FILE *f, bool save, bool moments) {
+    char *stage = nullptr;
+    CUDA_TRY(cudaMallocHost((void **)&stage, kCkChunk));
+    int rc = ck_copy(h, f, (char *)h->reg[0], (size_t)h->g.fs * NF * h->esize, save, stage);
+    if (!rc && moments) rc = ck_copy(h, f, (char *)h->d_mom, (size_t)h->g.ncell * NMOM * sizeof(double), save, stage);
+    cudaFreeHost(stage);
+    return rc;
+}
+}  // namespace
+
+int nuosc_save_checkpoint(nuosc_handle *h, const char *path) {
+    HANDLE_CHECK(h);
+    if (!path) return fail(NUOSC_ERR_INVALID, "null path");
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    if (int rc = check_status(h)) return rc;
+    CkHeader c{};
+    c.version = 1;
+    c.precision = h->precision;
+    c.nx = h->g.nx; c.nz = h->g.nz; c.nv = h->g.nv; c.nvs = h->g.nvs;
+    c.ghost = h->ko6 ? 3 : 2;
+    c.renorm = h->renorm;
+    c.mom_valid = h->mom_valid;
+    c.steps_done = h->steps_done;
+    c.x0 = h->x0; c.x1 = h->x1; c.z0 = h->z0; c.z1 = h->z1; c.dx = h->dx; c.dz = h->dz; c.dt = h->dt;
+    c.ko = h->ko; c.mu = h->mu; c.pmo = h->pmo; c.phy_time = h->phy_time; c.n0 = h->n_nue0[0]; c.n1 = h->n_nue0[1];
+    FILE *f = fopen(path, "wb");
+    if (!f) return fail(NUOSC_ERR_INVALID, "cannot open %s", path);
+    const bool ok = fwrite(kCkMagic, 1, 8, f) == 8 && fwrite(&c, sizeof c, 1, f) == 1 &&
+                    fwrite(h->G0.data(), sizeof(double), h->g.nv, f) == (size_t)h->g.nv &&
+                    fwrite(h->G0b.data(), sizeof(double), h->g.nv, f) == (size_t)h->g.nv;
+    int rc = ok ? ck_transfer(h, f, true, h->mom_valid) : fail(NUOSC_ERR_INVALID, "checkpoint: write failed");
+    if (fclose(f) != 0 && !rc) rc = fail(NUOSC_ERR_INVALID, "checkpoint: closing %s failed", path);
+    return rc;
+}
+
+int nuosc_load_checkpoint(nuosc_handle *h, const char *path) {
+    HANDLE_CHECK(h);
+    if (!path) return fail(NUOSC_ERR_INVALID, "null path");
+    FILE *f = fopen(path, "rb");
+    if (!f) return fail(NUOSC_ERR_INVALID, "cannot open %s", path);
+    char magic[8];
+    CkHeader c{};
+    int rc = 0;
+    if (fread(magic, 1, 8, f) != 8 || memcmp(magic, kCkMagic, 8) || fread(&c, sizeof c, 1, f) != 1 || c.version != 1)
+        rc = fail(NUOSC_ERR_INVALID, "%s is not a checkpoint of this library", path);
+    else if (c.precision != h->precision || c.nx != h->g.nx || c.nz != h->g.nz || c.nv != h->g.nv ||
+             c.nvs != h->g.nvs || c.ghost != (h->ko6 ? 3 : 2) || c.dx != h->dx || c.dz != h->dz || c.dt != h->dt ||
+             c.ko != h->ko)
+        rc = fail(NUOSC_ERR_INVALID, "checkpoint %s: grid %dx%dx%d (precision %d, ghost %d) does not match the handle",
+                  path, c.nx, c.nz, c.nv, c.precision, c.ghost);
+    std::vector<double> G0(c.nv > 0 ? c.nv : 0), G0b(G0.size());
+    if (!rc && (fread(G0.data(), sizeof(double), G0.size(), f) != G0.size() ||
+                fread(G0b.data(), sizeof(double), G0b.size(), f) != G0b.size()))
+        rc = fail(NUOSC_ERR_INVALID, "checkpoint: file is truncated");
+    if (!rc) {
+        CUDA_TRY(cudaStreamSynchronize(h->stream));
+        h->G0 = G0;
+        h->G0b = G0b;
+        rc = upload_spectra(h);
+    }
+    if (!rc) rc = ck_transfer(h, f, false, c.mom_valid != 0);
+    fclose(f);
+    if (rc) {
+        h->mom_valid = false;
+        return rc;
+    }
+    h->mom_valid = c.mom_valid != 0;
+    h->steps_done = c.steps_done;
+    h->phy_time = c.phy_time;
+    h->n_nue0[0] = c.n0;
+    h->n_nue0[1] = c.n1;
+    h->mu = c.mu;
+    h->pmo = c.pmo;
+    h->renorm = c.renorm != 0;
     return NUOSC_OK;
 }
 

@@ -15,6 +15,20 @@
 namespace nuosc {
 
 constexpr int NF = 8;  // ee, mm, emr, emi, bee, bmm, bemr, bemi
+
+// Seeded draws of the initial data: a counter-based hash (splitmix64
+// finaliser) of (seed, i, j), uniform in [0, 1) with 53 bits; host and device
+// give the same value.  Replaces the reference's rand() (nuosc_init.cpp:5, 33).
+__host__ __device__ inline uint64_t mix64(uint64_t z) {
+    z += 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+__host__ __device__ inline double seeded_uniform(uint64_t seed, int i, int j) {
+    const uint64_t key = ((uint64_t)(uint32_t)i << 32) | (uint64_t)(uint32_t)j;
+    return (double)(mix64(mix64(seed) ^ key) >> 11) * 0x1.0p-53;
+}
 constexpr int NMOM = 12;  // emRm[4], emIp[4], eemm[4] (nuosc_class.cpp:28-31)
 
 struct Geom {
@@ -174,7 +188,7 @@ cudaError_t launch_moment_finalize(const double *part, double *mom, Geom g, int 
 
 template <typename T>
 cudaError_t launch_init(T *reg, const double *G0, const double *G0b, Geom g, int ipt, double eps0,
-                        double sigma, double z0, double dz, uint64_t seed, cudaStream_t s);
+                        double sigma, double z0, double dz, uint64_t seed, const double *zprof, cudaStream_t s);
 // Analysis partial sums; `part` holds ANA_BLOCKS * ANA_NQ doubles, `out` ANA_NQ.
 constexpr int ANA_NQ = 12;
 constexpr int ANA_BLOCKS = 296;

@@ -148,19 +148,22 @@ cudaError_t launch_stage_direct(const StageArgs<T> &a, int mode, bool ko6, cudaS
 
 // ----------------------------------------------------------------------------
 // Seeded initial data (nuosc_init.cpp:70-127), one thread per (cell, v).
-// The perturbation of cell (i,j) is a counter-based hash of (seed, i, j), so
-// it is independent of the launch shape and identical to the host oracle's.
+// The perturbation of cell (i,j) is a counter-based hash of (seed, i, j)
+// (seeded_uniform), so it is independent of the launch shape and identical to
+// the host oracle's.
 // ----------------------------------------------------------------------------
-__device__ __forceinline__ uint64_t mix64(uint64_t z) {
-    z += 0x9E3779B97F4A7C15ull;
-    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
-    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
-    return z ^ (z >> 31);
-}
 
+// Initial data (fillInitValue, nuosc_init.cpp:24-130, and the advection
+// tests fillInitAdvtest / fillInitSquare / fillInitTriangle, :162-230):
+//   ipt 0..3   the generic branch: P1 = t(z or cell), P3 = sqrt(1 - t^2)
+//   ipt 4      the "NOC" branch: P1, P2 = zprof[j], zprof[nz + j] (a sum of
+//              Fourier modes in z computed on the host), P3 = sqrt(1 - P1^2 - P2^2)
+//   ipt 10/20/30  ee = the test profile in z (Advtest, Square, Triangle), all
+//              other fields 0 (G0 = G0b = 1)
+// Arithmetic is kept in the reference's order without FMA contraction.
 template <typename T>
 __global__ void k_init(T *reg, const double *G0, const double *G0b, Geom g, int ipt, double eps0, double sigma,
-                       double z0, double dz, uint64_t seed) {
+                       double z0, double dz, uint64_t seed, const double *zprof) {
     const int v = blockIdx.y * 32 + threadIdx.x;
     const long long cell = (long long)blockIdx.x * 8 + threadIdx.y;
     if (cell >= g.ncell || v >= g.nvs) return;
@@ -172,12 +175,46 @@ __global__ void k_init(T *reg, const double *G0, const double *G0b, Geom g, int 
         return;
     }
     const double Zj = __dadd_rn(z0, __dmul_rn(j + 0.5, dz));
+    if (ipt >= 10) {
+        double t = 0.0;
+        const double s2 = __dmul_rn(sigma, sigma);
+        if (ipt == 10) {  // nuosc_init.cpp:172-176
+            const double sd = 0.33, zs = __dadd_rn(Zj, -sd), zp = __dadd_rn(Zj, sd);
+            t = __dadd_rn(exp(-__dmul_rn(Zj, Zj) / __dmul_rn(1.0, s2)), __dmul_rn(zp, zp) <= s2 ? 1.0 : 0.0);
+            // (sigma + Z) - sd and (sigma - Z) + sd, in the reference's evaluation order
+            t = __dadd_rn(t, (zs < 0 && zs > -sigma) ? __dadd_rn(__dadd_rn(sigma, Zj), -sd) / sigma : 0.0);
+            t = __dadd_rn(t, (zs >= 0 && zs < sigma) ? __dadd_rn(__dadd_rn(sigma, -Zj), sd) / sigma : 0.0);
+            t = __dmul_rn(t, eps0);
+        } else if (ipt == 20) {  // :206-208
+            t = __dmul_rn(Zj, Zj) <= s2 ? eps0 : 0.0;
+        } else {  // :228-230
+            if (Zj < 0 && Zj > -sigma) t = __dmul_rn(__dadd_rn(sigma, Zj), eps0) / sigma;
+            else if (Zj >= 0 && Zj < sigma) t = __dmul_rn(__dadd_rn(sigma, -Zj), eps0) / sigma;
+        }
+        reg[o] = T(t);
+#pragma unroll
+        for (int f = 1; f < NF; ++f) reg[o + f * g.fs] = T(0);
+        return;
+    }
+    if (ipt == 4) {  // nuosc_init.cpp:47-62, every x
+        const double tr = zprof[j], ti = zprof[g.nz + j];
+        const double t2 = __dsqrt_rn(__dadd_rn(__dadd_rn(1.0, -__dmul_rn(tr, tr)), -__dmul_rn(ti, ti)));
+        const double hG = __dmul_rn(0.5, G0[v]), hGb = __dmul_rn(0.5, G0b[v]);
+        reg[o + 0 * g.fs] = T(__dmul_rn(hG, __dadd_rn(1.0, t2)));
+        reg[o + 1 * g.fs] = T(__dmul_rn(hG, __dadd_rn(1.0, -t2)));
+        reg[o + 2 * g.fs] = T(__dmul_rn(hG, tr));
+        reg[o + 3 * g.fs] = T(__dmul_rn(hG, ti));
+        reg[o + 4 * g.fs] = T(__dmul_rn(hGb, __dadd_rn(1.0, t2)));
+        reg[o + 5 * g.fs] = T(__dmul_rn(hGb, __dadd_rn(1.0, -t2)));
+        reg[o + 6 * g.fs] = T(__dmul_rn(hGb, tr));
+        reg[o + 7 * g.fs] = T(-__dmul_rn(hGb, ti));
+        return;
+    }
     double t;
     if (ipt == 0) {
         t = eps0 * exp(-Zj * Zj / (2.0 * sigma * sigma));
     } else if (ipt == 1) {
-        const uint64_t key = ((uint64_t)(uint32_t)i << 32) | (uint64_t)(uint32_t)j;
-        const double u = (double)(mix64(mix64(seed) ^ key) >> 11) * 0x1.0p-53;
+        const double u = seeded_uniform(seed, i, j);
         t = __dmul_rn(eps0, __dadd_rn(__dmul_rn(2.0, u), -1.0));
     } else if (ipt == 2) {
         t = eps0 * (1.0 + cos(2 * 3.14159265358979323846 * Zj / (2.0 * sigma * sigma))) * 0.5;
@@ -199,10 +236,10 @@ __global__ void k_init(T *reg, const double *G0, const double *G0b, Geom g, int 
 
 template <typename T>
 cudaError_t launch_init(T *reg, const double *G0, const double *G0b, Geom g, int ipt, double eps0, double sigma,
-                        double z0, double dz, uint64_t seed, cudaStream_t s) {
+                        double z0, double dz, uint64_t seed, const double *zprof, cudaStream_t s) {
     dim3 block(32, 8);
     dim3 grid((unsigned)((g.ncell + 7) / 8), (g.nvs + 31) / 32);
-    k_init<T><<<grid, block, 0, s>>>(reg, G0, G0b, g, ipt, eps0, sigma, z0, dz, seed);
+    k_init<T><<<grid, block, 0, s>>>(reg, G0, G0b, g, ipt, eps0, sigma, z0, dz, seed, zprof);
     return cudaGetLastError();
 }
 
@@ -211,7 +248,8 @@ cudaError_t launch_init(T *reg, const double *G0, const double *G0b, Geom g, int
 // ten full-size temporaries: each block reduces a fixed, strided set of cells
 // to ANA_NQ partials; a one-block pass sums the partials in block order.
 // Quantities: 0 maxdP, 1 sum w ee, 2 sum w bee, 3 sum w G dP, 4 sum w Gb dPb,
-// 5..7 aM01..aM03, 8 sum w G, 9 sum w Gb, 10 non-finite count.
+// 5..7 aM01..aM03, 8 sum w G, 9 sum w Gb, 10 non-finite count, 11 sum w ee^2
+// (with 1 and 8 the advection test's integrals I1, I2, nuosc_ana.cpp:58-61).
 // ----------------------------------------------------------------------------
 template <typename T>
 __global__ void __launch_bounds__(256) k_analysis(const T *__restrict__ st, const double *__restrict__ G0,
@@ -243,6 +281,7 @@ __global__ void __launch_bounds__(256) k_analysis(const T *__restrict__ st, cons
             q[7] += w * 0.5 * (ee - mm - bee + bmm);
             q[8] += w * G;
             q[9] += w * Gb;
+            q[11] += w * ee * ee;
             const double chk = ee + mm + emr + emi + bee + bmm + bemr + bemi;
             if (!isfinite(chk)) q[10] += 1.0;
         }
@@ -425,7 +464,7 @@ cudaError_t launch_renormalize(T *reg, const double *G0, const double *G0b, Geom
     template cudaError_t launch_moments<T>(const T *, double *, Quad, Geom, cudaStream_t);                    \
     template cudaError_t launch_stage_direct<T>(const StageArgs<T> &, int, bool, cudaStream_t);              \
     template cudaError_t launch_init<T>(T *, const double *, const double *, Geom, int, double, double, double, \
-                                        double, uint64_t, cudaStream_t);                                      \
+                                        double, uint64_t, const double *, cudaStream_t);                      \
     template cudaError_t launch_analysis<T>(const T *, const double *, const double *, const double *, Geom,   \
                                             double *, double *, cudaStream_t);                                \
     template cudaError_t launch_gather<T>(const T *, int, const int *, int, const int *, int, const double *,  \

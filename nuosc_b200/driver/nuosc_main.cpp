@@ -6,8 +6,11 @@
 // every DUMP_EVERY steps, printing the wall time per step in the reference's
 // "ns/step-grid" form and the closing [Summ] line.  The solve runs on one GPU
 // through the C ABI (nuosc_b200.hpp).  Differences: --np must be 1 1 (one
-// GPU per solve); --ipt 1 draws the perturbation from --seed instead of
-// rand(); extra flags --precision (0 FP64, 1 FP32), --seed and --device.
+// GPU per solve); --ipt 1 and --ipt 4 draw the perturbation from --seed
+// instead of rand() (ipt 4 for every x, not only the x = 0 column); --ipt
+// 10/20/30 run the advection tests, which the reference selects only when
+// built with ADV_TEST (nuosc.cpp:155-158), and print I1, I2; extra flags
+// --precision (0 FP64, 1 FP32), --seed and --device.
 #include "../../include/nuosc_b200.hpp"
 
 #include <chrono>
@@ -91,8 +94,15 @@ int main(int argc, char *argv[]) {
         state.set_renorm(renorm);
         printf("   Setting mu = %f\n   Setting pmo = %f\n   Setting renorm = %d\n", mu, pmo, (int)renorm);
         state.open_analysis_file("analysis.dat");
-        state.fillInitValue(ipt, alpha, eps0, sigma, lnue, lnueb, lnuex, lnuebx, seed);
-        state.analysis(true);
+        // ipt 10/20/30: the advection tests, which the reference's driver selects
+        // when built with ADV_TEST (nuosc.cpp:155-158); their analysis line
+        // prints the integrals I1, I2
+        const bool adv = ipt == 10 || ipt == 20 || ipt == 30;
+        if (ipt == 10) state.fillInitAdvtest(eps0, sigma);
+        else if (ipt == 20) state.fillInitSquare(eps0, sigma);
+        else if (ipt == 30) state.fillInitTriangle(eps0, sigma);
+        else state.fillInitValue(ipt, alpha, eps0, sigma, lnue, lnueb, lnuex, lnuebx, seed);
+        state.analysis(true, adv);
 
         if (DUMP_EVERY <= END_STEP) {
             std::vector<int> vslice;
@@ -111,7 +121,7 @@ int main(int argc, char *argv[]) {
                 t1 = std::chrono::high_resolution_clock::now();
             }
             state.step_rk4(1);
-            if (t % ANAL_EVERY == 0) state.analysis(true);
+            if (t % ANAL_EVERY == 0) state.analysis(true, adv);
             if (t % DUMP_EVERY == 0) state.checkSnapShot(t);
             if (t == 5 || t == 10 || t == 100 || t == 1000 || t == END_STEP) {
                 nuosc_synchronize(state.handle());

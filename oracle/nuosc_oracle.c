@@ -14,6 +14,9 @@
  *   icosahedron.h:36-171, Point.h:64-69   velocity quadrature (Voronoi weights)
  *   CartGrid.cpp:191-208, CartGrid.h:91    geometry and ghosted index
  *   nuosc_init.cpp:8-10,70-130             initial data (seeded epsilon injected)
+ *   nuosc_init.cpp:11-14,24-68             "NOC" initial data (ipt 4; seeded phases, every x)
+ *   nuosc_init.cpp:162-230                 advection tests (ipt 10 Advtest, 20 Square, 30 Triangle)
+ *   nuosc_ana.cpp:58-61,121                the advection test's integrals I1, I2
  *   nuosc_boundary.cpp:4-52                periodic ghost fill
  *   nuosc_class.cpp:11-307                 calRHS (moments, commutator, ADV, KO, vacuum)
  *   nuosc_class.cpp:313-372,374-427        vectorize and step_rk4
@@ -174,6 +177,8 @@ typedef struct orc_sim {
     double n_nue0[2];
     long lpts;
     double *reg[4][NF]; /* 0 stat, 1 rhs, 2 pre, 3 cor */
+    double *noc_phi;    /* explicit ipt = 4 phases (orc_set_noc_phases), or NULL: seeded */
+    int noc_nphi;
 } orc_sim;
 
 static inline long gidx(const orc_sim *s, int i, int j, int v) {
@@ -215,6 +220,7 @@ void orc_destroy(orc_sim *s) {
     for (int r = 0; r < 4; ++r)
         for (int f = 0; f < NF; ++f) free(s->reg[r][f]);
     free(s->vx); free(s->vy); free(s->vz); free(s->vw); free(s->G0); free(s->G0b);
+    free(s->noc_phi);
     free(s);
 }
 
@@ -239,8 +245,13 @@ static double gspec(double vx, double vz, double sx, double sz) {
  * 2: eps_p profile, 3: constant eps0.  lnuex/lnuebx <= 0 mean "infinite"
  * (the reference default DBL_MAX, nuosc.cpp:36-37).
  */
+static void fill_noc(orc_sim *s, double alpha, double lnue, double lnueb, uint64_t seed);
+static void fill_advtest(orc_sim *s, int ipt, double eps0, double sigma);
+
 void orc_fill_init(orc_sim *s, int ipt, double alpha, double eps0, double sigma, double lnue,
                    double lnueb, double lnuex, double lnuebx, uint64_t seed) {
+    if (ipt == 4) { fill_noc(s, alpha, lnue, lnueb, seed); return; }
+    if (ipt >= 10) { fill_advtest(s, ipt, eps0, sigma); return; }
     if (lnuex <= 0) lnuex = DBL_MAX;
     if (lnuebx <= 0) lnuebx = DBL_MAX;
     double ing0 = 0, ing1 = 0;
@@ -287,6 +298,129 @@ void orc_fill_init(orc_sim *s, int ipt, double alpha, double eps0, double sigma,
     s->n_nue0[1] = n01 * s->ds_L;
     s->phy_time = 0.0;
     free(ng); free(ngb);
+}
+
+/* Phases of the ipt = 4 initial data: n = 2 (nz/20) + 1 values (NULL: back
+ * to the seeded phases).  Lets a test feed the reference's rand() phases. */
+void orc_set_noc_phases(orc_sim *s, int n, const double *phi) {
+    free(s->noc_phi);
+    s->noc_phi = NULL;
+    s->noc_nphi = 0;
+    if (phi && n > 0) {
+        s->noc_phi = (double *)malloc(sizeof(double) * n);
+        memcpy(s->noc_phi, phi, sizeof(double) * n);
+        s->noc_nphi = n;
+    }
+}
+
+/* spectrum of the NOC branch: normalised over vz in [-1, 1] by erf (nuosc_init.cpp:11-14) */
+static double gnoc(double v, double sigma) {
+    const double v0 = 1.0;
+    const double N = sigma * sqrt(0.5 * M_PI) * (erf((1.0 + v0) / sigma / sqrt(2.0)) + erf((1.0 - v0) / sigma / sqrt(2.0)));
+    return exp(-(v - v0) * (v - v0) / (2.0 * sigma * sigma)) / N;
+}
+
+/*
+ * ipt = 4, the "NOC" branch (nuosc_init.cpp:24-68), restated for every x (the
+ * reference fills only the x = 0 column): amax = nz/20 modes k = -amax ..
+ * amax-1, k != 0, of amplitude 1e-7/|k| and phase phi[k + amax], with
+ * phi[m] = 2 pi U(seed, m, -1) unless explicit phases were set; P1, P2 =
+ * their cos and sin sums, P3 = sqrt(1 - P1^2 - P2^2); bemi = -emi.  n_nue0
+ * is set from the filled state (the reference leaves it unset here).
+ */
+static void fill_noc(orc_sim *s, double alpha, double lnue, double lnueb, uint64_t seed) {
+    const int amax = s->nz / 2 / 10;
+    double *phi = (double *)malloc(sizeof(double) * (2 * amax + 1));
+    for (int m = 0; m <= 2 * amax; ++m)
+        phi[m] = (s->noc_phi && m < s->noc_nphi) ? s->noc_phi[m] : 2.0 * M_PI * orc_uniform(seed, m, -1);
+    for (int v = 0; v < s->nv; ++v) {
+        s->G0[v] = gnoc(s->vz[v], lnue);
+        s->G0b[v] = alpha * gnoc(s->vz[v], lnueb);
+    }
+    const double pi2oL = 2.0 * M_PI / (s->z0 - s->z1);
+    double n00 = 0, n01 = 0;
+    double **st = s->reg[0];
+    for (int j = 0; j < s->nz; ++j) {
+        const double Zj = s->z0 + (j + 0.5) * s->dz;
+        double tr = 0.0, ti = 0.0;
+        for (int k = -amax; k < amax; ++k) {
+            if (k == 0) continue;
+            tr += 1.e-7 / abs(k) * cos(pi2oL * k * Zj + phi[k + amax]);
+            ti += 1.e-7 / abs(k) * sin(pi2oL * k * Zj + phi[k + amax]);
+        }
+        const double t2 = sqrt(1.0 - tr * tr - ti * ti);
+        for (int i = 0; i < s->nx; ++i)
+            for (int v = 0; v < s->nv; ++v) {
+                const long q = gidx(s, i, j, v);
+                const double G = s->G0[v], Gb = s->G0b[v];
+                st[0][q] = 0.5 * G * (1.0 + t2);
+                st[1][q] = 0.5 * G * (1.0 - t2);
+                st[2][q] = 0.5 * G * tr;
+                st[3][q] = 0.5 * G * ti;
+                st[4][q] = 0.5 * Gb * (1.0 + t2);
+                st[5][q] = 0.5 * Gb * (1.0 - t2);
+                st[6][q] = 0.5 * Gb * tr;
+                st[7][q] = -0.5 * Gb * ti;
+                n00 += s->vw[v] * st[0][q];
+                n01 += s->vw[v] * st[4][q];
+            }
+    }
+    s->n_nue0[0] = n00 * s->ds_L;
+    s->n_nue0[1] = n01 * s->ds_L;
+    s->phy_time = 0.0;
+    free(phi);
+}
+
+/*
+ * ipt = 10 fillInitAdvtest, 20 fillInitSquare, 30 fillInitTriangle
+ * (nuosc_init.cpp:162-230): G0 = G0b = 1, ee = the profile in z, the other
+ * fields 0.  n_nue0 is set from the filled state.
+ */
+static void fill_advtest(orc_sim *s, int ipt, double eps0, double sigma) {
+    for (int v = 0; v < s->nv; ++v) s->G0[v] = s->G0b[v] = 1.0;
+    double n00 = 0;
+    for (int j = 0; j < s->nz; ++j) {
+        const double Z = s->z0 + (j + 0.5) * s->dz;
+        double t = 0.0;
+        if (ipt == 10) {
+            const double sd = 0.33;
+            t = exp(-(Z * Z) / (1.0 * sigma * sigma)) + ((Z + sd) * (Z + sd) <= sigma * sigma) +
+                (int)(Z - sd < 0 && Z - sd > -sigma) * (sigma + Z - sd) / sigma +
+                (int)(Z - sd >= 0 && Z - sd < sigma) * (sigma - Z + sd) / sigma;
+            t = t * eps0;
+        } else if (ipt == 20) {
+            if (Z * Z <= sigma * sigma) t = eps0;
+        } else {
+            if (Z < 0 && Z > -sigma) t = (sigma + Z) * eps0 / sigma;
+            else if (Z >= 0 && Z < sigma) t = (sigma - Z) * eps0 / sigma;
+        }
+        for (int i = 0; i < s->nx; ++i)
+            for (int v = 0; v < s->nv; ++v) {
+                const long q = gidx(s, i, j, v);
+                s->reg[0][0][q] = t;
+                for (int f = 1; f < NF; ++f) s->reg[0][f][q] = 0.0;
+                n00 += s->vw[v] * t;
+            }
+    }
+    s->n_nue0[0] = n00 * s->ds_L;
+    s->n_nue0[1] = 0.0;
+    s->phy_time = 0.0;
+}
+
+/* The advection test's integrals (nuosc_ana.cpp:58-61,121): I1 = sum w ee / nor,
+ * I2 = sum w ee^2 / nor, nor = sum w G0 over all cells. */
+void orc_adv_integrals(const orc_sim *s, double *out) {
+    double I1 = 0, I2 = 0, nor = 0;
+    for (int i = 0; i < s->nx; ++i)
+        for (int j = 0; j < s->nz; ++j)
+            for (int v = 0; v < s->nv; ++v) {
+                const double ee = s->reg[0][0][gidx(s, i, j, v)];
+                I1 += s->vw[v] * ee;
+                I2 += s->vw[v] * ee * ee;
+                nor += s->vw[v] * s->G0[v];
+            }
+    out[0] = I1 / nor;
+    out[1] = I2 / nor;
 }
 
 /* Set G0/G0b directly (used with externally supplied state). */

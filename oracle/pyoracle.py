@@ -73,6 +73,9 @@ def _oracle_lib():
         lib.orc_nv.argtypes = [_I]
         lib.orc_uniform.restype = _D
         lib.orc_uniform.argtypes = [C.c_uint64, _I, _I]
+        lib.orc_set_noc_phases.argtypes = [_P, _I, _DP]
+        lib.orc_adv_integrals.argtypes = [_P, _DP]
+        lib.orc_adv_integrals.restype = None
         _olib = lib
     return _olib
 
@@ -154,6 +157,20 @@ class Oracle(_Sim):
 
     def set_time(self, t):
         self.lib.orc_set_time(self.h, t)
+
+    def set_noc_phases(self, phi):
+        """Explicit phases of the ipt = 4 initial data (None: the seeded ones)."""
+        if phi is None:
+            self.lib.orc_set_noc_phases(self.h, 0, None)
+        else:
+            phi = np.ascontiguousarray(phi, dtype=np.float64)
+            self.lib.orc_set_noc_phases(self.h, len(phi), _dp(phi))
+
+    def adv_integrals(self):
+        """(I1, I2) of the advection test (nuosc_ana.cpp:58-61)."""
+        out = np.zeros(2)
+        self.lib.orc_adv_integrals(self.h, _dp(out))
+        return out
 
     def calrhs(self):
         self.lib.orc_calrhs(self.h, 1, 0)

@@ -126,6 +126,15 @@ void ref_fill_init(void *h, int ipt, double alpha, double eps0, double sigma, do
     NuOsc *s = ((RefSim *)h)->s;
     if (lnuex <= 0) lnuex = DBL_MAX;
     if (lnuebx <= 0) lnuebx = DBL_MAX;
+    // the advection tests, selected by ipt in the reference's ADV_TEST driver (nuosc.cpp:155-158)
+    if (ipt == 10 || ipt == 20 || ipt == 30) {
+        quiet([&] {
+            if (ipt == 10) s->fillInitAdvtest(eps0, sigma);
+            else if (ipt == 20) s->fillInitSquare(eps0, sigma);
+            else s->fillInitTriangle(eps0, sigma);
+        });
+        return;
+    }
     if (ipt != 1) {
         quiet([&] { s->fillInitValue(ipt, alpha, eps0, sigma, lnue, lnueb, lnuex, lnuebx); });
         return;

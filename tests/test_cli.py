@@ -58,3 +58,23 @@ def test_cli_rejects_two_process_grid(gpu, tmp_path):
                        capture_output=True, text=True, timeout=300)
     assert r.returncode != 0
     assert r.stderr.strip()
+
+
+ADV_FLAGS = ["--ipt", "10", "--nv", "2", "--gz", "2", "--dz", "0.02", "--zmax", "0.5", "--mu", "0", "--pmo", "0",
+             "--eps0", "1", "--sigma", ".2", "--ko", "0.8", "--cfl", "0.25", "--END_STEP_T", ".5",
+             "--ANA_EVERY_T", ".1"]
+
+
+def test_cli_advection_unit_test(gpu, tmp_path):
+    """The reference's `make test2d_advec` run (Makefile:24-30, the UNITTEST
+    flags with --gz 2) through --ipt 10: 100 steps of pure advection with
+    4th-difference KO; the printed I1 (particle number) stays constant and I2
+    falls."""
+    r = subprocess.run([EXE] + ADV_FLAGS, cwd=tmp_path, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
+    rows = [line.split() for line in r.stdout.splitlines() if line.startswith("T=") and "I1=" in line]
+    assert len(rows) == 6  # t = 0 and every 20 steps
+    I1 = np.array([float(x[x.index("I1=") + 1]) for x in rows])
+    I2 = np.array([float(x[x.index("I2=") + 1]) for x in rows])
+    np.testing.assert_allclose(I1, I1[0], rtol=1e-4)  # printed with 5 digits
+    assert np.all(np.diff(I2) < 0)

@@ -302,7 +302,7 @@ def test_error_paths(nb):
     with pytest.raises(nb.NuoscError):
         s.updatePeriodicBoundary(7)
     with pytest.raises(nb.NuoscError) as e:
-        s.fillInitValue(4, **PHYS)
+        s.fillInitValue(5, **PHYS)
     assert e.value.code == 6
     # a non-finite state is reported by analysis() as a numeric error
     s.fillInitValue(1, seed=1, **PHYS)
@@ -378,12 +378,13 @@ def _tma_solve(nb, p, ko_order, seed, steps, tile=None, **phys):
     return s
 
 
-def _oracle_solve(p, ko_order, seed, steps, **phys):
+def _oracle_solve(p, ko_order, seed, steps, ipt=1, **phys):
     x0, x1, dx, cfl, ko, mu, pmo, nn = p
     o = po.Oracle(nn=int(nn), x0=x0, x1=x1, z0=x0, z1=x1, dx=dx, dz=dx, cfl=cfl, ko=ko, ko_order=ko_order, mu=mu,
                   pmo=pmo)
-    o.fill_init(ipt=1, seed=seed, **phys)
-    o.step(steps)
+    o.fill_init(ipt=ipt, seed=seed, **phys)
+    if steps:
+        o.step(steps)
     return o
 
 
@@ -466,3 +467,65 @@ def test_fp32_moment_summation_variants(nb):
         s.close()
     assert errs[1] < 1e-12, errs
     assert errs[0] > errs[1]
+
+
+ADV = dict(eps0=1.0, sigma=0.2)  # the reference's advection unit test (Makefile:24-30)
+
+
+def _adv_params(n, dx=0.02):
+    x0, x1 = po.box(n, dx)
+    return (x0, x1, dx, 0.25, 0.8, 0.0, 0.0, 2)
+
+
+@pytest.mark.parametrize("ipt", [10, 20, 30])
+def test_advection_initial_data_against_oracle(nb, ipt):
+    p = _adv_params(50)
+    s = make(nb, p, 4)
+    s.fillInitValue(ipt, 0.9, ADV["eps0"], ADV["sigma"], 0.6, 0.5)
+    o = _oracle_solve(p, 4, 0, 0, ipt=ipt, **ADV)
+    assert po.relerr(s.get_state(), o.get_state(0)) < 1e-15
+    np.testing.assert_array_equal(s.G0, np.ones(s.grid.nv))
+    s.close()
+
+
+@pytest.mark.parametrize("n,kernel", [(50, None), (64, 3)])
+def test_advection_test_against_oracle(nb, n, kernel):
+    """fillInitAdvtest with mu = pmo = 0 (the reference's `make test2d_advec`
+    physics, 4th-difference KO 0.8, CFL 0.25), 20 steps: the state within 1e-12
+    of the oracle, the I1/I2 integrals of analysis() equal the oracle's, and
+    I1 is conserved.  50x50 runs the cp.async/direct kernels (nz % 8 != 0),
+    64x64 the TMA kernel."""
+    p = _adv_params(n)
+    s = make(nb, p, 4, kernel=kernel)
+    s.fillInitValue(10, 0.9, ADV["eps0"], ADV["sigma"], 0.6, 0.5)
+    d0 = s.analysis()
+    s.step_rk4(20)
+    d1 = s.analysis()
+    o = _oracle_solve(p, 4, 0, 20, ipt=10, **ADV)
+    a, b = s.get_state(), o.get_state(0)
+    for f in range(8):
+        assert po.relerr(a[f], b[f]) < FP64_TOL, f
+    np.testing.assert_allclose([d1["I1"], d1["I2"]], o.adv_integrals(), rtol=1e-11)
+    assert abs(d1["I1"] - d0["I1"]) < 1e-11 * abs(d0["I1"])
+    assert d1["I2"] < d0["I2"]
+    s.close()
+
+
+@pytest.mark.parametrize("kernel", KERNELS)
+def test_noc_initial_data_against_oracle(nb, kernel):
+    """ipt = 4 ("NOC" Fourier-phase perturbation, seeded phases, every x)
+    against the oracle's restatement: the initial state to 1e-15, then 10 steps
+    on each stage kernel within 1e-12."""
+    p = box_params(64, 2)
+    s = make(nb, p, 6)
+    s.fillInitValue(4, 0.9, 1e-6, 1.0, 0.6, 0.5, seed=77)
+    o = _oracle_solve(p, 6, 77, 0, ipt=4, alpha=0.9, eps0=1e-6, sigma=1.0, lnue=0.6, lnueb=0.5)
+    assert po.relerr(s.get_state(), o.get_state(0)) < 1e-15
+    np.testing.assert_allclose(s.n_nue0, o.info()["n_nue0"], rtol=1e-12)
+    _kernel_ok(nb, s, kernel)
+    s.step_rk4(10)
+    o.step(10)
+    a, b = s.get_state(), o.get_state(0)
+    for f in range(8):
+        assert po.relerr(a[f], b[f]) < FP64_TOL, f
+    s.close()
