@@ -198,6 +198,47 @@ int nuosc_add_snapshot_at_xv(nuosc_handle *h, const int *fields, int nfields, co
                              const int *xidx, int n_xidx, const int *vidx, int n_vidx);
 int nuosc_check_snapshot(nuosc_handle *h, int t);
 
+/* ---- spatial domain decomposition: x-slabs ------------------------------
+ * Replaces the reference's CartGrid decomposition and halo exchange
+ * (CartGrid.cpp:130-200, 330-440; nuosc_boundary.cpp:64-208) for a split in x
+ * only (the reference's --np px 1).  nuosc_create_slab makes the handle of
+ * slab `rank` of params->px (params->pz must be 1): global box and spacing as
+ * in nuosc_create, the handle owns planes [xoff, xoff + nx) of the global nx
+ * (nx/px each, the first nx%px slabs one more; at least R = gx planes each),
+ * periodic in x across the slabs and in z inside each.  Its stage kernels
+ * read the R planes beyond each side from a halo buffer instead of wrapping,
+ * so before every RK stage k the buffer must hold the neighbours' planes of
+ * stage k's input: nuosc_halo_info lists the 32 pieces (per field, the R
+ * planes to send to each neighbour and where each neighbour's arrive), and
+ * either the caller moves them (NCCL send/recv between processes, one per
+ * GPU) or nuosc_halo_exchange_local copies them between slabs held by one
+ * process on one device.  nuosc_stage runs one stage; a step is stages 0..3,
+ * each preceded by an exchange.  With px = 1 nuosc_step_rk4 does the
+ * exchange itself (the slab is its own neighbour).  Slabs run the TMA stage
+ * kernel only (nz % 8 == 0), cannot join a batch, and their analysis is over
+ * their own cells: reduce nuosc_analysis_sums over the slabs (sum; max for
+ * entry 0) and convert with nuosc_diag_from_sums.  Seeded initial data use
+ * the global x index, so every decomposition gives the same solve. */
+typedef struct nuosc_halo {
+    void *send_lo[8], *send_hi[8]; /* device: the slab's first / last R planes of each field of stage k's input */
+    void *recv_lo[8], *recv_hi[8]; /* device: where the left / right neighbour's last / first R planes go */
+    size_t bytes;                  /* bytes of each piece (R contiguous planes of one field) */
+    int left, right;               /* ranks of the neighbour slabs (periodic in x) */
+} nuosc_halo;
+int nuosc_create_slab(const nuosc_params *params, int rank, nuosc_handle **out);
+int nuosc_get_slab(const nuosc_handle *h, int *px, int *rank, int *xoff, int *nx_global);
+int nuosc_stage(nuosc_handle *h, int k);
+int nuosc_halo_info(const nuosc_handle *h, int k, nuosc_halo *out);
+int nuosc_halo_exchange_local(nuosc_handle *const *slabs, int n, int k);
+/* the raw analysis sums of the handle's cells (12 doubles: 0 max |P|-1 over
+ * both flavours, 1 sum w ee, 2 sum w bee, 3 sum w G dP, 4 sum w Gb dPb,
+ * 5..7 the ELN moments, 8 sum w G, 9 sum w Gb, 10 non-finite count,
+ * 11 sum w ee^2), and the diagnostics record of (reduced) sums */
+int nuosc_analysis_sums(nuosc_handle *h, double *sums);
+int nuosc_diag_from_sums(const nuosc_handle *h, const double *sums, nuosc_diag *out);
+/* initial number densities n_nue0 (NuOsc::n_nue0) -- of the whole solve, for slabs */
+int nuosc_set_n_nue0(nuosc_handle *h, double n0, double n1);
+
 /* Checkpoint and restart of a solve (no counterpart in the reference, which
  * only writes slices).  save writes v_stat (raw, in the handle's precision),
  * the spectra G0/G0b, time, step count, n_nue0, mu, pmo, renorm and the cell

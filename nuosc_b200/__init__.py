@@ -74,14 +74,20 @@ class NuOsc:
     px, pz (must be 1), nv (icosahedron subdivision count), nphi (unused),
     gx, gz (3: 6th-difference KO; 2: 4th-difference KO), the box x0, x1, z0,
     z1, spacings dx, dz, CFL and ko.  Extra keywords: precision (FP64 or
-    FP32), device.
+    FP32), device, and slab_rank: with px > 1 (pz = 1) the handle is x-slab
+    `slab_rank` of the decomposed solve (nuosc_create_slab; see
+    nuosc_b200.slabs), as the reference's constructor takes its rank from MPI.
     """
 
-    def __init__(self, px, pz, nv, nphi, gx, gz, x0, x1, z0, z1, dx, dz, CFL, ko, precision=FP64, device=0):
+    def __init__(self, px, pz, nv, nphi, gx, gz, x0, x1, z0, z1, dx, dz, CFL, ko, precision=FP64, device=0,
+                 slab_rank=None):
         p = _lib.Params(px=px, pz=pz, nv=nv, nphi=nphi, gx=gx, gz=gz, x0=x0, x1=x1, z0=z0, z1=z1, dx=dx, dz=dz,
                         cfl=CFL, ko=ko, precision=precision, device=device)
         h = C.c_void_p()
-        check(lib().nuosc_create(C.byref(p), C.byref(h)))
+        if slab_rank is None:
+            check(lib().nuosc_create(C.byref(p), C.byref(h)))
+        else:
+            check(lib().nuosc_create_slab(C.byref(p), int(slab_rank), C.byref(h)))
         self._h = h
         self.CFL, self.ko, self.precision = CFL, ko, precision
         self.mu, self.pmo, self.renorm = 1.0, 0.1, False  # NuOsc defaults (nuosc_class.h:124-126)

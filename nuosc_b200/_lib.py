@@ -41,6 +41,12 @@ class Geometry(C.Structure):
                 ("device_bytes", C.c_size_t)]
 
 
+class Halo(C.Structure):
+    """nuosc_halo: the 32 halo pieces of one slab for one RK stage."""
+    _fields_ = [("send_lo", C.c_void_p * 8), ("send_hi", C.c_void_p * 8), ("recv_lo", C.c_void_p * 8),
+                ("recv_hi", C.c_void_p * 8), ("bytes", C.c_size_t), ("left", C.c_int), ("right", C.c_int)]
+
+
 class Diag(C.Structure):
     _fields_ = [(n, C.c_double) for n in
                 ("phy_time", "maxdP", "surv", "survb", "avgP", "avgPb", "aM0", "Lex", "ELNe")] + \
@@ -100,6 +106,14 @@ _SIGS = {
     "nuosc_check_snapshot": [_P, _I],
     "nuosc_gather": [_P, _I, _IP, _I, _IP, _I, _DP],
     "nuosc_synchronize": [_P],
+    "nuosc_create_slab": [C.POINTER(Params), _I, C.POINTER(_P)],
+    "nuosc_get_slab": [_P, _IP, _IP, _IP, _IP],
+    "nuosc_stage": [_P, _I],
+    "nuosc_halo_info": [_P, _I, C.POINTER(Halo)],
+    "nuosc_halo_exchange_local": [C.POINTER(_P), _I, _I],
+    "nuosc_analysis_sums": [_P, _DP],
+    "nuosc_diag_from_sums": [_P, _DP, C.POINTER(Diag)],
+    "nuosc_set_n_nue0": [_P, C.c_double, C.c_double],
     "nuosc_save_checkpoint": [_P, C.c_char_p],
     "nuosc_load_checkpoint": [_P, C.c_char_p],
     "nuosc_set_moment_sum": [_P, _I],

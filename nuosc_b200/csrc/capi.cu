@@ -99,6 +99,12 @@ struct nuosc_handle {
     long long launches = 0;
     bool mom_valid = false;  // d_mom holds the moments of v_stat
     unsigned fault_tx = 0;   // self-test of the TMA kernels' bounded waits (nuosc_selftest_overdeclare_tx)
+    // x-slab of a domain-decomposed solve (nuosc_create_slab): slab `rank` of
+    // `px`, global planes xoff .. xoff+nx-1 of nx_global; halo = the R planes
+    // on each side ([8][2R][nz][nvs]) that the halo exchange fills
+    int px = 1, rank = 0, xoff = 0, nx_global = 0;
+    void *halo = nullptr;
+    size_t halo_bytes = 0;
     long long steps_done = 0;  // RK4 steps since the initial data
     nuosc_batch *batch = nullptr;  // the live batch this handle belongs to
 
@@ -319,6 +325,7 @@ int run_stage_xmarch(nuosc_handle *h, bool tma, const XTile &tile, int mode, int
     a.cY = cY;
     a.status = h->d_status;
     a.fault_tx = tma ? h->fault_tx : 0u;
+    a.halo = tma ? (const T *)h->halo : nullptr;
     if (!h->mom_valid) {
         const int ps = h->prof_begin(4);
         CUDA_TRY(launch_moments<T>((const T *)h->reg[in], h->d_mom, a.q, h->g, h->stream));
@@ -368,6 +375,96 @@ int stage_path(nuosc_handle *h, XTile &tile) {
     }
 }
 
+// end of an RK4 step: renormalisation (nuosc_ana.cpp:140-166) and the counters
+template <typename T>
+int finish_step(nuosc_handle *h) {
+    if (h->renorm) {
+        CUDA_TRY(launch_renormalize<T>((T *)h->reg[0], h->dG0(), h->dG0b(), h->g, h->stream));
+        h->launches++;
+        h->mom_valid = false;
+    }
+    h->phy_time += h->dt;
+    h->steps_done++;
+    return 0;
+}
+
+// the stencil input register of stage k of the 13-pass TMA step
+constexpr int kStageInput[4] = {0, 2, 3, 2};
+
+// stage k (0..3) of the 13-pass TMA step (registers 0 U, 2 Y2 then Y4, 3 Y3,
+// 1 B); the step ends with stage 3
+template <typename T>
+int tma_stage(nuosc_handle *h, const XTile &tile, int k) {
+    const double dt = h->dt;
+    int rc;
+    switch (k) {
+    case 0: rc = run_stage_xmarch<T>(h, true, tile, MODE_S1Y, 0, -1, -1, -1, 2, 0.0, 0.5 * dt); break;
+    case 1: rc = run_stage_xmarch<T>(h, true, tile, MODE_S2B, 2, 0, -1, 1, 3, dt, 0.5 * dt); break;
+    case 2: rc = run_stage_xmarch<T>(h, true, tile, MODE_SY, 3, 0, -1, -1, 2, 0.0, dt); break;
+    default: rc = run_stage_xmarch<T>(h, true, tile, MODE_S4B, 2, 0, 1, 0, -1, dt / 6.0, 0.0); break;
+    }
+    if (rc || k < 3) return rc;
+    return finish_step<T>(h);
+}
+
+// The halo pieces of stage k's input of one slab: per field, its first and
+// last R planes (sent to the left / right neighbour) and the places of the
+// neighbours' planes in the halo buffer.
+void halo_pieces(const nuosc_handle *h, int k, nuosc_halo *o) {
+    const int R = h->ko6 ? 3 : 2;
+    const long long P = (long long)h->g.nz * h->g.nvs;
+    char *reg = (char *)h->reg[kStageInput[k]], *halo = (char *)h->halo;
+    for (int f = 0; f < NF; ++f) {
+        o->send_lo[f] = reg + (f * h->g.fs) * (long long)h->esize;
+        o->send_hi[f] = reg + (f * h->g.fs + (long long)(h->g.nx - R) * P) * (long long)h->esize;
+        o->recv_lo[f] = halo + halo_offset(f, -R, h->g.nx, R, P) * (long long)h->esize;
+        o->recv_hi[f] = halo + halo_offset(f, h->g.nx, h->g.nx, R, P) * (long long)h->esize;
+    }
+    o->bytes = (size_t)R * P * h->esize;
+    o->left = (h->rank - 1 + h->px) % h->px;
+    o->right = (h->rank + 1) % h->px;
+}
+
+// Halo exchange of n slabs of one solve held by this process on one device
+// (slab i's neighbours are i-1 and i+1, periodic): every copy runs on slab
+// 0's stream after all slabs' queued work, and every slab's stream waits for
+// the copies, so no stage overwrites a register a copy still reads.
+int halo_exchange_local(nuosc_handle *const *s, int n, int k) {
+    cudaStream_t cs = s[0]->stream;
+    std::vector<cudaEvent_t> evs;
+    auto event_on = [&](cudaStream_t st) -> cudaEvent_t {
+        cudaEvent_t e = nullptr;
+        if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return nullptr;
+        evs.push_back(e);
+        if (cudaEventRecord(e, st) != cudaSuccess) return nullptr;
+        return e;
+    };
+    int rc = 0;
+    for (int i = 1; i < n && !rc; ++i) {
+        cudaEvent_t e = event_on(s[i]->stream);
+        if (!e || cudaStreamWaitEvent(cs, e, 0) != cudaSuccess) rc = fail(NUOSC_ERR_CUDA, "halo exchange: event");
+    }
+    for (int i = 0; i < n && !rc; ++i) {
+        nuosc_halo me, lo, hi;
+        halo_pieces(s[i], k, &me);
+        halo_pieces(s[(i - 1 + n) % n], k, &lo);
+        halo_pieces(s[(i + 1) % n], k, &hi);
+        for (int f = 0; f < NF && !rc; ++f) {
+            if (cudaMemcpyAsync(me.recv_lo[f], lo.send_hi[f], me.bytes, cudaMemcpyDeviceToDevice, cs) != cudaSuccess ||
+                cudaMemcpyAsync(me.recv_hi[f], hi.send_lo[f], me.bytes, cudaMemcpyDeviceToDevice, cs) != cudaSuccess)
+                rc = fail(NUOSC_ERR_CUDA, "halo exchange: copy");
+        }
+    }
+    if (!rc) {
+        cudaEvent_t e = event_on(cs);
+        for (int i = 1; i < n && !rc; ++i)
+            if (!e || cudaStreamWaitEvent(s[i]->stream, e, 0) != cudaSuccess)
+                rc = fail(NUOSC_ERR_CUDA, "halo exchange: event");
+    }
+    for (cudaEvent_t e : evs) cudaEventDestroy(e);  // released once complete
+    return rc;
+}
+
 template <typename T>
 int step_impl(nuosc_handle *h, int nsteps) {
     const double dt = h->dt;
@@ -376,6 +473,11 @@ int step_impl(nuosc_handle *h, int nsteps) {
     if (path < 0) return fail(NUOSC_ERR_UNSUPPORTED, "the requested stage kernel does not support this geometry/tile");
     const bool xm = path > 0, tma = path == 2;
     if (!tma) tile = h->tile;
+    if (h->halo && !tma)
+        return fail(NUOSC_ERR_UNSUPPORTED, "x-slabs of a decomposed solve run on the TMA kernel only (nz %% 8 == 0)");
+    if (h->halo && h->px > 1)
+        return fail(NUOSC_ERR_UNSUPPORTED,
+                    "slab %d of %d: step with nuosc_stage and a halo exchange between the stages", h->rank, h->px);
     if (xm) {
         const size_t need = (size_t)h->g.ncell * xmarch_num_vblocks(h->g, h->tile) * 2 * NMOM * sizeof(double);
         if (int rc = ensure((void **)&h->d_part, &h->part_bytes, need, h)) return rc;
@@ -383,11 +485,12 @@ int step_impl(nuosc_handle *h, int nsteps) {
     for (int n = 0; n < nsteps; ++n) {
         int rc;
         if (tma) {
-            // 13-pass sequence (registers 0 U, 2 Y2 then Y4, 3 Y3, 1 B)
-            if ((rc = run_stage_xmarch<T>(h, tma, tile, MODE_S1Y, 0, -1, -1, -1, 2, 0.0, 0.5 * dt))) return rc;
-            if ((rc = run_stage_xmarch<T>(h, tma, tile, MODE_S2B, 2, 0, -1, 1, 3, dt, 0.5 * dt))) return rc;
-            if ((rc = run_stage_xmarch<T>(h, tma, tile, MODE_SY, 3, 0, -1, -1, 2, 0.0, dt))) return rc;
-            if ((rc = run_stage_xmarch<T>(h, tma, tile, MODE_S4B, 2, 0, 1, 0, -1, dt / 6.0, 0.0))) return rc;
+            for (int k = 0; k < 4; ++k) {
+                nuosc_handle *self = h;  // a single slab is its own neighbour on both sides
+                if (h->halo && (rc = halo_exchange_local(&self, 1, k))) return rc;
+                if ((rc = tma_stage<T>(h, tile, k))) return rc;
+            }
+            continue;
         } else if (xm) {
             if ((rc = run_stage_xmarch<T>(h, tma, tile, MODE_S1, 0, -1, -1, 1, 2, dt / 6.0, 0.5 * dt))) return rc;
             if ((rc = run_stage_xmarch<T>(h, tma, tile, MODE_S23, 2, 0, 1, 1, 3, dt / 3.0, 0.5 * dt))) return rc;
@@ -409,6 +512,16 @@ int step_impl(nuosc_handle *h, int nsteps) {
         h->steps_done++;
     }
     return 0;
+}
+
+template <typename T>
+int stage_impl(nuosc_handle *h, int k) {
+    XTile tile;
+    if (stage_path<T>(h, tile) != 2)
+        return fail(NUOSC_ERR_UNSUPPORTED, "nuosc_stage runs the TMA stage kernel, which does not take this geometry");
+    const size_t need = (size_t)h->g.ncell * xmarch_num_vblocks(h->g, h->tile) * 2 * NMOM * sizeof(double);
+    if (int rc = ensure((void **)&h->d_part, &h->part_bytes, need, h)) return rc;
+    return tma_stage<T>(h, tile, k);
 }
 
 template <typename T>
@@ -764,6 +877,50 @@ int nuosc_create(const nuosc_params *p, nuosc_handle **out) {
     return NUOSC_OK;
 }
 
+int nuosc_create_slab(const nuosc_params *p, int rank, nuosc_handle **out) {
+    g_err.clear();
+    if (!p || !out) return fail(NUOSC_ERR_INVALID, "null argument");
+    *out = nullptr;
+    if (p->px < 1 || p->pz != 1 || rank < 0 || rank >= p->px)
+        return fail(NUOSC_ERR_INVALID, "slab %d of px=%d pz=%d (x-slabs: pz = 1, 0 <= rank < px)", rank, p->px, p->pz);
+    if (!(p->dx > 0) || !(p->x1 > p->x0)) return fail(NUOSC_ERR_INVALID, "bad box or spacing");
+    const int nxg = (int)((p->x1 - p->x0) / p->dx), R = p->gx;
+    const int base = nxg / p->px, rem = nxg % p->px;
+    const int nx = base + (rank < rem ? 1 : 0), xoff = rank * base + std::min(rank, rem);
+    if (nx < R || nx < 4) return fail(NUOSC_ERR_INVALID, "slab of %d planes (need at least 4 and the ghost width)", nx);
+    nuosc_params q = *p;
+    q.px = q.pz = 1;
+    q.x0 = p->x0 + xoff * p->dx;
+    q.x1 = q.x0 + (nx + 0.5) * p->dx;  // int((x1 - x0)/dx) = nx exactly
+    nuosc_handle *h = nullptr;
+    if (int rc = nuosc_create(&q, &h)) return rc;
+    h->x1 = p->x0 + (xoff + nx) * p->dx;
+    h->ds_L = p->dx * p->dz / (p->z1 - p->z0) / (p->x1 - p->x0);  // of the whole box (nuosc_class.cpp:461)
+    h->px = p->px;
+    h->rank = rank;
+    h->xoff = xoff;
+    h->nx_global = nxg;
+    h->halo_bytes = (size_t)NF * 2 * R * h->g.nz * h->g.nvs * h->esize;
+    const cudaError_t e = dev_alloc(&h->halo, h->halo_bytes, h->device, h->stream);
+    if (e != cudaSuccess) {
+        nuosc_destroy(h);
+        return fail(NUOSC_ERR_OOM, "slab halo buffer (%.2f MB): %s", h->halo_bytes / 1e6, cudaGetErrorString(e));
+    }
+    h->device_bytes += h->halo_bytes;
+    cudaMemsetAsync(h->halo, 0, h->halo_bytes, h->stream);
+    *out = h;
+    return NUOSC_OK;
+}
+
+int nuosc_get_slab(const nuosc_handle *h, int *px, int *rank, int *xoff, int *nx_global) {
+    if (!h) return fail(NUOSC_ERR_INVALID, "null handle");
+    if (px) *px = h->px;
+    if (rank) *rank = h->rank;
+    if (xoff) *xoff = h->xoff;
+    if (nx_global) *nx_global = h->halo ? h->nx_global : h->g.nx;
+    return NUOSC_OK;
+}
+
 int nuosc_destroy(nuosc_handle *h) {
     if (!h) return NUOSC_OK;
     if (h->batch) return fail(NUOSC_ERR_INVALID, "destroy: the handle is a member of a live batch");
@@ -778,6 +935,7 @@ int nuosc_destroy(nuosc_handle *h) {
         dev_free(h->d_stage, h->stream);
         dev_free(h->d_idx, h->stream);
         dev_free(h->d_gather, h->stream);
+        dev_free(h->halo, h->stream);
         cudaStreamDestroy(h->stream);
     }
     if (h->anafile.is_open()) h->anafile.close();
@@ -822,6 +980,54 @@ int nuosc_get_tile(const nuosc_handle *h, int *tz, int *lx) {
     if (!h) return fail(NUOSC_ERR_INVALID, "null handle");
     if (tz) *tz = h->tile.tz;
     if (lx) *lx = h->tile.lx;
+    return NUOSC_OK;
+}
+
+int nuosc_stage(nuosc_handle *h, int k) {
+    HANDLE_CHECK(h);
+    if (k < 0 || k > 3) return fail(NUOSC_ERR_INVALID, "stage %d (0..3)", k);
+    if (h->kernel != NUOSC_KERNEL_AUTO && h->kernel != NUOSC_KERNEL_XTMA)
+        return fail(NUOSC_ERR_UNSUPPORTED, "nuosc_stage runs the TMA stage kernel");
+    return h->precision == NUOSC_FP64 ? stage_impl<double>(h, k) : stage_impl<float>(h, k);
+}
+
+int nuosc_halo_info(const nuosc_handle *h, int k, nuosc_halo *o) {
+    if (!h || !o) return fail(NUOSC_ERR_INVALID, "null argument");
+    if (!h->halo) return fail(NUOSC_ERR_INVALID, "not a slab (nuosc_create_slab)");
+    if (k < 0 || k > 3) return fail(NUOSC_ERR_INVALID, "stage %d (0..3)", k);
+    halo_pieces(h, k, o);
+    return NUOSC_OK;
+}
+
+int nuosc_halo_exchange_local(nuosc_handle *const *s, int n, int k) {
+    if (!s || n < 1) return fail(NUOSC_ERR_INVALID, "null argument");
+    if (k < 0 || k > 3) return fail(NUOSC_ERR_INVALID, "stage %d (0..3)", k);
+    for (int i = 0; i < n; ++i) {
+        if (!s[i] || !s[i]->halo) return fail(NUOSC_ERR_INVALID, "member %d is not a slab", i);
+        if (s[i]->px != n || s[i]->rank != i || s[i]->device != s[0]->device || s[i]->g.nz != s[0]->g.nz ||
+            s[i]->g.nvs != s[0]->g.nvs || s[i]->esize != s[0]->esize || s[i]->ko6 != s[0]->ko6)
+            return fail(NUOSC_ERR_INVALID, "slabs must be ranks 0..%d of one solve on one device, in order", n - 1);
+    }
+    CUDA_TRY(cudaSetDevice(s[0]->device));
+    return halo_exchange_local(s, n, k);
+}
+
+int nuosc_analysis_sums(nuosc_handle *h, double *q) {
+    HANDLE_CHECK(h);
+    if (!q) return fail(NUOSC_ERR_INVALID, "null argument");
+    return analysis_dispatch(h, q);
+}
+
+int nuosc_diag_from_sums(const nuosc_handle *h, const double *q, nuosc_diag *o) {
+    if (!h || !q || !o) return fail(NUOSC_ERR_INVALID, "null argument");
+    diag_from_sums(h, q, h->phy_time, o);
+    return NUOSC_OK;
+}
+
+int nuosc_set_n_nue0(nuosc_handle *h, double n0, double n1) {
+    if (!h) return fail(NUOSC_ERR_INVALID, "null handle");
+    h->n_nue0[0] = n0;
+    h->n_nue0[1] = n1;
     return NUOSC_OK;
 }
 
@@ -934,9 +1140,9 @@ int nuosc_fill_init(nuosc_handle *h, int ipt, double alpha, double eps0, double 
     }
     cudaError_t e = h->precision == NUOSC_FP64
                         ? launch_init<double>((double *)h->reg[0], h->dG0(), h->dG0b(), h->g, ipt, eps0, sigma, h->z0,
-                                              h->dz, seed, dprof, h->stream)
+                                              h->dz, seed, dprof, h->xoff, h->stream)
                         : launch_init<float>((float *)h->reg[0], h->dG0(), h->dG0b(), h->g, ipt, eps0, sigma, h->z0,
-                                             h->dz, seed, dprof, h->stream);
+                                             h->dz, seed, dprof, h->xoff, h->stream);
     if (dprof) {
         cudaStreamSynchronize(h->stream);  // zprof is host memory of this frame
         dev_free(dprof, h->stream);
@@ -1547,6 +1753,7 @@ int nuosc_batch_create(nuosc_handle *const *members, int n, nuosc_batch **out) {
         const nuosc_handle *h = members[i];
         if (!h) return fail(NUOSC_ERR_INVALID, "batch member %d is null", i);
         if (h->batch) return fail(NUOSC_ERR_INVALID, "batch member %d already belongs to a batch", i);
+        if (h->halo) return fail(NUOSC_ERR_UNSUPPORTED, "batch member %d is an x-slab of a decomposed solve", i);
         for (int j = 0; j < i; ++j)
             if (members[j] == h) return fail(NUOSC_ERR_INVALID, "batch member %d repeats member %d", i, j);
         if (h->device != members[0]->device || h->precision != members[0]->precision || h->ko6 != members[0]->ko6)

@@ -91,7 +91,19 @@ struct StageArgs {
     // front box of the instance's first tile declares this many bytes more
     // than its copies deliver, so every wait on it runs out
     unsigned fault_tx;
+    // x-slab of a domain-decomposed solve (nullptr: the stencil wraps x
+    // periodically inside the register): the R planes on each side of the
+    // slab, [8 fields][2R planes][nz][nvs], planes 0..R-1 left of plane 0 and
+    // R..2R-1 right of plane nx-1, filled by the halo exchange before the stage
+    const T *halo;
 };
+
+// element offset of plane p in [-R, 0) or [nx, nx + R) of field F (0..7) in a
+// slab's halo buffer
+__host__ __device__ inline long long halo_offset(int F, int p, int nx, int R, long long P) {
+    const int hp = p < 0 ? p + R : p - nx + R;
+    return ((long long)F * 2 * R + hp) * P;
+}
 
 // ---------------------------------------------------------------- launches
 template <typename T>
@@ -188,7 +200,8 @@ cudaError_t launch_moment_finalize(const double *part, double *mom, Geom g, int 
 
 template <typename T>
 cudaError_t launch_init(T *reg, const double *G0, const double *G0b, Geom g, int ipt, double eps0,
-                        double sigma, double z0, double dz, uint64_t seed, const double *zprof, cudaStream_t s);
+                        double sigma, double z0, double dz, uint64_t seed, const double *zprof, int xoff,
+                        cudaStream_t s);
 // Analysis partial sums; `part` holds ANA_BLOCKS * ANA_NQ doubles, `out` ANA_NQ.
 constexpr int ANA_NQ = 12;
 constexpr int ANA_BLOCKS = 296;

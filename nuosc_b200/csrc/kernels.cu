@@ -163,7 +163,7 @@ cudaError_t launch_stage_direct(const StageArgs<T> &a, int mode, bool ko6, cudaS
 // Arithmetic is kept in the reference's order without FMA contraction.
 template <typename T>
 __global__ void k_init(T *reg, const double *G0, const double *G0b, Geom g, int ipt, double eps0, double sigma,
-                       double z0, double dz, uint64_t seed, const double *zprof) {
+                       double z0, double dz, uint64_t seed, const double *zprof, int xoff) {
     const int v = blockIdx.y * 32 + threadIdx.x;
     const long long cell = (long long)blockIdx.x * 8 + threadIdx.y;
     if (cell >= g.ncell || v >= g.nvs) return;
@@ -214,7 +214,7 @@ __global__ void k_init(T *reg, const double *G0, const double *G0b, Geom g, int 
     if (ipt == 0) {
         t = eps0 * exp(-Zj * Zj / (2.0 * sigma * sigma));
     } else if (ipt == 1) {
-        const double u = seeded_uniform(seed, i, j);
+        const double u = seeded_uniform(seed, xoff + i, j);  // global x index in a slab
         t = __dmul_rn(eps0, __dadd_rn(__dmul_rn(2.0, u), -1.0));
     } else if (ipt == 2) {
         t = eps0 * (1.0 + cos(2 * 3.14159265358979323846 * Zj / (2.0 * sigma * sigma))) * 0.5;
@@ -236,10 +236,10 @@ __global__ void k_init(T *reg, const double *G0, const double *G0b, Geom g, int 
 
 template <typename T>
 cudaError_t launch_init(T *reg, const double *G0, const double *G0b, Geom g, int ipt, double eps0, double sigma,
-                        double z0, double dz, uint64_t seed, const double *zprof, cudaStream_t s) {
+                        double z0, double dz, uint64_t seed, const double *zprof, int xoff, cudaStream_t s) {
     dim3 block(32, 8);
     dim3 grid((unsigned)((g.ncell + 7) / 8), (g.nvs + 31) / 32);
-    k_init<T><<<grid, block, 0, s>>>(reg, G0, G0b, g, ipt, eps0, sigma, z0, dz, seed, zprof);
+    k_init<T><<<grid, block, 0, s>>>(reg, G0, G0b, g, ipt, eps0, sigma, z0, dz, seed, zprof, xoff);
     return cudaGetLastError();
 }
 
@@ -464,7 +464,7 @@ cudaError_t launch_renormalize(T *reg, const double *G0, const double *G0b, Geom
     template cudaError_t launch_moments<T>(const T *, double *, Quad, Geom, cudaStream_t);                    \
     template cudaError_t launch_stage_direct<T>(const StageArgs<T> &, int, bool, cudaStream_t);              \
     template cudaError_t launch_init<T>(T *, const double *, const double *, Geom, int, double, double, double, \
-                                        double, uint64_t, const double *, cudaStream_t);                      \
+                                        double, uint64_t, const double *, int, cudaStream_t);                 \
     template cudaError_t launch_analysis<T>(const T *, const double *, const double *, const double *, Geom,   \
                                             double *, double *, cudaStream_t);                                \
     template cudaError_t launch_gather<T>(const T *, int, const int *, int, const int *, int, const double *,  \

@@ -34,19 +34,31 @@ __device__ __forceinline__ void tail_point(const StageArgs<T> &a, const long lon
     if (act) {
         const int i = (int)(cell / g.nz), j = (int)(cell - (long long)i * g.nz);
         constexpr int R = KO6 ? 3 : 2;
-        long long oz[7], ox[7];
+        const long long hoff = (long long)half * 4 * g.fs;
+        const long long P = (long long)g.nz * g.nvs;
+        // x neighbours: field-0 pointer of this half and field stride per
+        // offset -- inside the register (periodic), or a slab's halo buffer
+        long long oz[7];
+        const T *xp[7];
+        long long xfs[7];
 #pragma unroll
         for (int k = -3; k <= 3; ++k) {
             const int kk = (k < -R || k > R) ? 0 : k;
             oz[k + 3] = ((long long)i * g.nz + wrap_index(j + kk, g.nz)) * g.nvs + v;
-            ox[k + 3] = ((long long)wrap_index(i + kk, g.nx) * g.nz + j) * g.nvs + v;
+            const int pl = i + kk;
+            if (a.halo && (pl < 0 || pl >= g.nx)) {
+                xp[k + 3] = a.halo + halo_offset(4 * half, pl, g.nx, R, P) + (long long)j * g.nvs + v;
+                xfs[k + 3] = 2 * R * P;
+            } else {
+                xp[k + 3] = a.in + hoff + ((long long)wrap_index(pl, g.nx) * g.nz + j) * g.nvs + v;
+                xfs[k + 3] = g.fs;
+            }
         }
         const double vxd = a.q.vx[v], vyd = a.q.vy[v], vzd = a.q.vz[v], wd = a.q.vw[v];
         const T fx = T(vxd * a.c.fxs), fz = T(vzd * a.c.fzs);
         const T kx = T(a.c.kx), kz = T(a.c.kz);
         const double *m = a.mom_in + cell * NMOM;
         const T ia = T(inp(m, vxd, vyd, vzd)), ib = T(inp(m + 4, vxd, vyd, vzd)), ie = T(inp(m + 8, vxd, vyd, vzd));
-        const long long hoff = (long long)half * 4 * g.fs;
         T c4[4], a4[4], k4[4];
 #pragma unroll
         for (int f = 0; f < 4; ++f) {
@@ -55,7 +67,7 @@ __device__ __forceinline__ void tail_point(const StageArgs<T> &a, const long lon
 #pragma unroll
             for (int k = 0; k < 7; ++k) {
                 zs[k] = __ldg(F + oz[k]);
-                xs[k] = __ldg(F + ox[k]);
+                xs[k] = __ldg(xp[k] + f * xfs[k]);
             }
             c4[f] = zs[3];
             a4[f] = adv_axis(zs, fz) + adv_axis(xs, fx);

@@ -67,6 +67,8 @@ struct __align__(64) TmaMaps {
     CUtensorMap r;    // R rows (wrapped halo)
     CUtensorMap pu;   // TZ rows of the stage's U register (L2 prefetch of the pointwise input)
     CUtensorMap pa;   // TZ rows of the final stage's B input (acc_src; L2 prefetch)
+    // the same four box shapes over a slab's halo buffer (planes right of the slab)
+    CUtensorMap hzr, htzr, htz, hr;
 };
 
 __device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
@@ -331,7 +333,12 @@ __device__ __forceinline__ bool xtma_march(const TmaMaps *const &mp, const Stage
         const unsigned full = smem_u32(&bars[s]);
         unsigned char *sp = smem + s * S::bytes;
         mbar_expect_tx(full, S::tx + (j == R ? fault_tx : 0u));
-        const int x = (xs + j) % rd<SA>(a.g.nx);
+        // plane xs + j; past the last plane it wraps (periodic) or, in a slab,
+        // comes from the halo buffer's right planes (box plane x - nx + R).
+        // Boxes start at plane xs >= 0, so the left halo is never a box.
+        const int nx = rd<SA>(a.g.nx), xl = xs + j;
+        const bool hal = xl >= nx && rd<SA>(a.halo) != nullptr;
+        const int x = hal ? xl - nx + R : xl % nx;
         const int nz = rd<SA>(a.g.nz);
         const TmaMaps &maps = *rd<SA>(mp);
         const int c1 = 4 * half, c0 = vb * VB;
@@ -340,12 +347,18 @@ __device__ __forceinline__ bool xtma_march(const TmaMaps *const &mp, const Stage
             const int zw = zstart < 0 ? zstart + nz : (zstart >= nz ? zstart - nz : zstart);
             int len = nz - zw;
             if (len > ZR - dst) len = ZR - dst;
-            const CUtensorMap *m = len == ZR ? &maps.zr : len == TZ + R ? &maps.tzr : len == TZ ? &maps.tz : &maps.r;
+            const CUtensorMap *m = len == ZR        ? (hal ? &maps.hzr : &maps.zr)
+                                   : len == TZ + R ? (hal ? &maps.htzr : &maps.tzr)
+                                   : len == TZ     ? (hal ? &maps.htz : &maps.tz)
+                                                   : (hal ? &maps.hr : &maps.r);
             tma_load_4d(smem_u32(sp + S::box + dst * 4 * VB * sizeof(T)), m, c0, c1, zw, x, full);
             zstart += len;
             dst += len;
         }
-        bulk_load(smem_u32(sp + S::mb), rd<SA>(a.mom_in) + ((long long)x * nz + z0) * NMOM, 8u * TZ * NMOM, full);
+        // the cell moments are read at a box's centre use, which is always an
+        // interior plane; a halo box (front use only) loads plane nx-1's, unread
+        const int xm = hal ? nx - 1 : x;
+        bulk_load(smem_u32(sp + S::mb), rd<SA>(a.mom_in) + ((long long)xm * nz + z0) * NMOM, 8u * TZ * NMOM, full);
         issued = j + 1;
         return true;
     };
@@ -421,15 +434,20 @@ __device__ __forceinline__ bool xtma_march(const TmaMaps *const &mp, const Stage
     const bool vac = VAC && a.c.pmo != 0.0;  // batched launches: instances without a vacuum term skip it
     const bool sw1 = (perm >> 2) & 1, sw2 = (perm >> 3) & 1;
 
-    // prime the register queue with planes xs-R .. xs+R-1
+    // prime the register queue with planes xs-R .. xs+R-1 (periodic, or from
+    // a slab's halo buffer outside [0, nx))
     T q[4][W][NP];
+    const T *halo = rd<SA>(a.halo);
 #pragma unroll
     for (int k = 0; k < 2 * R; ++k) {
-        const long long o = (long long)wrap_index(xs - R + k, g.nx) * P + own;
+        const int pl = xs - R + k;
+        const bool hal = halo != nullptr && (pl < 0 || pl >= g.nx);
+        const long long o = (long long)wrap_index(pl, g.nx) * P + own;
 #pragma unroll
         for (int f = 0; f < 4; ++f) {
             T t[NP];
-            if (vact) ldv<T, NP>(in + f * fs + o, t);
+            const T *src = hal ? halo + halo_offset(4 * half + f, pl, g.nx, R, P) + own : in + f * fs + o;
+            if (vact) ldv<T, NP>(src, t);
 #pragma unroll
             for (int p = 0; p < NP; ++p) q[f][k][p] = vact ? t[p] : T(0);
         }
@@ -806,9 +824,16 @@ template <typename T>
 bool make_maps(TmaMaps *m, const StageArgs<T> &a, int tz, int r) {
     memset((void *)&m->pu, 0, sizeof m->pu);
     memset((void *)&m->pa, 0, sizeof m->pa);
+    memset((void *)&m->hzr, 0, 4 * sizeof m->hzr);
+    // a slab's halo buffer as a register of 2R planes
+    Geom h = a.g;
+    h.nx = 2 * r;
+    h.fs = (long long)h.nx * h.nz * h.nvs;
     return make_map<T>(&m->zr, a.in, a.g, tz + 2 * r) && make_map<T>(&m->tzr, a.in, a.g, tz + r) &&
            make_map<T>(&m->tz, a.in, a.g, tz) && make_map<T>(&m->r, a.in, a.g, r) &&
-           (!a.u || make_map<T>(&m->pu, a.u, a.g, tz)) && (!a.acc_src || make_map<T>(&m->pa, a.acc_src, a.g, tz));
+           (!a.u || make_map<T>(&m->pu, a.u, a.g, tz)) && (!a.acc_src || make_map<T>(&m->pa, a.acc_src, a.g, tz)) &&
+           (!a.halo || (make_map<T>(&m->hzr, a.halo, h, tz + 2 * r) && make_map<T>(&m->htzr, a.halo, h, tz + r) &&
+                        make_map<T>(&m->htz, a.halo, h, tz) && make_map<T>(&m->hr, a.halo, h, r)));
 }
 
 template <typename T, int R, int MODE, int TZ, bool VAC, bool M64>

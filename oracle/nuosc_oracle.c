@@ -179,6 +179,7 @@ typedef struct orc_sim {
     double *reg[4][NF]; /* 0 stat, 1 rhs, 2 pre, 3 cor */
     double *noc_phi;    /* explicit ipt = 4 phases (orc_set_noc_phases), or NULL: seeded */
     int noc_nphi;
+    int xoff;           /* x-slab: global index of plane 0 (seeded ipt = 1 draws) */
 } orc_sim;
 
 static inline long gidx(const orc_sim *s, int i, int j, int v) {
@@ -275,7 +276,7 @@ void orc_fill_init(orc_sim *s, int ipt, double alpha, double eps0, double sigma,
             double Zj = s->z0 + (j + 0.5) * s->dz; /* CartGrid.cpp:200 */
             double tmpr;
             if (ipt == 0) tmpr = eps0 * exp(-(Zj) * (Zj) / (2.0 * sigma * sigma));
-            else if (ipt == 1) tmpr = eps0 * (2.0 * orc_uniform(seed, i, j) - 1.0);
+            else if (ipt == 1) tmpr = eps0 * (2.0 * orc_uniform(seed, s->xoff + i, j) - 1.0);
             else if (ipt == 2) tmpr = eps0 * (1.0 + cos(2 * M_PI * (Zj) / (2.0 * sigma * sigma))) * 0.5;
             else tmpr = eps0;
             double p3o = sqrt(1.0 - tmpr * tmpr);
@@ -443,7 +444,7 @@ void orc_get_state(const orc_sim *s, int reg, int f, double *compact) {
 void orc_set_time(orc_sim *s, double t) { s->phy_time = t; }
 
 /* Periodic ghost fill, z first then x; corners untouched (nuosc_boundary.cpp:4-52). */
-static void periodic_boundary(orc_sim *s, double **F) {
+static void boundary_z(orc_sim *s, double **F) {
 #pragma omp parallel for collapse(2)
     for (int i = 0; i < s->nx; ++i)
         for (int j = 0; j < s->gz; ++j)
@@ -452,6 +453,10 @@ static void periodic_boundary(orc_sim *s, double **F) {
                 long r0 = gidx(s, i, s->nz + j, v), r1 = gidx(s, i, j, v);
                 for (int f = 0; f < NF; ++f) { F[f][l0] = F[f][l1]; F[f][r0] = F[f][r1]; }
             }
+}
+
+static void periodic_boundary(orc_sim *s, double **F) {
+    boundary_z(s, F);
 #pragma omp parallel for collapse(2)
     for (int i = 0; i < s->gx; ++i)
         for (int j = 0; j < s->nz; ++j)
@@ -568,34 +573,63 @@ static void swapreg(orc_sim *s, int a, int b) {
     for (int f = 0; f < NF; ++f) { double *t = s->reg[a][f]; s->reg[a][f] = s->reg[b][f]; s->reg[b][f] = t; }
 }
 
-/* Classic RK4 exactly as step_rk4 (nuosc_class.cpp:374-427). */
-void orc_step_rk4(orc_sim *s, int nsteps) {
+/*
+ * x ghosts of a slab of an x-decomposed solve (the reference's CartGrid
+ * halo exchange, nuosc_boundary.cpp:64-208, for a split in x): the callback
+ * fills the x-ghost planes of register `reg` (its z ghosts are already
+ * filled, z first as in nuosc_boundary.cpp:4-52) before the calRHS of stage
+ * `stage`.  NULL: periodic in x inside the register.
+ */
+typedef void (*orc_halo_cb)(int stage, int reg, void *user);
+
+static void ghost_fill(orc_sim *s, int reg, int stage, orc_halo_cb cb, void *user) {
+    if (!cb) {
+        periodic_boundary(s, s->reg[reg]);
+        return;
+    }
+    boundary_z(s, s->reg[reg]);
+    cb(stage, reg, user);
+}
+
+static void step_rk4_impl(orc_sim *s, int nsteps, orc_halo_cb cb, void *user) {
     enum { STAT = 0, RHS = 1, PRE = 2, COR = 3 };
     const double dt = s->dt;
     for (int n = 0; n < nsteps; ++n) {
-        periodic_boundary(s, s->reg[STAT]);
+        ghost_fill(s, STAT, 0, cb, user);
         calrhs(s, s->reg[RHS], s->reg[STAT]);
         vec1(s, s->reg[PRE], s->reg[STAT], 0.5 * dt, s->reg[RHS]);
 
-        periodic_boundary(s, s->reg[PRE]);
+        ghost_fill(s, PRE, 1, cb, user);
         calrhs(s, s->reg[COR], s->reg[PRE]);
         vec1(s, s->reg[RHS], s->reg[RHS], 2.0, s->reg[COR]);
         vec1(s, s->reg[COR], s->reg[STAT], 0.5 * dt, s->reg[COR]);
         swapreg(s, PRE, COR);
 
-        periodic_boundary(s, s->reg[PRE]);
+        ghost_fill(s, PRE, 2, cb, user);
         calrhs(s, s->reg[COR], s->reg[PRE]);
         vec1(s, s->reg[RHS], s->reg[RHS], 2.0, s->reg[COR]);
         vec1(s, s->reg[COR], s->reg[STAT], dt, s->reg[COR]);
         swapreg(s, PRE, COR);
 
-        periodic_boundary(s, s->reg[PRE]);
+        ghost_fill(s, PRE, 3, cb, user);
         calrhs(s, s->reg[COR], s->reg[PRE]);
         vec2(s, s->reg[PRE], s->reg[STAT], 1.0 / 6.0 * dt, s->reg[COR], s->reg[RHS]);
         swapreg(s, PRE, STAT);
         s->phy_time += dt;
     }
 }
+
+/* Classic RK4 exactly as step_rk4 (nuosc_class.cpp:374-427). */
+void orc_step_rk4(orc_sim *s, int nsteps) { step_rk4_impl(s, nsteps, NULL, NULL); }
+
+/* The same for one x-slab: x ghosts from the halo-exchange callback. */
+void orc_step_rk4_slab(orc_sim *s, int nsteps, orc_halo_cb cb, void *user) { step_rk4_impl(s, nsteps, cb, user); }
+
+/* Ghosted array of field f of register reg ((nx+2gx)(nz+2gz)nv doubles, CartGrid::idx order). */
+double *orc_field(orc_sim *s, int reg, int f) { return s->reg[reg][f]; }
+
+/* Global x index of local plane 0 (an x-slab): the seeded draws use it. */
+void orc_set_xoff(orc_sim *s, int xoff) { s->xoff = xoff; }
 
 /*
  * Diagnostics of analysis() (nuosc_ana.cpp:3-137), summed in (x,z,v) order.

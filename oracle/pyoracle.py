@@ -28,6 +28,9 @@ _I = C.c_int
 _P = C.c_void_p
 _DP = C.POINTER(C.c_double)
 
+# callback of orc_step_rk4_slab: (stage, register) -> fill the x-ghost planes
+HALO_CB = C.CFUNCTYPE(None, _I, _I, _P)
+
 DIAG_NAMES = ["phy_time", "maxdP", "surv", "survb", "avgP", "avgPb", "aM0", "Lex", "ELNe"]
 
 
@@ -74,6 +77,10 @@ def _oracle_lib():
         lib.orc_uniform.restype = _D
         lib.orc_uniform.argtypes = [C.c_uint64, _I, _I]
         lib.orc_set_noc_phases.argtypes = [_P, _I, _DP]
+        lib.orc_step_rk4_slab.argtypes = [_P, _I, HALO_CB, _P]
+        lib.orc_field.restype = _DP
+        lib.orc_field.argtypes = [_P, _I, _I]
+        lib.orc_set_xoff.argtypes = [_P, _I]
         lib.orc_adv_integrals.argtypes = [_P, _DP]
         lib.orc_adv_integrals.restype = None
         _olib = lib
@@ -157,6 +164,24 @@ class Oracle(_Sim):
 
     def set_time(self, t):
         self.lib.orc_set_time(self.h, t)
+
+    def set_xoff(self, xoff):
+        """This oracle is an x-slab whose plane 0 is global plane xoff (seeded draws)."""
+        self.lib.orc_set_xoff(self.h, int(xoff))
+
+    def field(self, reg, f):
+        """Ghosted array of one field of a register, a numpy view ((nx+2g)(nz+2g)nv,
+        CartGrid::idx order)."""
+        i = self.info()
+        g = i["ghost"]
+        n = (i["nx"] + 2 * g) * (i["nz"] + 2 * g) * i["nv"]
+        return np.ctypeslib.as_array(self.lib.orc_field(self.h, reg, f), shape=(n,))
+
+    def step_slab(self, n, fill_x_ghosts):
+        """n RK4 steps of an x-slab: before each calRHS the z ghosts are filled
+        periodically and fill_x_ghosts(stage, reg) must fill the x ghosts."""
+        cb = HALO_CB(lambda stage, reg, user: fill_x_ghosts(stage, reg))
+        self.lib.orc_step_rk4_slab(self.h, n, cb, None)
 
     def set_noc_phases(self, phi):
         """Explicit phases of the ipt = 4 initial data (None: the seeded ones)."""
