@@ -533,12 +533,13 @@ def bench_serving(args, local, single):
                         "one_at_a_time_fp64_modelled": {k: one[k] for k in ("cell_steps_per_s", "latency_p50_s",
                                                                             "latency_p99_s", "makespan_s")}},
             "failed": {"saturated": rs["failed"], "poisson": rp["failed"],
-                       "poisson_failed_cell_steps_run": rp["failed_cell_steps_run"]},
+                       "saturated_failed_cell_steps_run": rs["failed_cell_steps_run"],
+                       "saturated_failed_cell_steps_counted": rs["failed_cell_steps_counted"]},
             "note": "single-large-solve reference = the 1024x1024x642 FP64/FP32 solves timed above, weighted by "
                     "the requests' FP64/FP32 cell-steps; one-at-a-time latencies from measured per-shape FP64 step "
                     "times (modelled: FIFO over measured per-shape step times, no host costs); a request whose "
-                    "streamed analysis reports a blown-up state is retired as failed and counted in 'failed', not "
-                    "in cell_steps_per_s or the latencies; "
+                    "streamed analysis reports a blown-up state is retired as failed ('failed'): its cell-steps up "
+                    "to its last good record count, the ones after it do not, and it has no latency; "
                     "the 512-request run is in profiles/serving_512_requests.md"}
 
 

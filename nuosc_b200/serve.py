@@ -24,8 +24,9 @@ parameters, a step count and a precision) arrive over time; the server
   * retires a solve as failed when a streamed record reports a blown-up state
     (a non-finite value or max||P|-1| >= 10, the reference's assert in
     nuosc_ana.cpp:131): it leaves its batch at the end of the quantum in
-    which the record arrives, and neither its steps nor its latency count
-    as served work;
+    which the record arrives; its steps up to its last good record count as
+    served work (the reference computes them too before it stops), the steps
+    after it do not, and it has no completion latency;
   * reports per-request time-to-completion (p50/p99) and the aggregate
     cell-steps/s (nx*nz*nv per RK4 step).
 
@@ -90,6 +91,7 @@ class Record:
     rejected: bool = False
     failed: bool = False  # retired before its last step because its state blew up
     steps_run: int = 0
+    last_good: int = 0  # step of the last streamed record with a finite state
 
     @property
     def latency(self):
@@ -213,6 +215,8 @@ class Server:
             rec = recs[rid]
             if d is None and rec.diverged_at < 0:
                 rec.diverged_at = step
+            if d is not None and rec.diverged_at < 0:
+                rec.last_good = step
             rec.diags.append((step, d))
             if self.on_diag:
                 self.on_diag(rid, step, d)
@@ -350,21 +354,26 @@ class Server:
 
     @staticmethod
     def _report(reqs, recs, makespan, busy, stats):
-        """Served = completed every requested step with a finite state; failed
-        solves (retired on a blown-up record) count neither their cell-steps nor
-        their latency, and their steps run are reported apart."""
+        """Served = completed every requested step with a finite state.  A failed
+        solve (retired on a blown-up record) adds the cell-steps up to its last
+        good record to the work done, not the ones after it, and no latency."""
         served = [recs[r.rid] for r in reqs if not recs[r.rid].rejected and not recs[r.rid].failed]
         failed = [recs[r.rid] for r in reqs if recs[r.rid].failed]
         lat = np.array([r.latency for r in served]) if served else np.zeros(1)
-        cs = float(sum(r.req.cell_steps for r in served))
+        cells = lambda r: r.req.nx * r.req.nz * r.req.nv  # noqa: E731
+        good = {r.req.rid: float(cells(r) * r.last_good) for r in failed}
+        cs = float(sum(r.req.cell_steps for r in served)) + sum(good.values())
         first = min(r.arrival for r in reqs) if reqs else 0.0
         return {
             "requests": len(reqs), "served": len(served), "rejected": sum(r.rejected for r in recs.values()),
             "failed": len(failed),
-            "failed_cell_steps_run": float(sum(r.req.nx * r.req.nz * r.req.nv * r.steps_run for r in failed)),
+            "failed_cell_steps_run": float(sum(cells(r) * r.steps_run for r in failed)),
+            "failed_cell_steps_counted": float(sum(good.values())),
             "fp32": sum(r.req.precision == 1 for r in served), "fp64": sum(r.req.precision == 0 for r in served),
-            "cell_steps_fp64": float(sum(r.req.cell_steps for r in served if r.req.precision == 0)),
-            "cell_steps_fp32": float(sum(r.req.cell_steps for r in served if r.req.precision == 1)),
+            "cell_steps_fp64": float(sum(r.req.cell_steps for r in served if r.req.precision == 0) +
+                                     sum(good[r.req.rid] for r in failed if r.req.precision == 0)),
+            "cell_steps_fp32": float(sum(r.req.cell_steps for r in served if r.req.precision == 1) +
+                                     sum(good[r.req.rid] for r in failed if r.req.precision == 1)),
             "cell_steps": cs, "makespan_s": makespan, "busy_s": busy,
             "cell_steps_per_s": cs / max(1e-9, makespan - first), "cell_steps_per_busy_s": cs / max(1e-9, busy),
             "latency_p50_s": float(np.percentile(lat, 50)), "latency_p99_s": float(np.percentile(lat, 99)),
