@@ -421,9 +421,9 @@ def bench_ours(args, world, rank, local):
 
 
 def bench_fp32(args, local, v64):
-    """The FP32 form of the same workload (state, stencil and the in-block
-    velocity sums in float; the cell moments and diagnostics in FP64): its
-    cell-steps/s and the ratio to FP64."""
+    """The FP32 form of the same workload (state and stencil in float; the
+    velocity-moment sums as the tile table says -- FP64 -- and the
+    diagnostics in FP64): its cell-steps/s and the ratio to FP64."""
     import torch
     import nuosc_b200 as nb
     w = workload(args.size, args.nn, nb.FP32)
@@ -445,7 +445,8 @@ def bench_fp32(args, local, v64):
     s.close()
     v = cells / (ms / 1e3)
     return {"value": v, "unit": METRIC, "ms_per_step": ms, "vs_fp64": v / v64, "steps": args.steps,
-            "note": "same workload, FP32 state; accuracy vs FP64 in profiles/fp32_vs_fp64_256x642.md"}
+            "note": "same workload, FP32 state, FP64 moment sums and diagnostics; accuracy vs FP64 in "
+                    "profiles/fp32_vs_fp64_1024x642.md"}
 
 
 def mixed_instances(n, seed, precision):
