@@ -455,6 +455,31 @@ def bench_fp32(args, local, v64):
                     "profiles/fp32_vs_fp64_1024x642.md"}
 
 
+def time_large(args, local, precision, gx, steps=3):
+    """cell-steps/s of the full-size workload at a given precision and ghost
+    width (KO order), W warm-up steps then `steps` timed ones."""
+    import torch
+    import nuosc_b200 as nb
+    w = workload(args.size, args.nn, precision)
+    s = nb.NuOsc(1, 1, w["nn"], 0, gx, gx, w["x0"], w["x1"], w["x0"], w["x1"], w["dx"], w["dx"], w["cfl"], w["ko"],
+                 precision=precision, device=local)
+    s.set_mu(w["mu"])
+    s.set_pmo(0.0)
+    s.fillInitValue(1, w["alpha"], w["eps0"], 1.0, w["lnue"], w["lnueb"], seed=w["seed"])
+    cells = s.grid.nx * s.grid.nz * s.grid.nv
+    st = torch.cuda.ExternalStream(nb.lib().nuosc_stream(s.handle))
+    s.step_rk4(args.warmup)
+    s.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    s.step_rk4(steps)
+    e1.record(st)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    s.close()
+    return cells / (ms / 1e3)
+
+
 def mixed_instances(n, seed, precision):
     """n solves of the mixed-instance recipe: nx, nz from {32, 64, 128, 256},
     nv from {42, 162, 642}, mu, alpha, spectra widths and eps amplitude drawn
@@ -504,24 +529,29 @@ def bench_batch(args, local, single):
 
 
 def bench_serving(args, local, single):
-    """Two bounded serving runs of mixed requests (70% FP32) under a 150 GB
+    """Bounded serving runs of mixed requests (70% FP32) under a 150 GB
     budget with continuous batching: all requests at once (throughput: its
     ratio to the single large solves doing the same cell-steps) and Poisson
     arrivals (p50/p99 completion latency, beside the same arrivals served one
-    at a time on the plain FP64 path)."""
+    at a time on the plain FP64 path), with the recipe's 6th-difference KO;
+    and all at once again with the 4th-difference KO, under which no request
+    blows up (the serving machinery's own throughput)."""
     from nuosc_b200 import serve
 
-    def ref_rate(rep):  # the large solves' rate for the served FP64/FP32 cell-steps mix
+    def ref_rate(rep, large=single):  # the large solves' rate for the served FP64/FP32 cell-steps mix
         cs64, cs32 = rep["cell_steps_fp64"], rep["cell_steps_fp32"]
-        return (cs64 + cs32) / (cs64 / single["f64"] + cs32 / single["f32"])
+        return (cs64 + cs32) / (cs64 / large["f64"] + cs32 / large["f32"])
 
     steps = (args.serve_min_steps, args.serve_max_steps)
     sat = serve.draw_requests(args.serve_requests, 0.0, 7, steps=steps)
     rs = serve.Server(budget_bytes=150e9, device=local).run(sat)
     reqs = serve.draw_requests(args.serve_requests, args.serve_rate, 7, steps=steps)
     rp = serve.Server(budget_bytes=150e9, device=local).run(reqs)
+    sat4 = serve.draw_requests(args.serve_requests, 0.0, 7, steps=steps, ko_order=4)
+    rs4 = serve.Server(budget_bytes=150e9, device=local).run(sat4)
+    large4 = {"f64": time_large(args, local, 0, 2), "f32": time_large(args, local, 1, 2)}
     t = serve.solo_fp64_step_times(reqs, device=local)
-    one = serve.fifo_one_at_a_time(reqs, {r.rid: t[(r.nx, r.nz, r.nn)] * r.steps for r in reqs})
+    one = serve.fifo_one_at_a_time(reqs, {r.rid: t[(r.nx, r.nz, r.nn, r.ko_order)] * r.steps for r in reqs})
 
     def loop_stats(r):  # device-busy time, quanta, batch rebuilds, host time per server phase
         return {"busy_s": r["busy_s"], "quanta": r["quanta"], "batch_builds": r["batch_builds"],
@@ -533,6 +563,11 @@ def bench_serving(args, local, single):
                           "makespan_s": rs["makespan_s"], "peak_resident": rs["peak_resident"],
                           "latency_p50_s": rs["latency_p50_s"], "latency_p99_s": rs["latency_p99_s"],
                           **loop_stats(rs)},
+            "saturated_ko4": {"cell_steps_per_s": rs4["cell_steps_per_s"],
+                              "vs_single_large_solve": rs4["cell_steps_per_s"] / ref_rate(rs4, large4),
+                              "single_large_solve_ko4": large4,
+                              "served": rs4["served"], "failed": rs4["failed"], "makespan_s": rs4["makespan_s"],
+                              "latency_p50_s": rs4["latency_p50_s"], "latency_p99_s": rs4["latency_p99_s"]},
             "poisson": {"rate_per_s": args.serve_rate, "cell_steps_per_s": rp["cell_steps_per_s"],
                         "cell_steps_per_busy_s": rp["cell_steps_per_busy_s"],
                         "latency_p50_s": rp["latency_p50_s"], "latency_p99_s": rp["latency_p99_s"],

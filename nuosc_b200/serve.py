@@ -71,6 +71,7 @@ class Request:
     precision: int  # 0 FP64, 1 FP32
     seed: int
     pmo: float = 0.0
+    ko_order: int = 6  # 6: the recipe's 6th-difference KO (3 ghosts); 4: 4th difference (2 ghosts)
 
     @property
     def nv(self):
@@ -98,8 +99,12 @@ class Record:
         return self.completed - self.req.arrival
 
 
-def draw_requests(n, rate, seed, steps=(100, 5000), fp32_frac=0.7, sizes=(32, 64, 128, 256), nns=(2, 4, 8)):
-    """n requests with Poisson arrivals at `rate` per second (rate <= 0: all at t=0)."""
+def draw_requests(n, rate, seed, steps=(100, 5000), fp32_frac=0.7, sizes=(32, 64, 128, 256), nns=(2, 4, 8),
+                  ko_order=6):
+    """n requests with Poisson arrivals at `rate` per second (rate <= 0: all at t=0).
+    ko_order 4 gives every request the 4th-difference KO instead of the
+    recipe's 6th-difference one, whose anti-dissipative grid-scale term makes
+    most long solves blow up (as in the reference)."""
     rng = np.random.default_rng(seed)
     t = 0.0
     out = []
@@ -112,7 +117,8 @@ def draw_requests(n, rate, seed, steps=(100, 5000), fp32_frac=0.7, sizes=(32, 64
             mu=float(rng.uniform(0.5, 2.0)), alpha=float(rng.uniform(0.7, 1.3)),
             lnue=float(rng.uniform(0.4, 0.8)), lnueb=float(rng.uniform(0.3, 0.7)),
             eps0=float(10 ** rng.uniform(-7, -3)), steps=int(round(math.exp(rng.uniform(lo, hi)))),
-            precision=1 if rng.uniform() < fp32_frac else 0, seed=int(rng.integers(1, 2 ** 62))))
+            precision=1 if rng.uniform() < fp32_frac else 0, seed=int(rng.integers(1, 2 ** 62)),
+            ko_order=ko_order))
     return out
 
 
@@ -141,7 +147,8 @@ def make_solver(req, device=0):
     eps = eps0 U(-1,1) per cell from the seed)."""
     import nuosc_b200 as nb
     Lx, Lz = req.nx * DX / 2, req.nz * DX / 2
-    s = nb.NuOsc(1, 1, req.nn, 0, 3, 3, -Lx, Lx, -Lz, Lz, DX, DX, CFL, KO, precision=req.precision, device=device)
+    g = 3 if req.ko_order == 6 else 2
+    s = nb.NuOsc(1, 1, req.nn, 0, g, g, -Lx, Lx, -Lz, Lz, DX, DX, CFL, KO, precision=req.precision, device=device)
     g = s.grid
     if (g.nx, g.nz) != (req.nx, req.nz):
         s.close()
@@ -398,13 +405,14 @@ def fifo_one_at_a_time(requests, service_s):
 
 def solo_fp64_step_times(requests, steps=10, warmup=2, device=0):
     """Measured FP64 step time (s) of the plain single-solve path for every
-    distinct (nx, nz, nn) among the requests (CUDA events on the solver's stream)."""
+    distinct (nx, nz, nn, ko_order) among the requests (CUDA events on the
+    solver's stream)."""
     import torch
     import nuosc_b200 as nb
     out = {}
-    for key in sorted({(r.nx, r.nz, r.nn) for r in requests}):
+    for key in sorted({(r.nx, r.nz, r.nn, r.ko_order) for r in requests}):
         r = Request(rid=-1, arrival=0, nx=key[0], nz=key[1], nn=key[2], mu=1.0, alpha=0.9, lnue=0.6, lnueb=0.5,
-                    eps0=1e-6, steps=steps, precision=0, seed=1)
+                    eps0=1e-6, steps=steps, precision=0, seed=1, ko_order=key[3])
         s = make_solver(r, device)
         st = torch.cuda.ExternalStream(nb.lib().nuosc_stream(s.handle))
         s.step_rk4(warmup)
@@ -429,16 +437,18 @@ def main():
     ap.add_argument("--min-steps", type=int, default=100)
     ap.add_argument("--max-steps", type=int, default=5000)
     ap.add_argument("--no-baseline", action="store_true", help="skip the one-at-a-time FP64 comparison")
+    ap.add_argument("--ko-order", type=int, default=6, choices=(6, 4))
     args = ap.parse_args()
-    reqs = draw_requests(args.requests, args.rate, args.seed, steps=(args.min_steps, args.max_steps))
+    reqs = draw_requests(args.requests, args.rate, args.seed, steps=(args.min_steps, args.max_steps),
+                         ko_order=args.ko_order)
     rep = Server(budget_bytes=args.budget_gb * 1e9,
                  max_resident_bytes=args.max_resident_gb * 1e9 if args.max_resident_gb > 0 else float("inf")).run(reqs)
-    rep.update({"rate_per_s": args.rate, "seed": args.seed, "budget_gb": args.budget_gb,
+    rep.update({"rate_per_s": args.rate, "seed": args.seed, "budget_gb": args.budget_gb, "ko_order": args.ko_order,
                 "max_resident_gb": args.max_resident_gb,
                 "steps_range": [args.min_steps, args.max_steps]})
     if not args.no_baseline:
         t = solo_fp64_step_times(reqs)
-        service = {r.rid: t[(r.nx, r.nz, r.nn)] * r.steps for r in reqs}
+        service = {r.rid: t[(r.nx, r.nz, r.nn, r.ko_order)] * r.steps for r in reqs}
         rep["one_at_a_time_fp64"] = {**fifo_one_at_a_time(reqs, service),
                                      "note": "same arrivals served in order on the plain FP64 path; service "
                                              "times from measured per-shape FP64 step times"}
