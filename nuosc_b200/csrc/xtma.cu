@@ -214,12 +214,20 @@ __device__ __forceinline__ void rhs_half(const T (&c)[4], T a, T b, T e, T mu, T
     }
 }
 
-// one reduce-scatter step over lane pairs (lane, lane^O): N values -> N/2;
-// the lane-permuted slot order makes the kept half always the lower one
-template <int N, int O, typename M>
-__device__ __forceinline__ void rs_step(M (&m)[16]) {
-#pragma unroll
-    for (int i = 0; i < N / 2; ++i) m[i] += __shfl_xor_sync(0xffffffffu, m[i + N / 2], O);
+// the weights 2jj and 2jj + 1 of this lane's NP velocities (one 16-byte load)
+template <typename T, int NP>
+__device__ __forceinline__ void ldw(const T *p, T (&a)[NP], T (&b)[NP]) {
+    if constexpr (NP == 2) {
+        const float4 t = *reinterpret_cast<const float4 *>(p);
+        a[0] = t.x;
+        a[1] = t.y;
+        b[0] = t.z;
+        b[1] = t.w;
+    } else {
+        const double2 t = *reinterpret_cast<const double2 *>(p);
+        a[0] = t.x;
+        b[0] = t.y;
+    }
 }
 
 // statically allocated per-CTA scratch of the march: the abort flag, the
@@ -236,7 +244,10 @@ struct MarchShared {
     // 16 lanes on one bank); a lane's NP stencil weights are one vector load
     double vq[kShared ? 3 : 1][kShared ? VB : 2];          // vx, vy, vz
     std::conditional_t<M64, double, float> wp[kShared ? vpt<T>() * 4 : 1][kShared ? 32 : 2];  // lane-permuted
-    T sw[8][32 * NP];                                       // stencil weights: z axis j = 0..3, x axis 4..7
+    // stencil weights, z axis j = 0..3 then x axis j = 4..7, in pairs: sw[jj][lane]
+    // holds weights 2jj (NP velocities) and 2jj + 1 (NP velocities), 16 bytes,
+    // so a lane reads all eight with four conflict-free 16-byte loads
+    __align__(16) T sw[4][32][2 * NP];
     int abort;
 };
 
@@ -372,13 +383,13 @@ __device__ __forceinline__ bool xtma_march(const TmaMaps *const &mp, const Stage
         }
     };
 
-    // per-velocity and uniform constants.  Lane-permuted moment weights: slot i
-    // of this lane holds moment (i ^ perm), moment k = (combo k>>2, weight
-    // k&3); perm = bits 1..4 of the lane.  With two velocities per thread
-    // (FP32) the per-velocity constants (FP64 velocities, float weights) live
-    // in shared memory and are read per plane, which keeps the register queue
-    // clear of spills.
-    const int perm = (lane >> 1) & 15;
+    // per-velocity and uniform constants.  Lane-permuted moment weights: slot s
+    // of this lane holds weight s ^ wq (weights w, w vx, w vy, w vz), wq = lane
+    // bits 4..3, the order the moment reduce-scatter needs.  With two
+    // velocities per thread (FP32) the per-velocity constants (FP64
+    // velocities, float weights) live in shared memory and are read per plane,
+    // which keeps the register queue clear of spills.
+    const int wq = (lane >> 3) & 3;
     constexpr bool kShared = MarchShared<T, M64>::kShared;
     auto &s_vq = sh.vq;
     auto &s_wp = sh.wp;
@@ -394,15 +405,15 @@ __device__ __forceinline__ bool xtma_march(const TmaMaps *const &mp, const Stage
             stencil_weights<R>(a.c.kx, vxd[p] * a.c.fxs, wx);
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
-                sh.sw[j][NP * lane + p] = T(wz[j]);
-                sh.sw[4 + j][NP * lane + p] = T(wx[j]);
+                sh.sw[j >> 1][lane][(j & 1) * NP + p] = T(wz[j]);
+                sh.sw[2 + (j >> 1)][lane][(j & 1) * NP + p] = T(wx[j]);
             }
         }
         const double wd = vact ? a.q.vw[vc + p] : 0.0;
         const double v4w[4] = {wd, vxd[p] * wd, vyd[p] * wd, vzd[p] * wd};
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-            const int k = j ^ (perm & 3);
+            const int k = j ^ wq;
             wperm[p][j] = k == 0 ? v4w[0] : k == 1 ? v4w[1] : k == 2 ? v4w[2] : v4w[3];
         }
     }
@@ -432,7 +443,6 @@ __device__ __forceinline__ bool xtma_march(const TmaMaps *const &mp, const Stage
     };
     const T p2s = T(2 * a.c.pmo * a.c.st), p2c = T(2 * a.c.pmo * a.c.ct), ps = T(a.c.pmo * a.c.st);
     const bool vac = VAC && a.c.pmo != 0.0;  // batched launches: instances without a vacuum term skip it
-    const bool sw1 = (perm >> 2) & 1, sw2 = (perm >> 3) & 1;
 
     // prime the register queue with planes xs-R .. xs+R-1 (periodic, or from
     // a slab's halo buffer outside [0, nx))
@@ -484,9 +494,12 @@ __device__ __forceinline__ bool xtma_march(const TmaMaps *const &mp, const Stage
                 }
             }
         }
+        // the front box (plane i + R) has to be waited for; the centre box was
+        // this warp's front box R planes ago (its slot is not refilled before
+        // its centre use), except for the first R centres, which are never fronts
         const int jf = i + R, sf = jf % NS, sc = i % NS;
         if (!mbar_wait(smem_u32(&bars[sf]), (unsigned)((jf / NS) & 1)) ||
-            !mbar_wait(smem_u32(&bars[sc]), (unsigned)((i / NS) & 1)) || *(volatile int *)&s_abort) {
+            (i < R && !mbar_wait(smem_u32(&bars[sc]), (unsigned)((i / NS) & 1))) || *(volatile int *)&s_abort) {
             s_abort = 1;
             break;
         }
@@ -504,11 +517,10 @@ __device__ __forceinline__ bool xtma_march(const TmaMaps *const &mp, const Stage
         T sten[4][NP];
         const T kzp = K(a.c.kz, kz), kxp = K(a.c.kx, kx);
         T swz[4][NP], swx[4][NP];  // this lane's stencil weights (shared memory, re-read per plane)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            ldv<T, NP>(&sh.sw[j][NP * lane], swz[j]);
-            ldv<T, NP>(&sh.sw[4 + j][NP * lane], swx[j]);
-        }
+        ldw<T, NP>(&sh.sw[0][lane][0], swz[0], swz[1]);
+        ldw<T, NP>(&sh.sw[1][lane][0], swz[2], swz[3]);
+        ldw<T, NP>(&sh.sw[2][lane][0], swx[0], swx[1]);
+        ldw<T, NP>(&sh.sw[3][lane][0], swx[2], swx[3]);
 #pragma unroll
         for (int f = 0; f < 4; ++f) {
             T zs[W][NP];
@@ -585,7 +597,11 @@ __device__ __forceinline__ bool xtma_march(const TmaMaps *const &mp, const Stage
                 for (int f = 0; f < 4; ++f) stv<T, NP>(bp + f * fs, ain[f]);
             }
         }
-        // velocity-moment partials of the written state (nuosc_class.cpp:69-71).
+        // velocity-moment partials of the written state (nuosc_class.cpp:69-71):
+        // moment 4c + j = sum over the block's velocities of weight j (w, w vx,
+        // w vy, w vz) times combination c (emr, emi, ee - mm; the neutrino half
+        // enters with sign -1 in combinations 0 and 2, applied to the final
+        // sum, which is exact).
         // M64 (every FP64 march; the FP32 march when the tile table says so):
         // products and the warp's reduce-scatter in double -- the float state
         // converts exactly and each product with a double weight is a double
@@ -594,37 +610,48 @@ __device__ __forceinline__ bool xtma_march(const TmaMaps *const &mp, const Stage
         // float-rounded weights, summed over the block's 64 velocities --, the
         // block's partial stored as double; the blocks and both halves are
         // summed in FP64 by the finalize either way.
+        // Each lane forms its 12 products (weight slots in its order s ^ wq) and
+        // the warp reduce-scatters them, pairing lanes over bits 4, 3, 2, 1, 0:
+        // over bit 4 weight slots 2 and 3 go to the partner, over bit 3 slot 1,
+        // which leaves every lane the three combinations of weight wq; over bit
+        // 2 the lanes with the bit clear keep combinations 0 and 1, the others
+        // combination 2; over bit 1 the former split 0 and 1 while the latter
+        // sum 2; over bit 0 both sum.  13 shuffle-adds for the 12 sums.
         {
             using M = std::conditional_t<M64, double, float>;
-            M mp[16];
-#pragma unroll
-            for (int k = 0; k < 16; ++k) mp[k] = M(0);
+            M acc[3][4];
 #pragma unroll
             for (int p = 0; p < NP; ++p) {
-                // combinations: neutrinos enter with sign -1, antineutrinos +1
                 const M ee = M(outm[0][p]), mm = M(outm[1][p]), emr = M(outm[2][p]), emi = M(outm[3][p]);
-                M d0 = half ? emr : -emr, d1 = emi, d2 = half ? ee - mm : mm - ee;
-                if (!vact) d0 = d1 = d2 = M(0);
-                // combos in slot order: dp[c] = d[c ^ (perm >> 2)], d[3] = 0
-                const M t0 = sw1 ? d1 : d0, t1 = sw1 ? d0 : d1, t2 = sw1 ? M(0) : d2, t3 = sw1 ? d2 : M(0);
-                const M dp[4] = {sw2 ? t2 : t0, sw2 ? t3 : t1, sw2 ? t0 : t2, sw2 ? t1 : t3};
+                const M d[3] = {emr, emi, ee - mm};
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
                     M wj;
                     if constexpr (kShared) wj = s_wp[4 * p + j][lane];
                     else wj = wperm[p][j];
 #pragma unroll
-                    for (int c = 0; c < 4; ++c) mp[4 * c + j] = fma(wj, dp[c], mp[4 * c + j]);
+                    for (int c = 0; c < 3; ++c) acc[c][j] = p == 0 ? wj * d[c] : fma(wj, d[c], acc[c][j]);
                 }
             }
-            rs_step<16, 16>(mp);
-            rs_step<8, 8>(mp);
-            rs_step<4, 4>(mp);
-            rs_step<2, 2>(mp);
-            mp[0] += __shfl_xor_sync(0xffffffffu, mp[0], 1);
-            if ((lane & 1) == 0 && perm < NMOM) {  // lanes 2k, 2k+1 hold moment perm
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                acc[c][0] += __shfl_xor_sync(0xffffffffu, acc[c][2], 16);
+                acc[c][1] += __shfl_xor_sync(0xffffffffu, acc[c][3], 16);
+            }
+#pragma unroll
+            for (int c = 0; c < 3; ++c) acc[c][0] += __shfl_xor_sync(0xffffffffu, acc[c][1], 8);
+            const bool b2 = (lane >> 2) & 1, b1 = (lane >> 1) & 1;
+            M k0 = b2 ? acc[2][0] : acc[0][0];
+            k0 += __shfl_xor_sync(0xffffffffu, b2 ? acc[0][0] : acc[2][0], 4);
+            const M k1 = acc[1][0] + __shfl_xor_sync(0xffffffffu, acc[1][0], 4);
+            M kk = (!b2 && b1) ? k1 : k0;
+            kk += __shfl_xor_sync(0xffffffffu, (b2 || b1) ? k0 : k1, 2);
+            kk += __shfl_xor_sync(0xffffffffu, kk, 1);
+            if ((lane & 1) == 0 && !(b2 && b1)) {  // lanes 0 mod 2 hold moment 4c + wq
+                const int c = b2 ? 2 : (int)b1;
+                const double v = (double)kk;
                 const long long cell = (long long)x * rd<SA>(a.g.nz) + zr;
-                rd<SA>(a.mom_part)[((cell * nvb + vb) * 2 + half) * NMOM + perm] = (double)mp[0];
+                rd<SA>(a.mom_part)[((cell * nvb + vb) * 2 + half) * NMOM + 4 * c + wq] = (half || c == 1) ? v : -v;
             }
         }
 #pragma unroll
