@@ -239,11 +239,11 @@ struct MarchShared {
     static constexpr bool kShared = vpt<T>() == 2;
     static constexpr int VB = vblock<T>();
     static constexpr int NP = vpt<T>();
-    // [component][p * 32 + lane], [4 p + j][lane] and [j][NP lane + p]:
-    // consecutive lanes read consecutive words (a lane-major layout would put
-    // 16 lanes on one bank); a lane's NP stencil weights are one vector load
-    double vq[kShared ? 3 : 1][kShared ? VB : 2];          // vx, vy, vz
-    std::conditional_t<M64, double, float> wp[kShared ? vpt<T>() * 4 : 1][kShared ? 32 : 2];  // lane-permuted
+    // [component][lane] and [j][lane], the lane's two velocities side by side
+    // (one 16-byte load, 8-byte for float weights); consecutive lanes read
+    // consecutive vectors (a lane-major layout would put 16 lanes on one bank)
+    double2 vq[kShared ? 3 : 1][kShared ? 32 : 1];                              // vx, vy, vz
+    std::conditional_t<M64, double2, float2> wp[kShared ? 4 : 1][kShared ? 32 : 1];  // lane-permuted
     // stencil weights, z axis j = 0..3 then x axis j = 4..7, in pairs: sw[jj][lane]
     // holds weights 2jj (NP velocities) and 2jj + 1 (NP velocities), 16 bytes,
     // so a lane reads all eight with four conflict-free 16-byte loads
@@ -419,13 +419,13 @@ __device__ __forceinline__ bool xtma_march(const TmaMaps *const &mp, const Stage
     }
     if constexpr (kShared) {
         if (r == 0) {
+            s_vq[0][lane] = make_double2(vxd[0], vxd[NP - 1]);
+            s_vq[1][lane] = make_double2(vyd[0], vyd[NP - 1]);
+            s_vq[2][lane] = make_double2(vzd[0], vzd[NP - 1]);
 #pragma unroll
-            for (int p = 0; p < NP; ++p) {
-                s_vq[0][p * 32 + lane] = vxd[p];
-                s_vq[1][p * 32 + lane] = vyd[p];
-                s_vq[2][p * 32 + lane] = vzd[p];
-#pragma unroll
-                for (int j = 0; j < 4; ++j) s_wp[4 * p + j][lane] = (std::conditional_t<M64, double, float>)wperm[p][j];
+            for (int j = 0; j < 4; ++j) {
+                if constexpr (M64) s_wp[j][lane] = make_double2(wperm[0][j], wperm[NP - 1][j]);
+                else s_wp[j][lane] = make_float2((float)wperm[0][j], (float)wperm[NP - 1][j]);
             }
         }
     }
@@ -499,7 +499,8 @@ __device__ __forceinline__ bool xtma_march(const TmaMaps *const &mp, const Stage
         // its centre use), except for the first R centres, which are never fronts
         const int jf = i + R, sf = jf % NS, sc = i % NS;
         if (!mbar_wait(smem_u32(&bars[sf]), (unsigned)((jf / NS) & 1)) ||
-            (i < R && !mbar_wait(smem_u32(&bars[sc]), (unsigned)((i / NS) & 1))) || *(volatile int *)&s_abort) {
+            (i < R && !mbar_wait(smem_u32(&bars[sc]), (unsigned)((i / NS) & 1))) ||
+            ((i & 3) == 0 && *(volatile int *)&s_abort)) {  // another warp's abort, looked at every 4th plane
             s_abort = 1;
             break;
         }
@@ -558,11 +559,16 @@ __device__ __forceinline__ bool xtma_march(const TmaMaps *const &mp, const Stage
         if (lane == 0) mbar_arrive(smem_u32(&bars[NS + sc]));  // centre use is the box's last use
 
         T outm[4][NP];
+        double2 vq2[3];
+        if constexpr (kShared) {
+#pragma unroll
+            for (int c = 0; c < 3; ++c) vq2[c] = s_vq[c][lane];
+        }
 #pragma unroll
         for (int p = 0; p < NP; ++p) {
-            const double ux = kShared ? s_vq[0][p * 32 + lane] : vxd[p];
-            const double uy = kShared ? s_vq[1][p * 32 + lane] : vyd[p];
-            const double uz = kShared ? s_vq[2][p * 32 + lane] : vzd[p];
+            const double ux = kShared ? (p ? vq2[0].y : vq2[0].x) : vxd[p];
+            const double uy = kShared ? (p ? vq2[1].y : vq2[1].x) : vyd[p];
+            const double uz = kShared ? (p ? vq2[2].y : vq2[2].x) : vzd[p];
             const T ia = T(inp(m, ux, uy, uz)), ib = T(inp(m + 4, ux, uy, uz)), ie = T(inp(m + 8, ux, uy, uz));
             const T cen[4] = {q[0][R][p], q[1][R][p], q[2][R][p], q[3][R][p]};
             const T st4[4] = {sten[0][p], sten[1][p], sten[2][p], sten[3][p]};
@@ -620,6 +626,11 @@ __device__ __forceinline__ bool xtma_march(const TmaMaps *const &mp, const Stage
         {
             using M = std::conditional_t<M64, double, float>;
             M acc[3][4];
+            std::conditional_t<M64, double2, float2> wp2[4];
+            if constexpr (kShared) {
+#pragma unroll
+                for (int j = 0; j < 4; ++j) wp2[j] = s_wp[j][lane];
+            }
 #pragma unroll
             for (int p = 0; p < NP; ++p) {
                 const M ee = M(outm[0][p]), mm = M(outm[1][p]), emr = M(outm[2][p]), emi = M(outm[3][p]);
@@ -627,7 +638,7 @@ __device__ __forceinline__ bool xtma_march(const TmaMaps *const &mp, const Stage
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
                     M wj;
-                    if constexpr (kShared) wj = s_wp[4 * p + j][lane];
+                    if constexpr (kShared) wj = p ? wp2[j].y : wp2[j].x;
                     else wj = wperm[p][j];
 #pragma unroll
                     for (int c = 0; c < 3; ++c) acc[c][j] = p == 0 ? wj * d[c] : fma(wj, d[c], acc[c][j]);
