@@ -307,9 +307,10 @@ int nuosc_get_profile(nuosc_handle *h, double *ms, long long *launches, int nkin
 
 /* ---- right-hand side without device allocation -------------------------
  * No counterpart in the reference.  For callers that may not call cudaMalloc:
- * code issuing work while its stream is being captured into a CUDA graph
- * (allocation is refused during capture), and host frameworks that keep all
- * device memory in their own allocator and hand a plugin only their buffers.
+ * host frameworks that reserve the device's memory for their own allocator
+ * (a pool sized at start-up, a serving runtime with a fixed budget) and hand
+ * a plugin only buffers they allocated; an allocation made behind their back
+ * fails when the pool holds the memory, or breaks their accounting.
  * The caller passes everything in its own device memory: `in` and `out` are
  * states laid out like the library's registers, [8 fields][nx][nz][nv_stride]
  * of double (NUOSC_FP64) or float (NUOSC_FP32), padding velocities zero, and

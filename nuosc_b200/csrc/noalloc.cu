@@ -1,9 +1,10 @@
 // noalloc.cu -- calRHS for callers that cannot allocate device memory.
 //
-// Some callers of this library may not call cudaMalloc: code that runs while
-// its stream is being captured into a CUDA graph (allocation calls are
-// refused during capture), and host frameworks that reserve all device
-// memory for their own allocator and hand plugins only their own buffers.
+// Some callers of this library may not call cudaMalloc: host frameworks that
+// reserve the device's memory for their own allocator at start-up (a memory
+// pool, a serving runtime with a fixed budget) and hand a plugin only buffers
+// they allocated -- an allocation behind their back either fails, because the
+// pool holds the memory, or breaks their accounting.
 // nuosc_calrhs_noalloc serves them: the caller passes the input and output
 // state (and the velocity quadrature) in its own device memory, and the one
 // piece of scratch the right-hand side needs -- the 12 velocity moments per
@@ -90,7 +91,8 @@ extern "C" int nuosc_calrhs_noalloc(const nuosc_rhs_desc *d, const void *in, voi
     if (!d->vx || !d->vy || !d->vz || !d->vw) return fail(NUOSC_ERR_INVALID, "calrhs_noalloc: null quadrature");
 
     // device address of the scratch array in the current context: looked up
-    // on the first call in that context (with its device current) and cached
+    // on the first call in that context (with its device current) and cached;
+    // that first call should come before any stream capture begins
     unsigned long long ctx = 0;
     if (!current_context_id(&ctx)) return fail(NUOSC_ERR_CUDA, "calrhs_noalloc: no current CUDA context");
     double *scratch = nullptr;

@@ -1,8 +1,9 @@
 """nuosc_calrhs_noalloc -- the right-hand side for callers that cannot allocate.
 
-Code that issues work while its stream is captured into a CUDA graph, or that
-runs inside a host framework owning all device memory, cannot let this library
-call cudaMalloc.  nuosc_calrhs_noalloc takes every buffer from the caller and
+A host framework that reserves the device's memory for its own allocator and
+hands plugins only buffers it allocated cannot let this library call
+cudaMalloc: the allocation fails when the pool holds the memory, or breaks the
+framework's accounting.  nuosc_calrhs_noalloc takes every buffer from the caller and
 keeps its only scratch (the per-cell velocity moments) in a fixed device
 array.  Here the test plays such a caller: it owns the device buffers (made
 through torch), calls the entry point through the C ABI twice in a row with
