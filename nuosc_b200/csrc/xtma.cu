@@ -237,7 +237,6 @@ __device__ __forceinline__ void ldw(const T *p, T (&a)[NP], T (&b)[NP]) {
 template <typename T, bool M64>
 struct MarchShared {
     static constexpr bool kShared = vpt<T>() == 2;
-    static constexpr int VB = vblock<T>();
     static constexpr int NP = vpt<T>();
     // [component][lane] and [j][lane], the lane's two velocities side by side
     // (one 16-byte load, 8-byte for float weights); consecutive lanes read
@@ -626,7 +625,7 @@ __device__ __forceinline__ bool xtma_march(const TmaMaps *const &mp, const Stage
         {
             using M = std::conditional_t<M64, double, float>;
             M acc[3][4];
-            std::conditional_t<M64, double2, float2> wp2[4];
+            [[maybe_unused]] std::conditional_t<M64, double2, float2> wp2[kShared ? 4 : 1];
             if constexpr (kShared) {
 #pragma unroll
                 for (int j = 0; j < 4; ++j) wp2[j] = s_wp[j][lane];
