@@ -320,6 +320,11 @@ __device__ __forceinline__ bool xtma_march(const TmaMaps *const &mp, const Stage
     const T *in = a.in + hoff;
     const int vc = vact ? v : 0;
     const long long own = (long long)zr * g.nvs + vc;
+    // per-plane addressing in 32 bits: within one flavour half, a field's
+    // offset f fs (f <= 3), a plane's x P and a cell's moment-partial index
+    // all fit (xtma_supported requires 3 fs < 2^32); only the half's own
+    // offset, hoff, needs 64 bits
+    const unsigned fs32 = (unsigned)fs, P32 = (unsigned)P, own32 = (unsigned)own;
 
     __syncthreads();  // the previous tile of this CTA (batched kernel) is done with the ring
     if (tid == 0) {
@@ -475,21 +480,21 @@ __device__ __forceinline__ bool xtma_march(const TmaMaps *const &mp, const Stage
             l2pref(i + CF::PFD);
         }
         const int x = xs + i;
-        const long long oc = hoff + (long long)x * P + own;
+        const unsigned ox = (unsigned)x * P32 + own32;  // element offset of (x, zr, v) within a field
         T uin[4][NP], ain[4][NP];  // U, B
         {
             // pointwise epilogue inputs first (they are not in the ring; L2 hits
             // after the tensor prefetch PFD planes earlier)
             constexpr bool LU = CF::PU, LA = CF::PA;
-            const T *up = LU ? rd<SA>(a.u) + oc : nullptr;
-            const T *ap = LA ? rd<SA>(a.acc_src) + oc : nullptr;
+            const T *up = LU ? rd<SA>(a.u) + hoff + ox : nullptr;
+            const T *ap = LA ? rd<SA>(a.acc_src) + hoff + ox : nullptr;
 #pragma unroll
             for (int f = 0; f < 4; ++f) {
 #pragma unroll
                 for (int p = 0; p < NP; ++p) uin[f][p] = ain[f][p] = T(0);
                 if (vact) {
-                    if (LU) ldv<T, NP>(up + f * fs, uin[f]);
-                    if (LA) ldv<T, NP>(ap + f * fs, ain[f]);
+                    if (LU) ldv<T, NP>(up + f * fs32, uin[f]);
+                    if (LA) ldv<T, NP>(ap + f * fs32, ain[f]);
                 }
             }
         }
@@ -593,13 +598,13 @@ __device__ __forceinline__ bool xtma_march(const TmaMaps *const &mp, const Stage
             }
         }
         if (vact) {
-            T *dp = (MODE == MODE_S4B ? rd<SA>(a.acc_dst) : rd<SA>(a.y_dst)) + oc;
+            T *dp = (MODE == MODE_S4B ? rd<SA>(a.acc_dst) : rd<SA>(a.y_dst)) + hoff + ox;
 #pragma unroll
-            for (int f = 0; f < 4; ++f) stv<T, NP>(dp + f * fs, outm[f]);
+            for (int f = 0; f < 4; ++f) stv<T, NP>(dp + f * fs32, outm[f]);
             if (MODE == MODE_S2B) {
-                T *bp = rd<SA>(a.acc_dst) + oc;
+                T *bp = rd<SA>(a.acc_dst) + hoff + ox;
 #pragma unroll
-                for (int f = 0; f < 4; ++f) stv<T, NP>(bp + f * fs, ain[f]);
+                for (int f = 0; f < 4; ++f) stv<T, NP>(bp + f * fs32, ain[f]);
             }
         }
         // velocity-moment partials of the written state (nuosc_class.cpp:69-71):
@@ -660,8 +665,9 @@ __device__ __forceinline__ bool xtma_march(const TmaMaps *const &mp, const Stage
             if ((lane & 1) == 0 && !(b2 && b1)) {  // lanes 0 mod 2 hold moment 4c + wq
                 const int c = b2 ? 2 : (int)b1;
                 const double v = (double)kk;
-                const long long cell = (long long)x * rd<SA>(a.g.nz) + zr;
-                rd<SA>(a.mom_part)[((cell * nvb + vb) * 2 + half) * NMOM + 4 * c + wq] = (half || c == 1) ? v : -v;
+                const unsigned cell = (unsigned)x * (unsigned)rd<SA>(a.g.nz) + (unsigned)zr;
+                rd<SA>(a.mom_part)[((cell * (unsigned)nvb + (unsigned)vb) * 2u + (unsigned)half) * NMOM + 4 * c + wq] =
+                    (half || c == 1) ? v : -v;
             }
         }
 #pragma unroll
@@ -978,9 +984,12 @@ struct BatchLaunch {
 
 template <typename T>
 bool xtma_supported(const Geom &g, XTile t) {
-    // nz >= tz + 6: the widest box (tz + 2R rows, R <= 3) fits in the z extent
+    // nz >= tz + 6: the widest box (tz + 2R rows, R <= 3) fits in the z extent;
+    // 3 fs < 2^32: the march's per-plane offsets within a flavour half are
+    // 32-bit (registers of up to 91 GB in FP64, 45 GB in FP32: every state
+    // whose four registers fit a B200)
     return (t.tz == 8 || t.tz == 16) && g.nz % t.tz == 0 && g.nz >= t.tz + 6 && g.nx >= 4 &&
-           g.nvs % vpt<T>() == 0 && encode_fn() != nullptr;
+           g.nvs % vpt<T>() == 0 && 3 * g.fs < (1ll << 32) && encode_fn() != nullptr;
 }
 
 template <typename T>
