@@ -393,6 +393,21 @@ typedef struct nuosc_batch_record {
 int nuosc_batch_step_stream(nuosc_batch *b, int nsteps, int every, nuosc_batch_record *out, int max_out,
                             int *n_out);
 int nuosc_batch_record_diag(const nuosc_batch *b, const nuosc_batch_record *r, nuosc_diag *d);
+/* Device-side stop of failed members.  The reference stops a run at the
+ * analysis whose max||P|-1| reaches 10 (the assert in nuosc_ana.cpp:131);
+ * this is that test inside a batch, without a host round trip.  With
+ * check_every > 0, every check_every steps of a member -- and at every record
+ * nuosc_batch_step_stream streams -- the member's analysis is evaluated on the
+ * device, and a member with a non-finite value or max||P|-1| >= 10 stops: the
+ * batch's later stage, tail and finalize work skips it, so its state stays as
+ * it was at that step (its step counter keeps counting the batch's steps).
+ * The other members' results do not change (bit for bit).  check_every 0 (the
+ * default) turns the checks off; a member that stopped stays stopped.
+ * nuosc_batch_halted synchronises the batch and writes steps[k] = the step at
+ * which member k (the order given to nuosc_batch_create; n entries) stopped,
+ * 0 while it runs. */
+int nuosc_batch_set_halt(nuosc_batch *b, int check_every);
+int nuosc_batch_halted(nuosc_batch *b, int *steps, int n);
 /* page-locked host memory for record buffers (NULL on failure) */
 void *nuosc_host_alloc(size_t bytes);
 void nuosc_host_free(void *p);

@@ -455,6 +455,19 @@ class Batch:
     def synchronize(self):
         check(lib().nuosc_batch_synchronize(self._b))
 
+    def set_halt(self, check_every):
+        """Stop a member on the device once its analysis (every `check_every`
+        of its steps, and at every streamed record) shows a non-finite value
+        or max||P|-1| >= 10, the reference's stop test; 0 turns it off."""
+        check(lib().nuosc_batch_set_halt(self._b, int(check_every)))
+
+    def halted(self):
+        """Per member (creation order): the step at which it stopped, 0 while it runs (synchronises)."""
+        n = len(self.members)
+        out = (C.c_int * n)()
+        check(lib().nuosc_batch_halted(self._b, out, n))
+        return [int(v) for v in out]
+
     def stream(self):
         return lib().nuosc_batch_stream(self._b)
 

@@ -128,6 +128,8 @@ _SIGS = {
     "nuosc_batch_destroy": [_P],
     "nuosc_batch_step_stream": [_P, _I, _I, _P, _I, _IP],
     "nuosc_batch_record_diag": [_P, C.POINTER(BatchRecord), C.POINTER(Diag)],
+    "nuosc_batch_set_halt": [_P, _I],
+    "nuosc_batch_halted": [_P, _IP, _I],
     "nuosc_release_cached_memory": [_I],
     "nuosc_selftest_wait_timeout": [_I, C.c_uint, C.POINTER(C.c_double)],
     "nuosc_selftest_overdeclare_tx": [_P, C.c_uint],

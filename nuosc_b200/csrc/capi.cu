@@ -1493,6 +1493,11 @@ struct nuosc_batch {
     cudaGraphExec_t exec = nullptr;
     std::vector<double> sig;        // member settings the tables were built from
     long long graph_launches = 0, kernel_launches = 0, per_step = 0;
+    // device-side stop of failed members: d_halt[i] = step at which member i
+    // (service order) met the stop criterion, 0 while it runs; checked every
+    // halt_every of its steps and at every streamed record (0: no checks)
+    int *d_halt = nullptr;
+    int halt_every = 0;
 };
 
 namespace {
@@ -1612,7 +1617,7 @@ int batch_build(nuosc_batch *b) {
             a.fault_tx = h->fault_tx;
             ti = xtma_batch_fill<T>(&host[((size_t)k * n + i) * b->item_bytes], a, b->ko6, b->tz, lxs[i]);
             if (v0 < h->g.nvs)
-                tails[k].push_back(TailItem<T>{a, v0, tail_lanes(h->g.nvs - v0), xtma_num_vblocks<T>(h->g), 0});
+                tails[k].push_back(TailItem<T>{a, v0, tail_lanes(h->g.nvs - v0), xtma_num_vblocks<T>(h->g), i});
             if (ti < 0) return fail(NUOSC_ERR_UNSUPPORTED, "batch member %d (%dx%d) cannot run %d-row TMA tiles", i,
                                     h->g.nx, h->g.nz, b->tz);
         }
@@ -1666,16 +1671,16 @@ int batch_build(nuosc_batch *b) {
     cudaError_t e = cudaMemsetAsync(b->d_counter, 0, 4 * sizeof(unsigned long long), b->stream);
     for (int k = 0; k < 4 && e == cudaSuccess; ++k) {
         e = launch_stage_xtma_batch<T>(b->d_buf + (size_t)k * n * b->item_bytes, b->d_starts, n, tiles,
-                                       b->d_counter + k, kStages[k].mode, b->ko6, b->tz, b->vac, b->m64, b->grid[k],
-                                       b->stream);
+                                       b->d_counter + k, b->d_halt, kStages[k].mode, b->ko6, b->tz, b->vac, b->m64,
+                                       b->grid[k], b->stream);
         if (e == cudaSuccess && b->ntail) {
             const size_t tb = 4 * (size_t)b->ntail * sizeof(TailItem<T>);
             e = launch_stage_tail_batch<T>((const TailItem<T> *)(b->d_tail + (size_t)k * b->ntail * sizeof(TailItem<T>)),
                                            (const long long *)(b->d_tail + tb), b->ntail, b->tail_threads,
-                                           kStages[k].mode, b->ko6, b->stream);
+                                           b->d_halt, kStages[k].mode, b->ko6, b->stream);
             per_step++;
         }
-        if (e == cudaSuccess) e = launch_moment_finalize_batch(b->d_fin, b->d_fstarts, n, nmom, b->stream);
+        if (e == cudaSuccess) e = launch_moment_finalize_batch(b->d_fin, b->d_fstarts, n, nmom, b->d_halt, b->stream);
         per_step += 2;
     }
     for (nuosc_handle *h : b->m) {
@@ -1721,18 +1726,26 @@ int batch_step_impl(nuosc_batch *b, int nsteps, int every, nuosc_batch_record *o
             nuosc_handle *h = b->m[i];
             h->phy_time += h->dt;  // as step_impl: dt added once per step
             h->steps_done++;
-            if (every <= 0 || h->steps_done % every) continue;
+            const bool rec = every > 0 && h->steps_done % every == 0;
+            const bool chk = b->halt_every > 0 && (rec || h->steps_done % b->halt_every == 0);
+            if (!rec && !chk) continue;
+            if (rec && nrec >= max_out)
+                return fail(NUOSC_ERR_INVALID, "batch_step_stream: more than %d records", max_out);
+            double *fin = h->d_ana + ANA_BLOCKS * ANA_NQ;
+            CUDA_TRY(launch_analysis<T>((const T *)h->reg[0], h->dG0(), h->dG0b(), h->quad().vw, h->g, h->d_ana, fin,
+                                        b->stream));
+            b->kernel_launches += 2;
+            if (chk) {  // the stop test on the device; a failed member's later work is skipped
+                CUDA_TRY(launch_halt_check(fin, b->d_halt + i, (int)h->steps_done, b->stream));
+                b->kernel_launches++;
+            }
+            if (!rec) continue;
             // streamed analysis record: the sums land in out[nrec] when the batch stream gets there
-            if (nrec >= max_out) return fail(NUOSC_ERR_INVALID, "batch_step_stream: more than %d records", max_out);
             nuosc_batch_record &r = out[nrec++];
             r.member = b->user_index[i];
             r.step = h->steps_done;
             r.phy_time = h->phy_time;
-            double *fin = h->d_ana + ANA_BLOCKS * ANA_NQ;
-            CUDA_TRY(launch_analysis<T>((const T *)h->reg[0], h->dG0(), h->dG0b(), h->quad().vw, h->g, h->d_ana, fin,
-                                        b->stream));
             CUDA_TRY(cudaMemcpyAsync(r.q, fin, ANA_NQ * sizeof(double), cudaMemcpyDeviceToHost, b->stream));
-            b->kernel_launches += 2;
             if (n_out) *n_out = nrec;
         }
     }
@@ -1808,6 +1821,9 @@ int nuosc_batch_create(nuosc_handle *const *members, int n, nuosc_batch **out) {
         e = cudaStreamSynchronize(h->stream);
         if (e != cudaSuccess) return bail(fail(NUOSC_ERR_CUDA, "batch_create: %s", cudaGetErrorString(e)));
     }
+    e = dev_alloc((void **)&b->d_halt, n * sizeof(int), b->device, b->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(b->d_halt, 0, n * sizeof(int), b->stream);
+    if (e != cudaSuccess) return bail(fail(NUOSC_ERR_CUDA, "batch_create: %s", cudaGetErrorString(e)));
     const int rc = b->precision == NUOSC_FP64 ? batch_build<double>(b) : batch_build<float>(b);
     if (rc) return bail(rc);
     for (nuosc_handle *h : b->m) h->batch = b;
@@ -1831,6 +1847,24 @@ int nuosc_batch_step_stream(nuosc_batch *b, int nsteps, int every, nuosc_batch_r
 }
 
 int nuosc_batch_step(nuosc_batch *b, int nsteps) { return nuosc_batch_step_stream(b, nsteps, 0, nullptr, 0, nullptr); }
+
+int nuosc_batch_set_halt(nuosc_batch *b, int check_every) {
+    if (!b) return fail(NUOSC_ERR_INVALID, "null batch");
+    if (check_every < 0) return fail(NUOSC_ERR_INVALID, "batch_set_halt: check_every %d", check_every);
+    b->halt_every = check_every;
+    return NUOSC_OK;
+}
+
+int nuosc_batch_halted(nuosc_batch *b, int *steps, int n) {
+    if (!b || !steps) return fail(NUOSC_ERR_INVALID, "null argument");
+    if (n != (int)b->m.size()) return fail(NUOSC_ERR_INVALID, "batch_halted: %d entries for %d members", n, (int)b->m.size());
+    CUDA_TRY(cudaSetDevice(b->device));
+    std::vector<int> h(n);
+    CUDA_TRY(cudaMemcpyAsync(h.data(), b->d_halt, n * sizeof(int), cudaMemcpyDeviceToHost, b->stream));
+    CUDA_TRY(cudaStreamSynchronize(b->stream));
+    for (int i = 0; i < n; ++i) steps[b->user_index[i]] = h[i];
+    return NUOSC_OK;
+}
 
 int nuosc_batch_record_diag(const nuosc_batch *b, const nuosc_batch_record *r, nuosc_diag *d) {
     if (!b || !r || !d) return fail(NUOSC_ERR_INVALID, "null argument");
@@ -1932,6 +1966,7 @@ int nuosc_batch_destroy(nuosc_batch *b) {
     if (b->stream) {
         dev_free(b->d_buf, b->stream);
         dev_free(b->d_tail, b->stream);
+        dev_free(b->d_halt, b->stream);
     }
     if (b->ev) cudaEventDestroy(b->ev);
     if (b->stream) cudaStreamDestroy(b->stream);

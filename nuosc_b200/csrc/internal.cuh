@@ -151,11 +151,12 @@ template <typename T>
 int xtma_batch_grid(int mode, bool ko6, int tz, bool vac, bool m64, int device);
 // starts[i] = tiles of instances 0..i-1 (instances ordered as the caller
 // wants them served); grid = xtma_batch_grid(...); *counter must be 0 at the
-// launch (the work-list cursor)
+// launch (the work-list cursor); halt[i] != 0 (halt may be null): instance i
+// has stopped, its tiles are skipped
 template <typename T>
 cudaError_t launch_stage_xtma_batch(const void *items, const long long *starts, int n, long long ntiles,
-                                    unsigned long long *counter, int mode, bool ko6, int tz, bool vac, bool m64,
-                                    int grid, cudaStream_t s);
+                                    unsigned long long *counter, const int *halt, int mode, bool ko6, int tz,
+                                    bool vac, bool m64, int grid, cudaStream_t s);
 // Tail of the TMA x-march stage (tail.cu): when the last velocity block of
 // the TMA kernel would hold at most a quarter block of real velocities, the
 // velocities from xtma_tail_v0 on are computed by a one-thread-per-(cell,
@@ -169,14 +170,15 @@ cudaError_t launch_stage_tail(const StageArgs<T> &a, int mode, bool ko6, int v0,
 template <typename T>
 struct TailItem {
     StageArgs<T> a;
-    int v0, twp, nvb, pad;
+    int v0, twp, nvb;
+    int member;  // the instance's index in the batch (its halt flag)
 };
 // starts[i]: first thread of item i (ranges of 2 * ncell * twp threads, one
 // per (cell, flavour half, tail lane), each rounded up to a multiple of 32);
-// total: threads of all items
+// total: threads of all items; halt as for launch_stage_xtma_batch
 template <typename T>
 cudaError_t launch_stage_tail_batch(const TailItem<T> *items, const long long *starts, int n, long long total,
-                                    int mode, bool ko6, cudaStream_t s);
+                                    const int *halt, int mode, bool ko6, cudaStream_t s);
 // moment_finalize of many instances in one launch (xmarch.cu); starts[i] =
 // sum over instances 0..i-1 of ncell * 12
 struct FinalizeItem {
@@ -186,7 +188,11 @@ struct FinalizeItem {
     int nvb;
 };
 cudaError_t launch_moment_finalize_batch(const FinalizeItem *items, const long long *starts, int n, long long total,
-                                         cudaStream_t s);
+                                         const int *halt, cudaStream_t s);
+// *halt = step when *halt is 0 and the analysis sums `sums` (launch_analysis's
+// out) meet the reference's stop criterion: a non-finite value or
+// max||P|-1| >= 10 (nuosc_ana.cpp:131) (kernels.cu)
+cudaError_t launch_halt_check(const double *sums, int *halt, int step, cudaStream_t s);
 // value a kernel writes into StageArgs::status when a bounded wait expires
 constexpr int NUOSC_TIMEOUT_CODE = 1;
 // one warp waits `spins` polls on an mbarrier that never completes, then sets

@@ -321,6 +321,19 @@ cudaError_t launch_analysis(const T *reg, const double *G0, const double *G0b, c
     return cudaGetLastError();
 }
 
+// The reference's stop test on one analysis (nuosc_ana.cpp:131: max||P|-1|
+// must stay below 10; a non-finite value fails too), applied on the device to
+// the raw sums of launch_analysis (sums[0] max||P|-1|, sums[10] non-finite
+// count): the first failing check records its step in *halt.
+__global__ void k_halt_check(const double *__restrict__ sums, int *__restrict__ halt, int step) {
+    if (threadIdx.x == 0 && *halt == 0 && (sums[10] > 0.0 || !(sums[0] < 10.0))) *halt = step;
+}
+
+cudaError_t launch_halt_check(const double *sums, int *halt, int step, cudaStream_t s) {
+    k_halt_check<<<1, 32, 0, s>>>(sums, halt, step);
+    return cudaGetLastError();
+}
+
 // ----------------------------------------------------------------------------
 // Snapshot gather (nuosc_snapshot.cpp:82-122): out[(ii*nz + j)*sv + vv] =
 // field(xidx[ii], j, vidx[vv]); fields 8..15 are the eval_conserved derived

@@ -139,7 +139,7 @@ __global__ void __launch_bounds__(TAIL_BLOCK, 3) k_stage_tail(const StageArgs<T>
 template <typename T, bool KO6, int MODE>
 __global__ void __launch_bounds__(TAIL_BLOCK, 2) k_stage_tail_batch(const TailItem<T> *__restrict__ items,
                                                                  const long long *__restrict__ starts, int n,
-                                                                 long long total) {
+                                                                 long long total, const int *__restrict__ halt) {
     const long long t = (long long)blockIdx.x * TAIL_BLOCK + threadIdx.x;
     if (t - (threadIdx.x & 31) >= total) return;  // whole warps past the end
     int lo = 0, hi = n - 1;
@@ -149,6 +149,7 @@ __global__ void __launch_bounds__(TAIL_BLOCK, 2) k_stage_tail_batch(const TailIt
         else hi = mid - 1;
     }
     const TailItem<T> &e = items[lo];
+    if (halt && halt[e.member]) return;  // a stopped instance: no work (whole warps: one item per warp)
     const long long u = t - starts[lo];
     const int l = (int)(u & (e.twp - 1));
     const long long ch = u / e.twp, cell = ch >> 1;
@@ -171,14 +172,14 @@ cudaError_t launch_tail_ko(const StageArgs<T> &a, int mode, int v0, int twp, int
 }
 
 template <typename T, bool KO6>
-cudaError_t launch_tail_batch_ko(const TailItem<T> *items, const long long *starts, int n, long long total, int mode,
-                                 cudaStream_t s) {
+cudaError_t launch_tail_batch_ko(const TailItem<T> *items, const long long *starts, int n, long long total,
+                                 const int *halt, int mode, cudaStream_t s) {
     const unsigned blocks = (unsigned)((total + TAIL_BLOCK - 1) / TAIL_BLOCK);
     switch (mode) {
-    case MODE_S1Y: k_stage_tail_batch<T, KO6, MODE_S1Y><<<blocks, TAIL_BLOCK, 0, s>>>(items, starts, n, total); break;
-    case MODE_S2B: k_stage_tail_batch<T, KO6, MODE_S2B><<<blocks, TAIL_BLOCK, 0, s>>>(items, starts, n, total); break;
-    case MODE_SY: k_stage_tail_batch<T, KO6, MODE_SY><<<blocks, TAIL_BLOCK, 0, s>>>(items, starts, n, total); break;
-    case MODE_S4B: k_stage_tail_batch<T, KO6, MODE_S4B><<<blocks, TAIL_BLOCK, 0, s>>>(items, starts, n, total); break;
+    case MODE_S1Y: k_stage_tail_batch<T, KO6, MODE_S1Y><<<blocks, TAIL_BLOCK, 0, s>>>(items, starts, n, total, halt); break;
+    case MODE_S2B: k_stage_tail_batch<T, KO6, MODE_S2B><<<blocks, TAIL_BLOCK, 0, s>>>(items, starts, n, total, halt); break;
+    case MODE_SY: k_stage_tail_batch<T, KO6, MODE_SY><<<blocks, TAIL_BLOCK, 0, s>>>(items, starts, n, total, halt); break;
+    case MODE_S4B: k_stage_tail_batch<T, KO6, MODE_S4B><<<blocks, TAIL_BLOCK, 0, s>>>(items, starts, n, total, halt); break;
     default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
@@ -202,17 +203,17 @@ cudaError_t launch_stage_tail(const StageArgs<T> &a, int mode, bool ko6, int v0,
 
 template <typename T>
 cudaError_t launch_stage_tail_batch(const TailItem<T> *items, const long long *starts, int n, long long total,
-                                    int mode, bool ko6, cudaStream_t s) {
+                                    const int *halt, int mode, bool ko6, cudaStream_t s) {
     if (n < 1 || total < 1) return cudaErrorInvalidValue;
-    return ko6 ? launch_tail_batch_ko<T, true>(items, starts, n, total, mode, s)
-               : launch_tail_batch_ko<T, false>(items, starts, n, total, mode, s);
+    return ko6 ? launch_tail_batch_ko<T, true>(items, starts, n, total, halt, mode, s)
+               : launch_tail_batch_ko<T, false>(items, starts, n, total, halt, mode, s);
 }
 
 template cudaError_t launch_stage_tail<double>(const StageArgs<double> &, int, bool, int, int, cudaStream_t);
 template cudaError_t launch_stage_tail<float>(const StageArgs<float> &, int, bool, int, int, cudaStream_t);
-template cudaError_t launch_stage_tail_batch<double>(const TailItem<double> *, const long long *, int, long long, int,
-                                                     bool, cudaStream_t);
-template cudaError_t launch_stage_tail_batch<float>(const TailItem<float> *, const long long *, int, long long, int,
-                                                    bool, cudaStream_t);
+template cudaError_t launch_stage_tail_batch<double>(const TailItem<double> *, const long long *, int, long long,
+                                                     const int *, int, bool, cudaStream_t);
+template cudaError_t launch_stage_tail_batch<float>(const TailItem<float> *, const long long *, int, long long,
+                                                    const int *, int, bool, cudaStream_t);
 
 }  // namespace nuosc

@@ -399,7 +399,7 @@ cudaError_t launch_moment_finalize(const double *part, double *mom, Geom g, int 
 namespace {
 // k_moment_finalize over the cells of many instances (same summation order)
 __global__ void k_moment_finalize_batch(const FinalizeItem *__restrict__ items, const long long *__restrict__ starts,
-                                        int n, long long total) {
+                                        int n, long long total, const int *__restrict__ halt) {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= total) return;
     int lo = 0, hi = n - 1;
@@ -408,6 +408,7 @@ __global__ void k_moment_finalize_batch(const FinalizeItem *__restrict__ items, 
         if (starts[mid] <= t) lo = mid;
         else hi = mid - 1;
     }
+    if (halt && halt[lo]) return;  // a stopped instance keeps its moments
     const FinalizeItem e = items[lo];
     const long long u = t - starts[lo];
     const long long cell = u / NMOM;
@@ -420,9 +421,9 @@ __global__ void k_moment_finalize_batch(const FinalizeItem *__restrict__ items, 
 }  // namespace
 
 cudaError_t launch_moment_finalize_batch(const FinalizeItem *items, const long long *starts, int n, long long total,
-                                         cudaStream_t s) {
+                                         const int *halt, cudaStream_t s) {
     if (n < 1 || total < 1) return cudaErrorInvalidValue;
-    k_moment_finalize_batch<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(items, starts, n, total);
+    k_moment_finalize_batch<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(items, starts, n, total, halt);
     return cudaGetLastError();
 }
 

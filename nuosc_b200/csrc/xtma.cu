@@ -737,14 +737,14 @@ struct __align__(64) BatchItem {
 template <typename T, int R, int MODE, int TZ, bool VAC, bool M64>
 __global__ void __launch_bounds__(32 * TZ, tma_ctas_per_sm<T, TZ>())
     k_xtma_batch(const BatchItem<T> *items, const long long *__restrict__ starts, int ninst, long long nitems,
-                 unsigned long long *counter) {
+                 unsigned long long *counter, const int *__restrict__ halt) {
     constexpr int NW = (int)(sizeof(StageArgs<T>) / 8);
     static_assert(sizeof(StageArgs<T>) % 8 == 0 && NW <= 32 * TZ, "StageArgs copy: one 8-byte word per thread");
     extern __shared__ __align__(1024) unsigned char smem[];
     __shared__ MarchShared<T, M64> sh;
     __shared__ __align__(16) StageArgs<T> s_a;
     __shared__ const TmaMaps *s_mp;
-    __shared__ int s_t[6];  // instance, z0, vb, xs, xe, half
+    __shared__ int s_t[6];  // instance (-1: no tiles left, -2: a stopped instance's tile), z0, vb, xs, xe, half
     for (;;) {
         __syncthreads();  // every thread is done with the previous tile's arguments
         if (threadIdx.x == 0) {
@@ -759,12 +759,12 @@ __global__ void __launch_bounds__(32 * TZ, tma_ctas_per_sm<T, TZ>())
                 }
                 const BatchItem<T> &e = items[lo];
                 long long loc = it - starts[lo];  // ((seg * 2 + half) * ntz + zt) * nvbm + vb
+                s_t[0] = (halt && halt[lo]) ? -2 : lo;
                 const int vb = (int)(loc % e.nvbm);
                 loc /= e.nvbm;
                 const int zt = (int)(loc % e.ntz);
                 loc /= e.ntz;
                 const int xs = (int)(loc >> 1) * e.lx;
-                s_t[0] = lo;
                 s_t[1] = zt * TZ;
                 s_t[2] = vb;
                 s_t[3] = xs;
@@ -783,7 +783,8 @@ __global__ void __launch_bounds__(32 * TZ, tma_ctas_per_sm<T, TZ>())
         }
         __syncthreads();
         const int lo = s_t[0];
-        if (lo < 0) break;
+        if (lo == -1) break;
+        if (lo == -2) continue;  // every thread: the loop's first barrier comes next
         if (threadIdx.x < NW)
             reinterpret_cast<long long *>(&s_a)[threadIdx.x] =
                 reinterpret_cast<const long long *>(&items[lo].a)[threadIdx.x];
@@ -945,9 +946,9 @@ int batch_grid_t(int device) {
 
 template <typename T, int R, int MODE, int TZ, bool VAC, bool M64>
 cudaError_t batch_launch_t(const void *items, const long long *starts, int n, long long ntiles,
-                           unsigned long long *counter, int grid, cudaStream_t s) {
+                           unsigned long long *counter, const int *halt, int grid, cudaStream_t s) {
     k_xtma_batch<T, R, MODE, TZ, VAC, M64><<<grid, 32 * TZ, batch_smem<T, R, MODE, TZ>(), s>>>(
-        (const BatchItem<T> *)items, starts, n, ntiles, counter);
+        (const BatchItem<T> *)items, starts, n, ntiles, counter, halt);
     return cudaGetLastError();
 }
 
@@ -975,8 +976,8 @@ struct BatchGrid {
 template <typename T, int R, int MODE, int TZ, bool VAC, bool M64>
 struct BatchLaunch {
     static cudaError_t run(const void *items, const long long *starts, int n, long long ntiles,
-                           unsigned long long *counter, int grid, cudaStream_t s) {
-        return batch_launch_t<T, R, MODE, TZ, VAC, M64>(items, starts, n, ntiles, counter, grid, s);
+                           unsigned long long *counter, const int *halt, int grid, cudaStream_t s) {
+        return batch_launch_t<T, R, MODE, TZ, VAC, M64>(items, starts, n, ntiles, counter, halt, grid, s);
     }
 };
 
@@ -1024,17 +1025,18 @@ int xtma_batch_grid(int mode, bool ko6, int tz, bool vac, bool m64, int device) 
 
 template <typename T>
 cudaError_t launch_stage_xtma_batch(const void *items, const long long *starts, int n, long long ntiles,
-                                    unsigned long long *counter, int mode, bool ko6, int tz, bool vac, bool m64,
-                                    int grid, cudaStream_t s) {
+                                    unsigned long long *counter, const int *halt, int mode, bool ko6, int tz,
+                                    bool vac, bool m64, int grid, cudaStream_t s) {
     if ((tz != 8 && tz != 16) || !tma_mode(mode) || n < 1 || grid < 1)
         return cudaErrorInvalidValue;
     if constexpr (sizeof(T) == 8)
-        return batch_dispatch<T, true, BatchLaunch>(mode, ko6, tz, vac, items, starts, n, ntiles, counter, grid, s);
+        return batch_dispatch<T, true, BatchLaunch>(mode, ko6, tz, vac, items, starts, n, ntiles, counter, halt, grid,
+                                                    s);
     else
-        return m64 ? batch_dispatch<T, true, BatchLaunch>(mode, ko6, tz, vac, items, starts, n, ntiles, counter, grid,
-                                                          s)
+        return m64 ? batch_dispatch<T, true, BatchLaunch>(mode, ko6, tz, vac, items, starts, n, ntiles, counter, halt,
+                                                          grid, s)
                    : batch_dispatch<T, false, BatchLaunch>(mode, ko6, tz, vac, items, starts, n, ntiles, counter,
-                                                           grid, s);
+                                                           halt, grid, s);
 }
 
 template <typename T>
@@ -1070,10 +1072,10 @@ template long long xtma_batch_fill<float>(void *, const StageArgs<float> &, bool
 template int xtma_batch_grid<double>(int, bool, int, bool, bool, int);
 template int xtma_batch_grid<float>(int, bool, int, bool, bool, int);
 template cudaError_t launch_stage_xtma_batch<double>(const void *, const long long *, int, long long,
-                                                     unsigned long long *, int, bool, int, bool, bool, int,
-                                                     cudaStream_t);
+                                                     unsigned long long *, const int *, int, bool, int, bool, bool,
+                                                     int, cudaStream_t);
 template cudaError_t launch_stage_xtma_batch<float>(const void *, const long long *, int, long long,
-                                                    unsigned long long *, int, bool, int, bool, bool, int,
-                                                    cudaStream_t);
+                                                    unsigned long long *, const int *, int, bool, int, bool, bool,
+                                                    int, cudaStream_t);
 
 }  // namespace nuosc

@@ -21,12 +21,14 @@ parameters, a step count and a precision) arrive over time; the server
   * streams the analysis record (Pee, max||P|-1|, ...) of every solve every
     100 of its steps -- queued on the device between the batch's steps, no
     host synchronisation -- and at its last step;
-  * retires a solve as failed when a streamed record reports a blown-up state
-    (a non-finite value or max||P|-1| >= 10, the reference's assert in
-    nuosc_ana.cpp:131): it leaves its batch at the end of the quantum in
-    which the record arrives; its steps up to its last good record count as
-    served work (the reference computes them too before it stops), the steps
-    after it do not, and it has no completion latency;
+  * retires a solve as failed when its state blows up (a non-finite value or
+    max||P|-1| >= 10, the reference's assert in nuosc_ana.cpp:131): the batch
+    applies that test on the device every `halt_every` steps of each member
+    (and at every streamed record) and stops a failing member at once -- its
+    work is skipped for the rest of the quantum --, and the member leaves its
+    batch at the end of the quantum; its steps up to its last passing check
+    count as served work (the reference computes them too before it stops),
+    the steps after it do not, and it has no completion latency;
   * reports per-request time-to-completion (p50/p99) and the aggregate
     cell-steps/s (nx*nz*nv per RK4 step).
 
@@ -53,6 +55,7 @@ DX = 0.1
 CFL = 0.4
 KO = 0.1
 STREAM_EVERY = 100
+HALT_EVERY = 10  # one analysis pass per 10 steps: about 0.8 % of a step's memory traffic
 
 
 @dataclass
@@ -92,7 +95,7 @@ class Record:
     rejected: bool = False
     failed: bool = False  # retired before its last step because its state blew up
     steps_run: int = 0
-    last_good: int = 0  # step of the last streamed record with a finite state
+    last_good: int = 0  # step of the last streamed record, or device-side check, with a passing state
 
     @property
     def latency(self):
@@ -181,7 +184,8 @@ class Server:
     """
 
     def __init__(self, budget_bytes=150e9, device=0, stream_every=STREAM_EVERY, on_diag=None, on_complete=None,
-                 solver_factory=None, batch_factory="default", quantum_s=0.25, max_resident_bytes=1.2e9):
+                 solver_factory=None, batch_factory="default", quantum_s=0.25, max_resident_bytes=1.2e9,
+                 halt_every=HALT_EVERY):
         self.budget = float(budget_bytes)
         # bytes of one state register summed over the resident solves beyond
         # which admitting more only time-shares a saturated GPU (every
@@ -191,6 +195,9 @@ class Server:
         self.quantum_s = float(quantum_s)  # target wall time of one quantum (admission granularity)
         self.device = device
         self.every = int(stream_every)
+        # steps between the device-side stop tests of a batch member (0: off;
+        # failed solves then run to the end of their quantum)
+        self.halt_every = int(halt_every)
         self.on_diag = on_diag
         self.on_complete = on_complete
         self.solver_factory = solver_factory or make_solver
@@ -244,17 +251,30 @@ class Server:
                 ratio = max(0.05, min(20.0, dt_q / q / model))
                 stats["quanta"] += 1
                 tc = time.perf_counter()
+                halted = {}  # rid -> step at which the batch stopped it on the device
+                got = []
                 for prec, buf in bufs.items():
                     ids = members[prec]
-                    for m, step, d in batches[prec].collect(buf):
-                        stream(ids[m], step, d)
+                    got += [(ids[m], step, d) for m, step, d in batches[prec].collect(buf)]
+                    if self.halt_every > 0 and hasattr(batches[prec], "halted"):
+                        for m, h in enumerate(batches[prec].halted()):
+                            if h > 0:
+                                halted[ids[m]] = h
+                for rid, step, d in got:
+                    if step <= halted.get(rid, step):  # (a stopped solve's later records repeat its stopped state)
+                        stream(rid, step, d)
+                for rid, h in halted.items():
+                    if recs[rid].diverged_at < 0:
+                        stream(rid, h, None)  # the failing device-side check is the solve's last record
+                    recs[rid].last_good = max(recs[rid].last_good, h - self.halt_every)  # the previous check passed
                 host["collect_s"] += time.perf_counter() - tc
                 done = []
                 for rid in ran:
                     a = active[rid]
                     a[1] += q
-                    recs[rid].steps_run = a[1]
-                    stats["steps_run"] += q
+                    ran_steps = min(a[1], halted[rid]) if rid in halted else a[1]
+                    stats["steps_run"] += ran_steps - recs[rid].steps_run
+                    recs[rid].steps_run = ran_steps
                     if a[1] == recs[rid].req.steps or recs[rid].diverged_at >= 0:
                         done.append(rid)
                 for rid in done:
@@ -292,6 +312,8 @@ class Server:
                             batches[prec] = None
                         if ids and self.batch_factory is not None:
                             batches[prec] = self.batch_factory([active[rid][0] for rid in ids])
+                            if self.halt_every > 0 and hasattr(batches[prec], "set_halt"):
+                                batches[prec].set_halt(self.halt_every)
                             stats["batch_builds"] += 1
                         members[prec] = ids
                 host["build_s"] += time.perf_counter() - tc

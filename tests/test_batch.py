@@ -130,3 +130,59 @@ def test_batch_rejects_bad_membership(nb):
     finally:
         for s in (a, c, d):
             s.close()
+
+
+def off_polarised(nb, s):
+    """A state whose polarisation is far off |P| = 1 (emr 20x the diagonal):
+    max||P|-1| is about 19, so the reference's stop test fails at once."""
+    st = s.get_state()
+    st[2] = 20.0 * st[0]
+    s.set_state(st)
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_batch_halt_stops_failed_member(nb, precision):
+    """nuosc_batch_set_halt: the member that fails the stop test is stopped at
+    the first device-side check (step 5) and keeps that state; the others run
+    on.  Every member equals its solo run bit for bit: the stopped one after 5
+    steps, the others after 20."""
+    specs = [dict(nx=48, nz=32, nn=2, seed=31), dict(nx=32, nz=32, nn=4, seed=32),
+             dict(nx=64, nz=48, nn=8, seed=33)]
+    batch = [build(nb, precision=precision, **sp) for sp in specs]
+    solo = [build(nb, precision=precision, **sp) for sp in specs]
+    off_polarised(nb, batch[1])
+    off_polarised(nb, solo[1])
+    with pytest.raises(nb.NuoscError):
+        solo[1].analysis()  # the state fails the reference's test from the start
+    bt = nb.Batch(batch)
+    bt.set_halt(5)
+    bt.step_rk4(20)
+    bt.synchronize()
+    assert bt.halted() == [0, 5, 0]
+    bt.close()
+    solo[0].step_rk4(20)
+    solo[1].step_rk4(5)
+    solo[2].step_rk4(20)
+    for a, b in zip(batch, solo):
+        assert np.array_equal(bits(a), bits(b))
+    for s in batch + solo:
+        s.close()
+
+
+def test_batch_without_halt_steps_every_member(nb):
+    """Checks off (the default): a failing member is stepped like the others."""
+    specs = [dict(nx=48, nz=32, nn=2, seed=41), dict(nx=32, nz=32, nn=2, seed=42)]
+    batch = [build(nb, **sp) for sp in specs]
+    solo = [build(nb, **sp) for sp in specs]
+    off_polarised(nb, batch[1])
+    off_polarised(nb, solo[1])
+    bt = nb.Batch(batch)
+    bt.step_rk4(10)
+    bt.synchronize()
+    assert bt.halted() == [0, 0]
+    bt.close()
+    for a, b in zip(batch, solo):
+        b.step_rk4(10)
+        assert np.array_equal(bits(a), bits(b))
+    for s in batch + solo:
+        s.close()
