@@ -580,8 +580,9 @@ def bench_serving(args, local, single):
             "note": "single-large-solve reference = the 1024x1024x642 FP64/FP32 solves timed above, weighted by "
                     "the requests' FP64/FP32 cell-steps; one-at-a-time latencies from measured per-shape FP64 step "
                     "times (modelled: FIFO over measured per-shape step times, no host costs); a request whose "
-                    "streamed analysis reports a blown-up state is retired as failed ('failed'): its cell-steps up "
-                    "to its last good record count, the ones after it do not, and it has no latency; "
+                    "state fails the reference's stop test (non-finite, or max||P|-1| >= 10; checked on the device "
+                    "every 10 steps) is stopped on the device and retired as failed ('failed'): its cell-steps up "
+                    "to its last passing check count, the ones after it do not, and it has no latency; "
                     "the 512-request run is in profiles/serving_512_requests.md"}
 
 
