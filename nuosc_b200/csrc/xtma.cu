@@ -20,12 +20,13 @@
 //     before the waits and the stencil; the issuing lane prefetches their TZ
 //     rows into L2 two planes ahead with a tensor prefetch
 //     (cp.async.bulk.prefetch.tensor), so the loads find them in L2;
-//   * moment partials (FP64; in FP32 summed in float over the block, stored
-//     as double): each lane holds its 16 (12 + 4 zero) partial moments in
-//     a lane-dependent permuted order (weights permuted once per tile, the
-//     three moment combinations by two selects per plane), so the
-//     reduce-scatter over the 32 lanes of the warp keeps the lower half at
-//     every step (15 shuffle-adds + 1).
+//   * moment partials (FP64 products and sums; FP32 state may sum in float
+//     within the block, stored as double): each lane forms its 12 products
+//     (3 combinations x 4 weights, the weights in a lane-permuted order set
+//     once per tile) and the warp reduce-scatters them over its 32 lanes
+//     with 13 shuffle-adds;
+//   * a stopped instance of a batch (its halt flag set by the device-side
+//     stop test) has its tiles skipped.
 // All mbarrier waits are bounded: on expiry the kernel records the timeout in
 // the status word, stops marching and, before returning, waits (again
 // bounded) for the copies it issued.  Requires nz % TZ == 0.
