@@ -1,9 +1,11 @@
 """Serving loop (nuosc_b200.serve).
 
-CPU: the scheduling logic with fake solvers -- every request runs exactly
+CPU: the scheduling logic with fake solvers and batches -- every request runs exactly
 its step count, analysis records are streamed every `every` steps and at the
 last step, admission keeps the resident footprint within the budget and
-follows arrival order, oversize requests are rejected, and the one-at-a-time
+follows arrival order, oversize requests are rejected, failed solves are
+retired (after a blown-up record, or at once by the batch's device-side stop)
+with their work counted up to their last passing check, and the one-at-a-time
 queue model.
 GPU: a mixed FP32/FP64 stream of overlapping requests through the real
 batched path; every request's final state and every streamed record equals
@@ -261,4 +263,74 @@ def test_blown_up_solves_are_retired_as_failed():
     assert rep["cell_steps"] == sum(r.cell_steps for r in ok) + (200 + 0) * 32 * 32 * 42
     assert rep["failed_cell_steps_run"] == (300 + 100) * 32 * 32 * 42
     assert rep["failed_cell_steps_counted"] == 200 * 32 * 32 * 42
+    assert not FakeBatch.live
+
+
+class HaltBatch(BlowUpBatch):
+    """A fake batch with the device-side stop (Batch.set_halt/halted): every
+    `halt_every` of a member's steps, and at every streamed record, the stop
+    test runs on the member's state; a member that fails it stops stepping,
+    while its step counter (kept on the solver, as the handle keeps it) goes
+    on and its later records repeat its stopped state."""
+
+    def __init__(self, solvers):
+        super().__init__(solvers)
+        self.halt_every = 0
+        for s in self.solvers:
+            if not hasattr(s, "counter"):
+                s.counter, s.stopped = s.steps, 0
+
+    def set_halt(self, k):
+        self.halt_every = k
+
+    def halted(self):
+        return [s.stopped for s in self.solvers]
+
+    def step_stream(self, n, every):
+        recs = []
+        for _ in range(n):
+            for m, s in enumerate(self.solvers):
+                s.counter += 1
+                if not s.stopped:
+                    s.step_rk4(1)
+                rec = s.counter % every == 0
+                if rec or (self.halt_every and s.counter % self.halt_every == 0):
+                    d, bad = serve._analysis(s)
+                    if bad and self.halt_every and not s.stopped:
+                        s.stopped = s.counter
+                    if rec:
+                        recs.append((m, s.counter, d))
+        return recs
+
+
+def test_device_stop_retires_failed_solves_at_once():
+    """With the batch's device-side stop (checks every 10 steps) a failed solve
+    stops at its first failing check even in the middle of a long quantum: it
+    runs no further steps, its records after the stop are dropped, the failing
+    check is its last record, and its steps up to the previous (passing)
+    check count as served work."""
+    reqs = serve.draw_requests(6, rate=0.0, seed=4, steps=(900, 1000), sizes=(32,), nns=(2,))
+    BlowUpSolver.bad = {reqs[1].rid: 250, reqs[4].rid: 100}
+    made, diags = {}, {}
+
+    def factory(req, device):
+        made[req.rid] = BlowUpSolver(req)
+        return made[req.rid]
+
+    srv = serve.Server(budget_bytes=1e12, stream_every=100, solver_factory=factory, batch_factory=HaltBatch,
+                       quantum_s=1e9, halt_every=10,
+                       on_diag=lambda rid, step, d: diags.setdefault(rid, []).append((step, d)))
+    rep = srv.run(reqs)
+    assert rep["failed"] == 2 and rep["served"] == 4
+    assert made[reqs[1].rid].steps == 250 and made[reqs[4].rid].steps == 100
+    assert diags[reqs[1].rid][-1] == (250, None) and all(d is not None for _, d in diags[reqs[1].rid][:-1])
+    assert [s for s, _ in diags[reqs[1].rid]] == [0, 100, 200, 250]
+    assert diags[reqs[4].rid][-1] == (100, None)
+    cells = 32 * 32 * 42
+    ok = [r for r in reqs if r.rid not in BlowUpSolver.bad]
+    assert rep["cell_steps"] == sum(r.cell_steps for r in ok) + (240 + 90) * cells
+    assert rep["failed_cell_steps_run"] == (250 + 100) * cells
+    assert rep["failed_cell_steps_counted"] == (240 + 90) * cells
+    for r in ok:
+        assert made[r.rid].steps == r.steps
     assert not FakeBatch.live
