@@ -1683,10 +1683,12 @@ int batch_build(nuosc_batch *b) {
         if (e == cudaSuccess) e = launch_moment_finalize_batch(b->d_fin, b->d_fstarts, n, nmom, b->d_halt, b->stream);
         per_step += 2;
     }
-    for (nuosc_handle *h : b->m) {
+    for (int i = 0; i < n; ++i) {
+        nuosc_handle *h = b->m[i];
         if (!h->renorm || e != cudaSuccess) continue;
-        e = launch_renormalize<T>((T *)h->reg[0], h->dG0(), h->dG0b(), h->g, b->stream);
-        if (e == cudaSuccess) e = launch_moments<T>((const T *)h->reg[0], h->d_mom, h->quad(), h->g, b->stream);
+        e = launch_renormalize<T>((T *)h->reg[0], h->dG0(), h->dG0b(), h->g, b->stream, b->d_halt + i);
+        if (e == cudaSuccess)
+            e = launch_moments<T>((const T *)h->reg[0], h->d_mom, h->quad(), h->g, b->stream, b->d_halt + i);
         per_step += 2;
     }
     cudaGraph_t graph = nullptr;

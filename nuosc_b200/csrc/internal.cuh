@@ -106,8 +106,9 @@ __host__ __device__ inline long long halo_offset(int F, int p, int nx, int R, lo
 }
 
 // ---------------------------------------------------------------- launches
+// halt (null by default): a batch member's stop flag; when set, nothing is done
 template <typename T>
-cudaError_t launch_moments(const T *reg, double *mom, Quad q, Geom g, cudaStream_t s);
+cudaError_t launch_moments(const T *reg, double *mom, Quad q, Geom g, cudaStream_t s, const int *halt = nullptr);
 template <typename T>
 cudaError_t launch_stage_direct(const StageArgs<T> &a, int mode, bool ko6, cudaStream_t s);
 
@@ -224,6 +225,7 @@ cudaError_t launch_export(const T *reg_field, double *dst, Geom g, int layout, i
 template <typename T>
 cudaError_t launch_vectorize(T *dst, const T *a, double c, const T *b, const T *d, Geom g, cudaStream_t s);
 template <typename T>
-cudaError_t launch_renormalize(T *reg, const double *G0, const double *G0b, Geom g, cudaStream_t s);
+cudaError_t launch_renormalize(T *reg, const double *G0, const double *G0b, Geom g, cudaStream_t s,
+                               const int *halt = nullptr);
 
 }  // namespace nuosc

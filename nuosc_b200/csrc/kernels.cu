@@ -12,7 +12,9 @@ namespace nuosc {
 // reduction (fixed order, so the result is deterministic).
 // ----------------------------------------------------------------------------
 template <typename T>
-__global__ void __launch_bounds__(256) k_moments(const T *__restrict__ in, double *__restrict__ mom, Quad q, Geom g) {
+__global__ void __launch_bounds__(256) k_moments(const T *__restrict__ in, double *__restrict__ mom, Quad q, Geom g,
+                                                 const int *__restrict__ halt) {
+    if (halt && *halt) return;  // a stopped batch member keeps its moments
     const int lane = threadIdx.x & 31;
     const long long cell = (long long)blockIdx.x * 8 + (threadIdx.x >> 5);
     if (cell >= g.ncell) return;
@@ -46,9 +48,9 @@ __global__ void __launch_bounds__(256) k_moments(const T *__restrict__ in, doubl
 }
 
 template <typename T>
-cudaError_t launch_moments(const T *reg, double *mom, Quad q, Geom g, cudaStream_t s) {
+cudaError_t launch_moments(const T *reg, double *mom, Quad q, Geom g, cudaStream_t s, const int *halt) {
     const long long blocks = (g.ncell + 7) / 8;
-    k_moments<T><<<(unsigned)blocks, 256, 0, s>>>(reg, mom, q, g);
+    k_moments<T><<<(unsigned)blocks, 256, 0, s>>>(reg, mom, q, g, halt);
     return cudaGetLastError();
 }
 
@@ -442,7 +444,8 @@ cudaError_t launch_vectorize(T *dst, const T *a, double c, const T *b, const T *
 // (including its ee = G0 + tmp convention) so set_renorm(1) behaves the same.
 // ----------------------------------------------------------------------------
 template <typename T>
-__global__ void k_renormalize(T *st, const double *G0, const double *G0b, Geom g) {
+__global__ void k_renormalize(T *st, const double *G0, const double *G0b, Geom g, const int *halt) {
+    if (halt && *halt) return;  // a stopped batch member keeps its state
     const int v = blockIdx.y * 32 + threadIdx.x;
     const long long cell = (long long)blockIdx.x * 8 + threadIdx.y;
     if (cell >= g.ncell || v >= g.nv) return;
@@ -466,15 +469,15 @@ __global__ void k_renormalize(T *st, const double *G0, const double *G0b, Geom g
     st[o + 7 * fs] = T(bemi * iPb);
 }
 template <typename T>
-cudaError_t launch_renormalize(T *reg, const double *G0, const double *G0b, Geom g, cudaStream_t s) {
+cudaError_t launch_renormalize(T *reg, const double *G0, const double *G0b, Geom g, cudaStream_t s, const int *halt) {
     dim3 block(32, 8), grid((unsigned)((g.ncell + 7) / 8), (g.nvs + 31) / 32);
-    k_renormalize<T><<<grid, block, 0, s>>>(reg, G0, G0b, g);
+    k_renormalize<T><<<grid, block, 0, s>>>(reg, G0, G0b, g, halt);
     return cudaGetLastError();
 }
 
 // ---------------------------------------------------------------- instances
 #define NUOSC_INSTANTIATE(T)                                                                                   \
-    template cudaError_t launch_moments<T>(const T *, double *, Quad, Geom, cudaStream_t);                    \
+    template cudaError_t launch_moments<T>(const T *, double *, Quad, Geom, cudaStream_t, const int *);       \
     template cudaError_t launch_stage_direct<T>(const StageArgs<T> &, int, bool, cudaStream_t);              \
     template cudaError_t launch_init<T>(T *, const double *, const double *, Geom, int, double, double, double, \
                                         double, uint64_t, const double *, int, cudaStream_t);                 \
@@ -485,7 +488,7 @@ cudaError_t launch_renormalize(T *reg, const double *G0, const double *G0b, Geom
     template cudaError_t launch_import<T>(T *, const double *, Geom, int, int, int, cudaStream_t);            \
     template cudaError_t launch_export<T>(const T *, double *, Geom, int, int, int, cudaStream_t);            \
     template cudaError_t launch_vectorize<T>(T *, const T *, double, const T *, const T *, Geom, cudaStream_t); \
-    template cudaError_t launch_renormalize<T>(T *, const double *, const double *, Geom, cudaStream_t);
+    template cudaError_t launch_renormalize<T>(T *, const double *, const double *, Geom, cudaStream_t, const int *);
 
 NUOSC_INSTANTIATE(double)
 NUOSC_INSTANTIATE(float)

@@ -186,3 +186,29 @@ def test_batch_without_halt_steps_every_member(nb):
         assert np.array_equal(bits(a), bits(b))
     for s in batch + solo:
         s.close()
+
+
+def test_batch_halt_stops_renormalised_member(nb):
+    """A stopped member with renormalisation on is left alone too (the batch's
+    renormalisation and moment passes skip it): a non-finite value planted in
+    member 1 fails the stop test at step 5, and member 1 then stays its solo
+    state after 5 steps while member 0 (renormalised as well) runs 12."""
+    specs = [dict(nx=48, nz=32, nn=2, seed=51, renorm=True), dict(nx=32, nz=32, nn=2, seed=52, renorm=True)]
+    batch = [build(nb, **sp) for sp in specs]
+    solo = [build(nb, **sp) for sp in specs]
+    for s in (batch[1], solo[1]):
+        st = s.get_state()
+        st[0, 3, 5, 7] = np.nan
+        s.set_state(st)
+    bt = nb.Batch(batch)
+    bt.set_halt(5)
+    bt.step_rk4(12)
+    bt.synchronize()
+    assert bt.halted() == [0, 5]
+    bt.close()
+    solo[0].step_rk4(12)
+    solo[1].step_rk4(5)
+    for a, b in zip(batch, solo):
+        assert np.array_equal(bits(a), bits(b))
+    for s in batch + solo:
+        s.close()
