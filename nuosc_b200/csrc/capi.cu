@@ -1859,7 +1859,8 @@ int nuosc_batch_set_halt(nuosc_batch *b, int check_every) {
 
 int nuosc_batch_halted(nuosc_batch *b, int *steps, int n) {
     if (!b || !steps) return fail(NUOSC_ERR_INVALID, "null argument");
-    if (n != (int)b->m.size()) return fail(NUOSC_ERR_INVALID, "batch_halted: %d entries for %d members", n, (int)b->m.size());
+    if (n != (int)b->m.size())
+        return fail(NUOSC_ERR_INVALID, "batch_halted: %d entries for %d members", n, (int)b->m.size());
     CUDA_TRY(cudaSetDevice(b->device));
     std::vector<int> h(n);
     CUDA_TRY(cudaMemcpyAsync(h.data(), b->d_halt, n * sizeof(int), cudaMemcpyDeviceToHost, b->stream));
