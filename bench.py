@@ -443,14 +443,16 @@ def bench_fp32(args, local, v64):
     s.step_rk4(args.warmup)
     s.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(st)
-    s.step_rk4(args.steps)
-    e1.record(st)
-    e1.synchronize()
+    with ClockSampler(local) as clk:  # the FP32 run's own clocks (the ratio compares two timed regions)
+        e0.record(st)
+        s.step_rk4(args.steps)
+        e1.record(st)
+        e1.synchronize()
     ms = e0.elapsed_time(e1) / args.steps
     s.close()
     v = cells / (ms / 1e3)
     return {"value": v, "unit": METRIC, "ms_per_step": ms, "vs_fp64": v / v64, "steps": args.steps,
+            "clocks": clk.summary(),
             "note": "same workload, FP32 state, FP64 moment sums and diagnostics; accuracy vs FP64 in "
                     "profiles/fp32_vs_fp64_1024x642.md"}
 
