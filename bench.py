@@ -18,11 +18,11 @@ e2e      the same metric through the public C ABI with host buffers: upload
          analysis() (diagnostics read back), download the final state.
 roofline the dominant stage kernel (largest share of the live step time)
          timed with CUDA events on the solver's stream: the state passes that
-         stage reads and writes in the 13-pass step (S1 2, S2 4, S3 3, S4 4)
+         stage reads and writes in the 12-pass step (S1 2, S2 4, S3 3, S4 3)
          x 8 fields x 8 B per cell-velocity / mean launch time, against
          the measured HBM copy bandwidth in MEASURED_PEAKS.json.  Step figures
          use the classic RK4 sequence's 1024 B per cell-step (step_frac,
-         frac_vs_8tbs) and the 832 B this implementation moves (step_moved_*);
+         frac_vs_8tbs) and the 768 B this implementation moves (step_moved_*);
          ncu's DRAM traffic per launch is `traffic` (per step: step_traffic).
 N > 1    one independent full-size solve per GPU (the reference's hot path has
          no exchange on one GPU); value = all ranks' cell-steps / max time.
@@ -54,15 +54,15 @@ METRIC = "cell-steps/s"
 # Y (5 each); S4 reads Y and A, writes U (3) -- 16 passes x 8 fields x
 # sizeof(real) per cell-step, the fixed work figure the roofline counts.
 BYTES_PER_CELL_STEP = {"f64": 1024, "f32": 512}
-# State passes (8 fields each) per stage launch in the 13-pass step of the TMA
+# State passes (8 fields each) per stage launch in the 12-pass step of the TMA
 # path: S1 reads U, writes Y2; S2 reads Y2 and U, writes Y3 and B; S3 reads Y3
-# and U, writes Y4; S4 reads Y4, U and B, writes U.
-STAGE_PASSES = {"stage_s1": 2, "stage_s2": 4, "stage_s3": 3, "stage_s4": 4}
+# and U, writes Y4; S4 reads Y4 and B, writes U.
+STAGE_PASSES = {"stage_s1": 2, "stage_s2": 4, "stage_s3": 3, "stage_s4": 3}
 # The classic sequence's passes for the same stage work (S1 3, S2 5, S3 5, S4 3),
 # reported beside as classic_frac
 CLASSIC_PASSES = {"stage_s1": 3, "stage_s2": 5, "stage_s3": 5, "stage_s4": 3}
 STAGE_NAMES = {"stage_s1": "S1", "stage_s2": "S2", "stage_s3": "S3", "stage_s4": "S4"}
-MOVED_BYTES_PER_CELL_STEP = {"f64": 13 * 64, "f32": 13 * 32}
+MOVED_BYTES_PER_CELL_STEP = {"f64": 12 * 64, "f32": 12 * 32}
 
 
 def workload(size, nn, precision):

@@ -59,16 +59,15 @@ struct Quad {
 //   MODE_S23 : acc_dst = acc_src + cA*k ;     y_dst = u  + cY*k
 //   MODE_S4  : acc_dst = acc_src + cA*k
 // (the classic 16-pass sequence of the direct and cp.async paths), and the
-// 13-pass sequence of the TMA path:
+// 12-pass sequence of the TMA path:
 //   MODE_S1Y : y_dst = in + cY*k                       (Y2 = U + dt/2 k1)
-//   MODE_S2B : y_dst = u + cY*k ; acc_dst = (in - u) + cA*k
-//                                   (Y3 = U + dt/2 k2, B = dt/2 k1 + dt k2)
+//   MODE_S2B : y_dst = u + cY*k ; acc_dst = (u + in) + cA*k
+//                                   (Y3 = U + dt/2 k2, B = U + Y2 + dt k2)
 //   MODE_SY  : y_dst = u + cY*k                        (Y4 = U + dt k3)
-//   MODE_S4B : acc_dst = u + (acc_src + (in - u))/3 + cA*k
-// In S4B, in = Y4, acc_src = B and cA = dt/6, so the update is
-// U + dt/6 (k1 + 2 k2 + 2 k3 + k4); dt/2 k1 = Y2 - U and dt k3 = Y4 - U are
-// recovered as differences of nearby values (exact by Sterbenz where they
-// lie within a factor 2).
+//   MODE_S4B : acc_dst = (acc_src + in)/3 + cA*k
+// In S4B, in = Y4, acc_src = B and cA = dt/6: (B + Y4)/3 = U + dt/6 k1 +
+// dt/3 k2 + dt/3 k3, so the update is U + dt/6 (k1 + 2 k2 + 2 k3 + k4)
+// without reading U.
 enum StageMode {
     MODE_RHS = 0, MODE_S1 = 1, MODE_S23 = 2, MODE_S4 = 3, MODE_S1Y = 5, MODE_SY = 6, MODE_S4B = 7, MODE_S2B = 8
 };

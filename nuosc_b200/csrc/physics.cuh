@@ -29,6 +29,19 @@ __device__ __forceinline__ double inp(const double *m, double vx, double vy, dou
     return m[0] - m[1] * vx - m[2] * vy - m[3] * vz;
 }
 
+// s/3 + t, with s the 3U-sized sum B + Y4 of the 12-pass step's last stage and
+// t the small dt/6 k4.  q = s * (1/3) carries the rounded constant's relative
+// error (3e-8 in float) on the whole sum -- a bias that would grow U by that
+// much every step --; the exact remainder r = s - 3q (one fma) restores
+// s/3 = q + r/3, and the small terms are summed before the one rounding at
+// U's size.
+template <typename T>
+__device__ __forceinline__ T third_plus(T s, T t) {
+    const T q = s * T(1.0 / 3.0);
+    const T r = fma(-q, T(3), s);
+    return q + fma(r, T(1.0 / 3.0), t);
+}
+
 // Self-interaction and vacuum terms for one flavour half.  `c` holds the
 // centre values (ee, mm, emr, emi) or (bee, bmm, bemr, bemi); `a`, `b`, `e`
 // are INP(emRm), INP(emIp), INP(eemm).  Adds into out[0..3] (which hold

@@ -89,13 +89,11 @@ __device__ __forceinline__ void tail_point(const StageArgs<T> &a, const long lon
                 a.y_dst[idx] = outm[f];
             } else if (MODE == MODE_S2B) {
                 const T u = a.u[idx];
-                a.acc_dst[idx] = (c4[f] - u) + cA * kv[f];  // B = dt/2 k1 + dt k2
+                a.acc_dst[idx] = (u + c4[f]) + cA * kv[f];  // B = U + Y2 + dt k2
                 outm[f] = u + cY * kv[f];                   // Y3
                 a.y_dst[idx] = outm[f];
             } else {
-                // U + [B + (Y4 - U)]/3 + dt/6 k4, as the TMA kernel
-                const T u = a.u[idx];
-                outm[f] = u + fma(a.acc_src[idx] + (c4[f] - u), T(1.0 / 3.0), cA * kv[f]);
+                outm[f] = third_plus(a.acc_src[idx] + c4[f], cA * kv[f]);  // (B + Y4)/3 + dt/6 k4
                 a.acc_dst[idx] = outm[f];
             }
         }

@@ -268,8 +268,8 @@ template <typename T, int R, int MODE, int TZ>
 struct MarchCfg {
     static constexpr int D = TZ == 16 ? 3 : 2;  // boxes issued ahead of their first use
     static constexpr int PFD = 2;                 // L2 prefetch distance of the pointwise inputs, planes
-    static constexpr bool PU = MODE == MODE_SY || MODE == MODE_S2B || MODE == MODE_S4B;  // reads U pointwise
-    static constexpr bool PA = MODE == MODE_S4B;                                       // reads B pointwise
+    static constexpr bool PU = MODE == MODE_SY || MODE == MODE_S2B;  // reads U pointwise
+    static constexpr bool PA = MODE == MODE_S4B;                     // reads B pointwise
     static constexpr int NS = R + D + 2;  // a box lives from its front use to its centre use, plus slack
     static constexpr size_t ring = (size_t)NS * Slot<T, TZ, R>::bytes;
     static constexpr size_t smem = ring + 2 * NS * 8;  // box ring | mbarriers
@@ -588,13 +588,10 @@ __device__ __forceinline__ bool xtma_march(const TmaMaps *const &mp, const Stage
                     outm[f][p] = uin[f][p] + cY * kk[f];  // Y4
                 } else if (MODE == MODE_S2B) {
                     const T u = uin[f][p];
-                    ain[f][p] = (cen[f] - u) + cA * kk[f];  // B = dt/2 k1 + dt k2
+                    ain[f][p] = (u + cen[f]) + cA * kk[f];  // B = U + Y2 + dt k2
                     outm[f][p] = u + cY * kk[f];            // Y3
                 } else {
-                    // U + [B + (Y4 - U)]/3 + dt/6 k4: the increments are summed
-                    // first, U is added last
-                    const T u = uin[f][p];
-                    outm[f][p] = u + fma(ain[f][p] + (cen[f] - u), T(1.0 / 3.0), cA * kk[f]);
+                    outm[f][p] = third_plus(ain[f][p] + cen[f], cA * kk[f]);  // (B + Y4)/3 + dt/6 k4
                 }
             }
         }

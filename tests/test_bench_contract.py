@@ -62,7 +62,7 @@ def test_step_traffic_from_profiles():
             continue
         want = sum(t[k] for k in keys)
         assert bench.step_traffic(dt, 1024, 642) == want
-        # within 10 % of the bytes the 13-pass step moves (832 / 416 B per cell-step)
+        # within 10 % of the bytes the 12-pass step moves (768 / 384 B per cell-step)
         moved = bench.MOVED_BYTES_PER_CELL_STEP[dt] * 1024 * 1024 * 642
         assert 1.0 <= want / moved < 1.1
     assert bench.step_traffic("f64", 512, 642) is None
