@@ -266,7 +266,10 @@ class Server:
                 for rid, h in halted.items():
                     if recs[rid].diverged_at < 0:
                         stream(rid, h, None)  # the failing device-side check is the solve's last record
-                    recs[rid].last_good = max(recs[rid].last_good, h - self.halt_every)  # the previous check passed
+                    # the previous check passed: the last multiple of halt_every below h, or a later
+                    # passing record, which stream() has already counted
+                    prev = (h - 1) // self.halt_every * self.halt_every
+                    recs[rid].last_good = max(recs[rid].last_good, prev)
                 host["collect_s"] += time.perf_counter() - tc
                 done = []
                 for rid in ran:

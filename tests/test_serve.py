@@ -334,3 +334,29 @@ def test_device_stop_retires_failed_solves_at_once():
     for r in ok:
         assert made[r.rid].steps == r.steps
     assert not FakeBatch.live
+
+
+def test_device_stop_counts_work_to_the_last_passing_check():
+    """With records every 15 steps and checks every 10, the check grid and the
+    record grid interleave (10, 15, 20, 30, 40, 45, ...). A solve that blows
+    up at step 41 fails the check at record step 45; the last check it passed
+    is the one at step 40, and its work is counted up to there."""
+    reqs = serve.draw_requests(3, rate=0.0, seed=5, steps=(300, 300), sizes=(32,), nns=(2,))
+    BlowUpSolver.bad = {reqs[0].rid: 41}
+    made, diags = {}, {}
+
+    def factory(req, device):
+        made[req.rid] = BlowUpSolver(req)
+        return made[req.rid]
+
+    srv = serve.Server(budget_bytes=1e12, stream_every=15, solver_factory=factory, batch_factory=HaltBatch,
+                       quantum_s=1e9, halt_every=10,
+                       on_diag=lambda rid, step, d: diags.setdefault(rid, []).append((step, d)))
+    rep = srv.run(reqs)
+    assert rep["failed"] == 1 and rep["served"] == 2
+    assert made[reqs[0].rid].steps == 45
+    assert [s for s, _ in diags[reqs[0].rid]] == [0, 15, 30, 45] and diags[reqs[0].rid][-1] == (45, None)
+    cells = 32 * 32 * 42
+    assert rep["failed_cell_steps_counted"] == 40 * cells
+    assert rep["failed_cell_steps_run"] == 45 * cells
+    assert not FakeBatch.live
