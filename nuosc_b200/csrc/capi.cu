@@ -1706,6 +1706,12 @@ int batch_build(nuosc_batch *b) {
 
 template <typename T>
 int batch_step_impl(nuosc_batch *b, int nsteps, int every, nuosc_batch_record *out, int max_out, int *n_out) {
+    if (every > 0) {  // the records this call streams must fit before anything is launched
+        long long need = 0;
+        for (const nuosc_handle *h : b->m) need += (h->steps_done + nsteps) / every - h->steps_done / every;
+        if (need > max_out)
+            return fail(NUOSC_ERR_INVALID, "batch_step_stream: %lld records for a buffer of %d", need, max_out);
+    }
     if (batch_signature(b) != b->sig)
         if (int rc = batch_build<T>(b)) return rc;
     // after everything queued on the members' streams

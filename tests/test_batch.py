@@ -132,6 +132,33 @@ def test_batch_rejects_bad_membership(nb):
             s.close()
 
 
+def test_batch_stream_refuses_small_record_buffer(nb):
+    """nuosc_batch_step_stream with a record buffer smaller than the records
+    the call streams is refused before anything runs: no member steps, and
+    the same call with room for its records then matches solo stepping."""
+    import ctypes as C
+    a, b = build(nb, 32, 32, 2), build(nb, 48, 32, 2, seed=4)
+    ta, tb = build(nb, 32, 32, 2), build(nb, 48, 32, 2, seed=4)
+    try:
+        with nb.Batch([a, b]) as bt:
+            recs = (nb._lib.BatchRecord * 4)()
+            n = C.c_int(-1)
+            rc = nb.lib().nuosc_batch_step_stream(bt.handle, 10, 5, recs, 3, C.byref(n))  # needs 2 x 2 records
+            assert rc == nb._lib.ERR_INVALID and n.value == 0
+            assert a.step_count == 0 and b.step_count == 0
+            rc = nb.lib().nuosc_batch_step_stream(bt.handle, 10, 5, recs, 4, C.byref(n))
+            assert rc == nb._lib.OK and n.value == 4
+            assert sorted((r.member, r.step) for r in recs) == [(0, 5), (0, 10), (1, 5), (1, 10)]
+            bt.synchronize()
+        ta.step_rk4(10)
+        tb.step_rk4(10)
+        assert_same(a, ta)
+        assert_same(b, tb)
+    finally:
+        for s in (a, b, ta, tb):
+            s.close()
+
+
 def off_polarised(nb, s):
     """A state whose polarisation is far off |P| = 1 (emr 20x the diagonal):
     max||P|-1| is about 19, so the reference's stop test fails at once."""
