@@ -244,7 +244,8 @@ int nuosc_set_n_nue0(nuosc_handle *h, double n0, double n1);
  * the spectra G0/G0b, time, step count, n_nue0, mu, pmo, renorm and the cell
  * moments held for v_stat; load restores them into a handle created with
  * the same grid, velocity count, precision, ghost width, dt and ko (else
- * NUOSC_ERR_INVALID).  A run stopped after step n, saved, loaded into a new
+ * NUOSC_ERR_INVALID; a file of another grid or of the wrong size is refused
+ * before the handle is changed).  A run stopped after step n, saved, loaded into a new
  * handle and continued is bit-identical to the uninterrupted run.  Both
  * synchronise the handle's stream and stage the state through 256 MB of
  * page-locked host memory. */

@@ -1370,12 +1370,25 @@ int nuosc_load_checkpoint(nuosc_handle *h, const char *path) {
              c.ko != h->ko)
         rc = fail(NUOSC_ERR_INVALID, "checkpoint %s: grid %dx%dx%d (precision %d, ghost %d) does not match the handle",
                   path, c.nx, c.nz, c.nv, c.precision, c.ghost);
+    if (!rc) {  // the whole file is checked before the handle is touched
+        const long long want = 8 + (long long)sizeof c + 2ll * c.nv * (long long)sizeof(double) +
+                               (long long)h->g.fs * NF * h->esize +
+                               (c.mom_valid ? (long long)h->g.ncell * NMOM * (long long)sizeof(double) : 0);
+        const long here = ftell(f);
+        long long size = -1;
+        if (here >= 0 && fseek(f, 0, SEEK_END) == 0) size = ftell(f);
+        if (size != want || fseek(f, here, SEEK_SET) != 0)
+            rc = fail(NUOSC_ERR_INVALID, "checkpoint %s: %lld bytes, expected %lld", path, size, want);
+    }
     std::vector<double> G0(c.nv > 0 ? c.nv : 0), G0b(G0.size());
     if (!rc && (fread(G0.data(), sizeof(double), G0.size(), f) != G0.size() ||
                 fread(G0b.data(), sizeof(double), G0b.size(), f) != G0b.size()))
         rc = fail(NUOSC_ERR_INVALID, "checkpoint: file is truncated");
     if (!rc) {
-        CUDA_TRY(cudaStreamSynchronize(h->stream));
+        const cudaError_t e = cudaStreamSynchronize(h->stream);
+        if (e != cudaSuccess) rc = fail(NUOSC_ERR_CUDA, "checkpoint: %s", cudaGetErrorString(e));
+    }
+    if (!rc) {
         h->G0 = G0;
         h->G0b = G0b;
         rc = upload_spectra(h);

@@ -68,3 +68,32 @@ def test_checkpoint_of_another_grid_is_refused(gpu, tmp_path):
         other.close()
     with pytest.raises(nb.NuoscError):
         _solver(nb).load_checkpoint(str(tmp_path / "missing.ck"))
+
+
+def test_truncated_checkpoint_leaves_the_handle_unchanged(gpu, tmp_path):
+    """A checkpoint file cut short (or with bytes appended) is refused before
+    anything is read into the handle: its state, spectra and step count stay
+    as they were."""
+    import nuosc_b200 as nb
+    a = _solver(nb)
+    a.fillInitValue(1, 0.9, 1e-3, 1.0, 0.6, 0.5, seed=2)
+    a.step_rk4(3)
+    path = tmp_path / "a.ck"
+    a.save_checkpoint(str(path))
+    a.close()
+    raw = path.read_bytes()
+    b = _solver(nb)
+    b.fillInitValue(1, 1.1, 1e-4, 0.8, 0.5, 0.4, seed=5)
+    before, d_before = b.get_state(), b.analysis()
+    for bad in (raw[:-8], raw + b"\0" * 8):
+        cut = tmp_path / "bad.ck"
+        cut.write_bytes(bad)
+        with pytest.raises(nb.NuoscError) as e:
+            b.load_checkpoint(str(cut))
+        assert e.value.code == nb._lib.ERR_INVALID
+        assert b.step_count == 0
+        assert np.array_equal(b.get_state().view(np.uint64), before.view(np.uint64))
+        assert b.analysis() == d_before
+    b.load_checkpoint(str(path))  # the intact file still loads
+    assert b.step_count == 3
+    b.close()
