@@ -191,7 +191,11 @@ int nuosc_analysis(nuosc_handle *h, nuosc_diag *out);
 int nuosc_open_analysis_file(nuosc_handle *h, const char *path);
 
 /* NuOsc::addSnapShotAtV / addSnapShotAtXV / checkSnapShot (nuosc_snapshot.cpp:13-122).
- * `fields` are NUOSC_* field ids of the current v_stat (0..15). */
+ * `fields` are NUOSC_* field ids of the current v_stat (0..15).  `fntpl` is a
+ * printf format given the step number alone: at most one integer conversion
+ * (e.g. "ee%06d.bin"; flags, width and precision allowed, no '*' or length
+ * modifier), '%' written as "%%" elsewhere; any other template is refused
+ * with NUOSC_ERR_INVALID. */
 int nuosc_add_snapshot_at_v(nuosc_handle *h, const int *fields, int nfields, const char *fntpl, int every,
                             const int *vidx, int n_vidx);
 int nuosc_add_snapshot_at_xv(nuosc_handle *h, const int *fields, int nfields, const char *fntpl, int every,

@@ -676,6 +676,23 @@ int get_state_impl(nuosc_handle *h, int reg, int field, double *host, int layout
     return 0;
 }
 
+// A snapshot file-name template is a printf format given one int (the step):
+// at most one integer conversion (flags, width and precision allowed, no '*'
+// and no length modifier), every other '%' written as "%%".
+bool step_template_ok(const char *t) {
+    int conversions = 0;
+    for (const char *p = t; *p; ++p) {
+        if (*p != '%') continue;
+        if (*++p == '%') continue;
+        while (*p && strchr("-+ #0", *p)) ++p;
+        while (*p >= '0' && *p <= '9') ++p;
+        if (*p == '.')
+            for (++p; *p >= '0' && *p <= '9';) ++p;
+        if (!*p || !strchr("diuoxX", *p) || ++conversions > 1) return false;
+    }
+    return true;
+}
+
 int write_meta(nuosc_handle *h, const Snapshot &s, bool at_xv) {
     char filename[4096];
     std::string tmp = s.fntpl + ".meta";
@@ -1260,6 +1277,8 @@ int nuosc_open_analysis_file(nuosc_handle *h, const char *path) {
 int nuosc_add_snapshot_at_v(nuosc_handle *h, const int *fields, int nfields, const char *fntpl, int every,
                             const int *vidx, int n_vidx) {
     if (!h || !fntpl) return fail(NUOSC_ERR_INVALID, "null argument");
+    if (!step_template_ok(fntpl))
+        return fail(NUOSC_ERR_INVALID, "snapshot template %s: one integer conversion at most", fntpl);
     if (int rc = check_indices(h, fields, nfields, nullptr, 0, vidx, n_vidx)) return rc;
     Snapshot s;
     s.fields.assign(fields, fields + nfields);
@@ -1275,6 +1294,8 @@ int nuosc_add_snapshot_at_v(nuosc_handle *h, const int *fields, int nfields, con
 int nuosc_add_snapshot_at_xv(nuosc_handle *h, const int *fields, int nfields, const char *fntpl, int every,
                              const int *xidx, int n_xidx, const int *vidx, int n_vidx) {
     if (!h || !fntpl) return fail(NUOSC_ERR_INVALID, "null argument");
+    if (!step_template_ok(fntpl))
+        return fail(NUOSC_ERR_INVALID, "snapshot template %s: one integer conversion at most", fntpl);
     if (n_xidx <= 0 || !xidx) return fail(NUOSC_ERR_INVALID, "no x indices");
     if (int rc = check_indices(h, fields, nfields, xidx, n_xidx, vidx, n_vidx)) return rc;
     Snapshot s;

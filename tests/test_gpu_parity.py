@@ -261,6 +261,11 @@ def test_snapshot_files_match_reference(nb, tmp_path):
     for name in ("ee000000.bin", "ee000000.bin.meta", "xv000000.bin", "xv000000.bin.meta"):
         mine = (tmp_path / name).read_bytes()
         assert mine == g[name.replace(".", "_")].tobytes(), name
+    # a file-name template is a format given the step alone
+    for bad in ("ee%s.bin", "ee%d_%d.bin", "ee%ld.bin", "ee%*d.bin"):
+        with pytest.raises(nb.NuoscError) as e:
+            s.addSnapShotAtV([0], str(tmp_path / bad), 1, [0])
+        assert e.value.code == nb._lib.ERR_INVALID
 
 
 def test_gather_derived_fields(nb):
