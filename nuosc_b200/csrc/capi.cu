@@ -793,6 +793,15 @@ int diag_check(const nuosc_diag &d) {
 
 }  // namespace
 
+// The box, spacing and coefficients of nuosc_params: finite, positive
+// spacing, and cell counts int((x1 - x0)/dx), int((z1 - z0)/dz) below 2^30.
+static bool box_ok(const nuosc_params *p) {
+    for (double x : {p->x0, p->x1, p->z0, p->z1, p->dx, p->dz, p->cfl, p->ko})
+        if (!std::isfinite(x)) return false;
+    if (!(p->dx > 0) || !(p->dz > 0) || !(p->x1 > p->x0) || !(p->z1 > p->z0)) return false;
+    return (p->x1 - p->x0) / p->dx < 1073741824.0 && (p->z1 - p->z0) / p->dz < 1073741824.0;
+}
+
 extern "C" {
 
 const char *nuosc_last_error(void) { return g_err.c_str(); }
@@ -819,8 +828,7 @@ int nuosc_create(const nuosc_params *p, nuosc_handle **out) {
     if (p->nv < 1 || p->nv > 64) return fail(NUOSC_ERR_INVALID, "icosahedron subdivision nv=%d out of range", p->nv);
     if (p->gx != p->gz || (p->gx != 2 && p->gx != 3))
         return fail(NUOSC_ERR_INVALID, "ghost width gx=%d gz=%d: must be equal and 2 or 3", p->gx, p->gz);
-    if (!(p->dx > 0) || !(p->dz > 0) || !(p->x1 > p->x0) || !(p->z1 > p->z0))
-        return fail(NUOSC_ERR_INVALID, "bad box or spacing");
+    if (!box_ok(p)) return fail(NUOSC_ERR_INVALID, "bad box, spacing or coefficient (finite; dx, dz > 0)");
     if (p->precision != NUOSC_FP64 && p->precision != NUOSC_FP32)
         return fail(NUOSC_ERR_INVALID, "precision %d", p->precision);
     nuosc_handle *h = new nuosc_handle;
@@ -900,7 +908,7 @@ int nuosc_create_slab(const nuosc_params *p, int rank, nuosc_handle **out) {
     *out = nullptr;
     if (p->px < 1 || p->pz != 1 || rank < 0 || rank >= p->px)
         return fail(NUOSC_ERR_INVALID, "slab %d of px=%d pz=%d (x-slabs: pz = 1, 0 <= rank < px)", rank, p->px, p->pz);
-    if (!(p->dx > 0) || !(p->x1 > p->x0)) return fail(NUOSC_ERR_INVALID, "bad box or spacing");
+    if (!box_ok(p)) return fail(NUOSC_ERR_INVALID, "bad box, spacing or coefficient (finite; dx, dz > 0)");
     const int nxg = (int)((p->x1 - p->x0) / p->dx), R = p->gx;
     const int base = nxg / p->px, rem = nxg % p->px;
     const int nx = base + (rank < rem ? 1 : 0), xoff = rank * base + std::min(rank, rem);

@@ -64,11 +64,18 @@ def test_bad_arguments_return_codes():
                 ko=0.1, precision=0, device=0)
     for bad, code in ((dict(px=2), _lib.ERR_UNSUPPORTED), (dict(gx=4, gz=4), _lib.ERR_INVALID),
                       (dict(gx=3, gz=2), _lib.ERR_INVALID), (dict(dx=0.0), _lib.ERR_INVALID),
-                      (dict(precision=7), _lib.ERR_INVALID), (dict(nv=0), _lib.ERR_INVALID)):
+                      (dict(precision=7), _lib.ERR_INVALID), (dict(nv=0), _lib.ERR_INVALID),
+                      (dict(ko=float("nan")), _lib.ERR_INVALID), (dict(cfl=float("inf")), _lib.ERR_INVALID),
+                      (dict(x1=float("inf")), _lib.ERR_INVALID), (dict(dz=-0.1), _lib.ERR_INVALID),
+                      (dict(dx=1e-12), _lib.ERR_INVALID)):  # (0.8 / 1e-12 cells: more than an int holds)
         p = _lib.Params(**{**base, **bad})
         h = C.c_void_p()
         assert lib.nuosc_create(C.byref(p), C.byref(h)) == code
         assert not h.value
+        if code == _lib.ERR_INVALID and "gx" not in bad and "precision" not in bad and "nv" not in bad:
+            p = _lib.Params(**{**base, "px": 2, **bad})
+            assert lib.nuosc_create_slab(C.byref(p), 0, C.byref(h)) == _lib.ERR_INVALID
+            assert not h.value
 
 
 @pytest.mark.skipif(has_gpu(), reason="checks the no-device path")
