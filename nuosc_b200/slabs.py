@@ -43,7 +43,12 @@ def exchange(send_lo, send_hi, recv_lo, recv_hi, left, right, rank, group=None):
     lists of equal-sized tensors (CUDA for NCCL, CPU for gloo); left, right and
     rank are ranks of `group`.  A slab that is its own neighbour (one slab)
     copies locally.  Sends to the right carry tag 2f, sends to the left 2f+1,
-    so with two slabs (left == right) each piece still meets its place."""
+    so with two slabs (left == right) each piece still meets its place under
+    gloo.  NCCL ignores tags and matches the operations between two ranks in
+    the order they are issued; per field every rank issues send right,
+    receive left, send left, receive right, so with two slabs rank a's sends
+    to b (send_hi[f], then send_lo[f]) meet b's receives from a (recv_lo[f],
+    then recv_hi[f]) in the same order."""
     import torch.distributed as dist
     if left == rank and right == rank:
         for f in range(len(send_lo)):
