@@ -27,9 +27,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 TILES = os.path.join(HERE, "tiles.txt")
 DEFAULT_LX = (32, 64, 128, 256, 1 << 20)
 # Largest summation error of the fused FP32 cell moments accepted, relative to
-# the largest moment: FP64 accumulation of the stored state's values (the
-# north star's "FP64 or compensated two-sum" moments) stays near 1e-15; float
-# partials are near 1e-7 and are rejected.
+# the largest moment: FP64 accumulation of the stored state's values stays
+# near 1e-15 (a compensated float two-sum would have to reach the same bar);
+# float partials are near 1e-7 and are rejected.
 MSUM_TOL = 1e-12
 
 
