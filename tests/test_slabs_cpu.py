@@ -94,3 +94,41 @@ def test_split_covers_the_planes():
         assert parts[0][0] == 0 and sum(n for _, n in parts) == nx
         assert all(parts[r][0] + parts[r][1] == parts[r + 1][0] for r in range(px - 1))
         assert max(n for _, n in parts) - min(n for _, n in parts) <= 1
+
+
+def _reduce_main(rank, world, port, out):
+    os.environ.update(RANK=str(rank), WORLD_SIZE=str(world), MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    sys.path.insert(0, ROOT)
+    import datetime
+
+    import torch.distributed as dist
+    from nuosc_b200 import slabs
+
+    dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=60))
+    q = np.arange(12, dtype=np.float64) * (rank + 1) + 0.25 * rank
+    q[0] = [3.0, 7.5, 1.0][rank]  # max||P|-1| of this slab
+    out.put((rank, slabs._reduce_sums(q)))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_diagnostic_sums_reduce_over_slabs(world):
+    """The slabs' raw analysis sums combine as the whole solve's: the maximum
+    for max||P|-1| (entry 0), the sum for every other entry (the weighted
+    sums and the non-finite count), on every rank alike."""
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    out = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_reduce_main, args=(r, world, port, out)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = dict(out.get(timeout=300) for _ in range(world))
+    for p in procs:
+        p.join(timeout=60)
+    assert all(p.exitcode == 0 for p in procs)
+    want = sum(np.arange(12, dtype=np.float64) * (r + 1) + 0.25 * r for r in range(world))
+    want[0] = max([3.0, 7.5, 1.0][:world])
+    for r in range(world):
+        assert np.array_equal(res[r], want)
