@@ -383,7 +383,8 @@ int nuosc_batch_step(nuosc_batch *b, int nsteps);
  * count (nuosc_step_count) reaches a multiple of `every`, the analysis of
  * that member is queued on the batch stream right after that step and its raw
  * sums are copied into the next record of `out` -- no host synchronisation.
- * *n_out = records queued (at most max_out, else NUOSC_ERR_INVALID); they are
+ * *n_out = records queued; a call whose records would not fit in max_out is
+ * refused with NUOSC_ERR_INVALID before any member steps.  Records are
  * complete after nuosc_batch_synchronize.  `out` should be page-locked
  * (nuosc_host_alloc): a pageable buffer makes each copy synchronous.
  * nuosc_batch_record_diag turns a record into the nuosc_diag that
